@@ -1,0 +1,287 @@
+"""Benchmark driver: python bench.py --gpus N --steps K --warmup W [--impl ours|reference]
+
+Prints ONE JSON line on rank 0 (see the field list in `emit`). Workloads
+(--workload) are the hot-path configurations with synthetic seeded inputs:
+
+  laplace  2D Laplace Jacobi, single block 4096x4096 FP64, 5-point stencil,
+           seeded U[0,1) Dirichlet ring, interior 0; a step is one iteration
+           (apply_stencil + max|delta| reduction read back + copy).
+
+`value` is device-timed (CUDA events on the runtime stream) with inputs
+resident in HBM; `e2e` times the same work through the public C-ABI call
+from host buffers (field upload, per-step result read-back, field download)
+by wall clock. With N > 1 (torchrun) every rank runs its own replica of the
+workload (weak scaling, no data-path collective) and rank 0 reports the
+whole-job rate over the slowest rank's time.
+
+--impl reference times the reference's own OpenMP build (oracle/_ref) on the
+host cores for the same workload and metric (rank 0 only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, value, local):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is None:
+        return
+    import torch
+    torch.cuda.synchronize(local)
+    pg.barrier()
+    torch.cuda.synchronize(local)
+
+
+# ---------------------------------------------------------------------------
+# Laplace
+# ---------------------------------------------------------------------------
+LAP_N = 4096
+
+
+def cpu_reference_laplace(iters, threads):
+    import oracle
+    exe = oracle.reference_binary("laplace2d_seeded")
+    if exe is None:
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+    with tempfile.TemporaryDirectory() as td:
+        r = subprocess.run([exe, str(LAP_N), str(LAP_N), str(iters), "1"], cwd=td, capture_output=True, text=True,
+                           env=env, timeout=600, check=True)
+    secs = [float(l.split()[1]) for l in r.stdout.splitlines() if l.startswith("wall_seconds")][0]
+    return LAP_N * LAP_N * iters / secs, secs
+
+
+def bench_laplace(args, world, rank, local, pg):
+    import numpy as np
+
+    from ops_b200 import apps, seeded
+    from ops_b200 import ops as O
+
+    peaks, peak_kind = load_peaks()
+    O.ops_init(local, 0)
+    field = seeded.laplace_field(LAP_N, LAP_N, 1)
+    cells = LAP_N * LAP_N
+    K, W = args.steps, args.warmup
+
+    # value: W untimed + K timed iterations, inputs resident, CUDA events.
+    barrier(pg, local)
+    O.reset_counters()
+    with ClockSampler(local) as cs:
+        _, errs, secs = apps.laplace2d(field, K, warmup=W)
+    clocks = cs.summary()
+    c = O.counters()
+    launches_timed = int(round(c["kernels"] * K / max(1, K + W)))
+    barrier(pg, local)
+    secs = max_over_ranks(pg, secs, local)
+
+    # roofline: per-kernel CUDA-event durations of the dominant kernel.
+    O.set_kernel_timing(1)
+    O.clear_kernel_timing()
+    apps.laplace2d(field, K, warmup=0)
+    n, ms = O.kernel_time("laplace2d/apply_stencil")
+    O.set_kernel_timing(0)
+    avg_s = ms * 1e-3 / max(n, 1)
+    alg_bytes = 16.0 * cells  # read A, write Anew per cell-update
+    achieved = alg_bytes / avg_s / 1e9
+
+    # e2e: the public C-ABI call from host buffers, wall clock.
+    import torch
+    pinned = torch.from_numpy(field).pin_memory().numpy()
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    out, _, _ = apps.laplace2d(pinned, K, warmup=0)
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(pg, t1 - t0, local)
+
+    value = world * cells * K / secs
+    line = {
+        "metric": "cell-updates/s",
+        "value": value,
+        "unit": "cell-updates/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": secs * 1e3 / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded SplitMix64 boundary ring, interior 0)",
+        "config": {"workload": "laplace2d_jacobi_4096x4096_fp64", "grid": [LAP_N, LAP_N], "halo": 1,
+                   "step": "apply_stencil + max|delta| readback + copy (elided by renaming)",
+                   "l2": "inputs larger than L2 (two 134 MB fields)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "kernel": "laplace2d/apply_stencil", "alg_bytes_per_launch": alg_bytes,
+                     "avg_launch_ms": avg_s * 1e3, "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": world * cells * K / e2e_s, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": field.nbytes / K, "d2h_bytes_per_step": 8 + out.nbytes / K,
+                "note": "one C-ABI call: field upload, K iterations each reading max|delta| back, field download"},
+        "gpu_launches": launches_timed,
+        "clocks": clocks,
+        "final_error": float(errs[-1]),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        base = cpu_reference_laplace(args.cpu_iters, threads)
+        if base:
+            line["cpu_baseline"] = {"value": base[0], "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                                    "sample": f"reference laplace2d OpenMP build, {LAP_N}^2, {args.cpu_iters} iterations,"
+                                              f" {base[1]:.2f} s"}
+    return line
+
+
+def reference_laplace(args, world, rank):
+    threads = os.cpu_count() or 1
+    iters = max(1, min(args.steps, 200))
+    base = cpu_reference_laplace(iters, threads)
+    if base is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/bin/laplace2d_seeded was not built"}
+    v, secs = base
+    return {
+        "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": iters, "warmup": 0, "ms_per_step": secs * 1e3 / iters, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64 boundary ring, interior 0)",
+        "config": {"workload": "laplace2d_jacobi_4096x4096_fp64", "grid": [LAP_N, LAP_N]},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                         "sample": f"{iters} iterations of the reference OpenMP build on {threads} host threads"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+WORKLOADS = {"laplace": (bench_laplace, reference_laplace)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="laplace")
+    ap.add_argument("--cpu-iters", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local, pg = dist_setup(args)
+    ours, ref = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(ref(args, world, rank)), flush=True)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    line = ours(args, world, rank, local, pg)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+/*
+ * OPS-B200: C-ABI of the B200-native OPS execution backend.
+ *
+ * Plain C types only (handles are ints, data are pointers + sizes). Every
+ * entry point returns 0 (or a non-negative handle) on success and a negative
+ * OPS_B200_ERR_* code on failure; ops_b200_last_error() then describes it.
+ * Each declaration names the reference OPS interface it stands in for
+ * (paths relative to the OPS source tree).
+ *
+ * Threading: one host thread drives one process-wide instance, as in the
+ * reference (ops/c/src/core/ops_instance.cpp:37). Loops are queued lazily and
+ * run on one CUDA stream; ops_b200_reduction_result, the data-access calls
+ * and ops_b200_execute are the synchronisation points.
+ */
+#ifndef OPS_B200_H
+#define OPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define OPS_B200_OK 0
+#define OPS_B200_ERR_ARG (-1)          /* invalid argument or handle        */
+#define OPS_B200_ERR_CUDA (-2)         /* CUDA runtime error / no device    */
+#define OPS_B200_ERR_STATE (-3)        /* call not valid in current state   */
+#define OPS_B200_ERR_NOTFOUND (-4)     /* unknown loop kernel name          */
+#define OPS_B200_ERR_TIMEOUT (-5)      /* a bounded device-side wait expired */
+#define OPS_B200_ERR_UNSUPPORTED (-6)  /* outside what the backend supports */
+
+/* Access modes and argument kinds keep the reference's values
+ * (ops/c/include/ops_lib_core.h:84-93). */
+#define OPS_B200_READ 0
+#define OPS_B200_WRITE 1
+#define OPS_B200_RW 2
+#define OPS_B200_INC 3
+#define OPS_B200_MIN 4
+#define OPS_B200_MAX 5
+#define OPS_B200_ARG_GBL 0
+#define OPS_B200_ARG_DAT 1
+#define OPS_B200_ARG_IDX 2
+#define OPS_B200_ARG_REDUCE 3
+/* Memory spaces (ops_memspace, ops/c/include/ops_lib_core.h). */
+#define OPS_B200_HOST 1
+#define OPS_B200_DEVICE 2
+
+/* Description of the last failure on this thread (never NULL). */
+const char *ops_b200_last_error(void);
+
+/* ops_init (ops/c/src/core/ops_dummy_singlenode.cpp:979): selects the CUDA
+ * device and creates the instance. Fails with OPS_B200_ERR_CUDA when no GPU
+ * is present; there is no CPU execution path. */
+int ops_b200_init(int device, int diags);
+/* ops_exit (ops/c/src/core/ops_lib_core.cpp): frees all device storage. */
+int ops_b200_exit(void);
+
+/* ops_decl_block (ops/c/include/ops_lib_core.h:611). Returns a block handle. */
+int ops_b200_decl_block(int dims, const char *name);
+
+/* ops_decl_dat -> ops_decl_dat_char (ops/c/include/ops_lib_core.h:647,
+ * ops/c/src/core/ops_device_singlenode_common.cpp:44). size/base/d_m/d_p have
+ * `dims` entries; the allocated extent is size - d_m + d_p per dimension.
+ * `data` (may be NULL) holds that full extent, x fastest, and is copied.
+ * Returns a dat handle. */
+int ops_b200_decl_dat(int block, int dim, const int *size, const int *base, const int *d_m, const int *d_p,
+                      const void *data, int type_size, const char *type, const char *name);
+
+/* ops_decl_stencil / ops_decl_strided_stencil
+ * (ops/c/src/core/ops_lib_core.cpp:640,689). `stride` may be NULL. */
+int ops_b200_decl_stencil(int dims, int points, const int *stencil, const char *name);
+int ops_b200_decl_strided_stencil(int dims, int points, const int *stencil, const int *stride, const char *name);
+
+/* ops_decl_reduction_handle (ops/c/src/core/ops_lib_core.cpp:1119). */
+int ops_b200_decl_reduction_handle(int size, const char *type, const char *name);
+
+/* ops_decl_const / ops_update_const (ops/c/include/ops_lib_core.h:947,971):
+ * flushes queued loops, then updates every kernel constant of that name. */
+int ops_b200_decl_const(const char *name, int dim, const char *type, const void *data);
+int ops_b200_update_const(const char *name, int dim, const char *type, const void *data);
+
+/* One loop argument (ops_arg, ops/c/include/ops_lib_core.h:509). */
+typedef struct ops_b200_arg {
+  int argtype;      /* OPS_B200_ARG_*                                      */
+  int dat;          /* DAT: dat handle                                     */
+  int stencil;      /* DAT: stencil handle                                 */
+  int dim;          /* components (DAT), elements (GBL), width (REDUCE)    */
+  int acc;          /* OPS_B200_READ ... OPS_B200_MAX                      */
+  int opt;          /* DAT: 1 active, 0 disabled (ops_arg_dat_opt)         */
+  int reduction;    /* REDUCE: reduction handle                            */
+  int elem_size;    /* GBL: bytes per element                              */
+  const void *gbl;  /* GBL: payload, copied when the loop is queued        */
+} ops_b200_arg;
+
+/* ops_par_loop (ops/c/include/ops_seq_v2.h:312, queued like
+ * create_kerneldesc_and_enque, ops/c/src/core/ops_lazy.cpp:1403). `kernel`
+ * names a registered sm_100a loop kernel ("<app>/<kernel>", e.g.
+ * "laplace2d/apply_stencil"); range has 2*dim entries {begin, end, ...}. */
+int ops_b200_par_loop(const char *kernel, const char *name, int block, int dim, const int *range, int nargs,
+                      const ops_b200_arg *args);
+/* 1 if a loop kernel of that name is registered, else 0. */
+int ops_b200_has_kernel(const char *kernel);
+
+/* ops_execute (ops/c/src/core/ops_lazy.cpp:1248): run all queued loops. */
+int ops_b200_execute(void);
+
+/* ops_reduction_result (ops/c/src/core/ops_lib_core.cpp:1143): flushes the
+ * queue and copies the handle's value (size bytes) to `out`. */
+int ops_b200_reduction_result(int handle, void *out);
+
+/* ops_dat_set_data / ops_dat_fetch_data
+ * (ops/c/src/core/ops_dummy_singlenode.cpp:737-808): the full extent
+ * (halos included), x fastest; `bytes` must equal that extent. */
+int ops_b200_dat_set_data(int dat, const void *data, size_t bytes);
+int ops_b200_dat_fetch_data(int dat, void *data, size_t bytes);
+/* ops_dat_get_extents: disp/size of the full extent (dims entries each). */
+int ops_b200_dat_get_extents(int dat, int *disp, int *size);
+/* ops_dat_get_raw_pointer / ops_dat_release_raw_data
+ * (ops/c/src/core/ops_dummy_singlenode.cpp:662-735). Returns a pointer to
+ * logical index 0 in the requested memory space; stride[0..2] receives the
+ * x pitch and the y/z extents in elements. */
+int ops_b200_dat_get_raw_pointer(int dat, int memspace, void **ptr, int *stride);
+int ops_b200_dat_release_raw_data(int dat, int acc);
+
+/* Runtime options: "graphs" (CUDA-graph replay of repeated flushes, default
+ * 1) and "fusion" (copy elision and chain kernels, default 1). */
+int ops_b200_set_option(const char *name, int value);
+/* Counters since the last reset: kernels launched by this library, CUDA
+ * graphs launched, loops queued. */
+int ops_b200_counters(long long *kernels, long long *graphs, long long *loops);
+int ops_b200_reset_counters(void);
+
+/* Per-kernel device timing: while enabled, every launch is bracketed by CUDA
+ * events on the runtime stream (graph replay is bypassed). Query by kernel
+ * name ("laplace2d/apply_stencil", a chain rule name, ...): launches and total
+ * milliseconds since the last clear. */
+int ops_b200_set_kernel_timing(int on);
+int ops_b200_kernel_time(const char *kernel, long long *launches, double *total_ms);
+int ops_b200_clear_kernel_timing(void);
+
+/* ---- apps ----------------------------------------------------------------
+ * Reference app drivers restated in C++ on the runtime above; they issue the
+ * same sequence of loops as the reference drivers.
+ *
+ * Laplace Jacobi (apps/c/laplace2d_tutorial/step7/laplace2d.cpp:41-124):
+ * `field_in` is A's full extent ((imax+2)*(jmax+2) doubles, x fastest, halo
+ * ring = boundary values); `warmup` + `iters` fixed iterations of
+ * apply_stencil + max reduction + copy. Outputs (each may be NULL): final A
+ * extent, the max |delta| of each of the `warmup + iters` iterations, and the
+ * device seconds (CUDA events) of the last `iters` iterations. */
+int ops_b200_app_laplace2d(int imax, int jmax, int warmup, int iters, const double *field_in, double *field_out,
+                           double *err_per_iter, double *device_seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPS_B200_H */

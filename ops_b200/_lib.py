@@ -1,0 +1,88 @@
+"""ctypes binding of the OPS-B200 C-ABI (include/ops_b200.h).
+
+The shared library is built in-tree (ops_b200/libops_b200.so, see build.py).
+There is no fallback: if the library is missing or cannot be loaded, every
+entry point of this package raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libops_b200.so")
+
+OK = 0
+ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOTFOUND, ERR_TIMEOUT, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
+READ, WRITE, RW, INC, MIN, MAX = 0, 1, 2, 3, 4, 5
+ARG_GBL, ARG_DAT, ARG_IDX, ARG_REDUCE = 0, 1, 2, 3
+HOST, DEVICE = 1, 2
+
+
+class OpsError(RuntimeError):
+    """A failed C-ABI call (mirrors OPSException, ops/c/include/ops_exceptions.h:46)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Arg(ctypes.Structure):
+    _fields_ = [("argtype", ctypes.c_int), ("dat", ctypes.c_int), ("stencil", ctypes.c_int),
+                ("dim", ctypes.c_int), ("acc", ctypes.c_int), ("opt", ctypes.c_int),
+                ("reduction", ctypes.c_int), ("elem_size", ctypes.c_int), ("gbl", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OpsError(ERR_STATE, f"{LIB_PATH} is missing: build it with `python ops_b200/build.py`")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def check(rc):
+    if rc < 0:
+        msg = lib().ops_b200_last_error().decode()
+        raise OpsError(rc, msg)
+    return rc
+
+
+def _declare(L):
+    i, d, P, cp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
+    sz, ll = ctypes.c_size_t, ctypes.c_longlong
+    sig = {
+        "ops_b200_last_error": ([], cp),
+        "ops_b200_init": ([i, i], i),
+        "ops_b200_exit": ([], i),
+        "ops_b200_decl_block": ([i, cp], i),
+        "ops_b200_decl_dat": ([i, i, P, P, P, P, P, i, cp, cp], i),
+        "ops_b200_decl_stencil": ([i, i, P, cp], i),
+        "ops_b200_decl_strided_stencil": ([i, i, P, P, cp], i),
+        "ops_b200_decl_reduction_handle": ([i, cp, cp], i),
+        "ops_b200_decl_const": ([cp, i, cp, P], i),
+        "ops_b200_update_const": ([cp, i, cp, P], i),
+        "ops_b200_par_loop": ([cp, cp, i, i, P, i, P], i),
+        "ops_b200_has_kernel": ([cp], i),
+        "ops_b200_execute": ([], i),
+        "ops_b200_reduction_result": ([i, P], i),
+        "ops_b200_dat_set_data": ([i, P, sz], i),
+        "ops_b200_dat_fetch_data": ([i, P, sz], i),
+        "ops_b200_dat_get_extents": ([i, P, P], i),
+        "ops_b200_dat_get_raw_pointer": ([i, i, P, P], i),
+        "ops_b200_dat_release_raw_data": ([i, i], i),
+        "ops_b200_set_option": ([cp, i], i),
+        "ops_b200_counters": ([P, P, P], i),
+        "ops_b200_reset_counters": ([], i),
+        "ops_b200_set_kernel_timing": ([i], i),
+        "ops_b200_kernel_time": ([cp, P, P], i),
+        "ops_b200_clear_kernel_timing": ([], i),
+        "ops_b200_app_laplace2d": ([i, i, i, i, P, P, P, P], i),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res

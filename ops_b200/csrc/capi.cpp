@@ -1,0 +1,244 @@
+// extern "C" entry points of include/ops_b200.h over the C++ runtime.
+#include "../../include/ops_b200.h"
+
+#include <string>
+
+#include "runtime.h"
+
+namespace {
+thread_local std::string g_last_error = "no error";
+
+template <class F>
+int guarded(F &&f) {
+  try {
+    return f();
+  } catch (const opsb::Error &e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return OPS_B200_ERR_STATE;
+  } catch (...) {
+    g_last_error = "unknown exception";
+    return OPS_B200_ERR_STATE;
+  }
+}
+
+opsb::Runtime &rt() {
+  if (!opsb::Runtime::exists()) throw opsb::Error(opsb::E_STATE, "ops_b200_init has not been called");
+  return opsb::Runtime::get();
+}
+
+std::vector<opsb::Arg> convert_args(int nargs, const ops_b200_arg *args) {
+  std::vector<opsb::Arg> out;
+  if (nargs < 0 || nargs > OPSB_MAX_ARGS) throw opsb::Error(opsb::E_ARG, "bad argument count");
+  for (int i = 0; i < nargs; i++) {
+    const ops_b200_arg &a = args[i];
+    switch (a.argtype) {
+      case OPS_B200_ARG_DAT:
+        out.push_back(opsb::arg_dat_opt(a.dat, a.dim, a.stencil, a.acc, a.opt));
+        break;
+      case OPS_B200_ARG_GBL:
+        if (!a.gbl || a.dim <= 0 || a.elem_size <= 0) throw opsb::Error(opsb::E_ARG, "bad global argument");
+        out.push_back(opsb::arg_gbl(a.gbl, a.dim, a.elem_size, a.acc));
+        break;
+      case OPS_B200_ARG_REDUCE:
+        out.push_back(opsb::arg_reduce(a.reduction, a.dim, a.acc));
+        break;
+      case OPS_B200_ARG_IDX:
+        out.push_back(opsb::arg_idx());
+        break;
+      default:
+        throw opsb::Error(opsb::E_ARG, "unknown argument type");
+    }
+  }
+  return out;
+}
+}  // namespace
+
+extern "C" {
+
+const char *ops_b200_last_error(void) { return g_last_error.c_str(); }
+
+int ops_b200_init(int device, int diags) {
+  return guarded([&] {
+    opsb::Runtime::get().init(device, diags);
+    return 0;
+  });
+}
+
+int ops_b200_exit(void) {
+  return guarded([&] {
+    opsb::Runtime::destroy();
+    return 0;
+  });
+}
+
+int ops_b200_decl_block(int dims, const char *name) {
+  return guarded([&] { return rt().decl_block(dims, name); });
+}
+
+int ops_b200_decl_dat(int block, int dim, const int *size, const int *base, const int *d_m, const int *d_p,
+                      const void *data, int type_size, const char *type, const char *name) {
+  return guarded([&] {
+    if (!size || !d_m || !d_p) throw opsb::Error(opsb::E_ARG, "size, d_m and d_p are required");
+    return rt().decl_dat(block, dim, size, base, d_m, d_p, data, type_size, type, name);
+  });
+}
+
+int ops_b200_decl_stencil(int dims, int points, const int *stencil, const char *name) {
+  return guarded([&] {
+    if (!stencil) throw opsb::Error(opsb::E_ARG, "stencil offsets required");
+    return rt().decl_stencil(dims, points, stencil, nullptr, name);
+  });
+}
+
+int ops_b200_decl_strided_stencil(int dims, int points, const int *stencil, const int *stride, const char *name) {
+  return guarded([&] {
+    if (!stencil) throw opsb::Error(opsb::E_ARG, "stencil offsets required");
+    return rt().decl_stencil(dims, points, stencil, stride, name);
+  });
+}
+
+int ops_b200_decl_reduction_handle(int size, const char *type, const char *name) {
+  return guarded([&] { return rt().decl_reduction(size, type, name); });
+}
+
+int ops_b200_decl_const(const char *name, int dim, const char *type, const void *data) {
+  return guarded([&] {
+    if (!name || !data) throw opsb::Error(opsb::E_ARG, "constant name and data required");
+    rt().decl_const(name, dim, type, data);
+    return 0;
+  });
+}
+
+int ops_b200_update_const(const char *name, int dim, const char *type, const void *data) {
+  return ops_b200_decl_const(name, dim, type, data);
+}
+
+int ops_b200_par_loop(const char *kernel, const char *name, int block, int dim, const int *range, int nargs,
+                      const ops_b200_arg *args) {
+  return guarded([&] {
+    if (!kernel || !range || (nargs > 0 && !args)) throw opsb::Error(opsb::E_ARG, "kernel, range and args required");
+    const opsb::LoopInfo *li = opsb::Runtime::find_loop(kernel);
+    if (!li) throw opsb::Error(opsb::E_NOTFOUND, std::string("no registered loop kernel named ") + kernel);
+    std::vector<opsb::Arg> a = convert_args(nargs, args);
+    rt().par_loop(li, name, block, dim, range, a.data(), (int)a.size());
+    return 0;
+  });
+}
+
+int ops_b200_has_kernel(const char *kernel) { return kernel && opsb::Runtime::find_loop(kernel) ? 1 : 0; }
+
+int ops_b200_execute(void) {
+  return guarded([&] {
+    rt().execute();
+    return 0;
+  });
+}
+
+int ops_b200_reduction_result(int handle, void *out) {
+  return guarded([&] {
+    if (!out) throw opsb::Error(opsb::E_ARG, "output pointer required");
+    rt().reduction_result(handle, out);
+    return 0;
+  });
+}
+
+int ops_b200_dat_set_data(int dat, const void *data, size_t bytes) {
+  return guarded([&] {
+    if (!data) throw opsb::Error(opsb::E_ARG, "data pointer required");
+    rt().dat_set_data(dat, data, bytes);
+    return 0;
+  });
+}
+
+int ops_b200_dat_fetch_data(int dat, void *data, size_t bytes) {
+  return guarded([&] {
+    if (!data) throw opsb::Error(opsb::E_ARG, "data pointer required");
+    rt().dat_fetch_data(dat, data, bytes);
+    return 0;
+  });
+}
+
+int ops_b200_dat_get_extents(int dat, int *disp, int *size) {
+  return guarded([&] {
+    rt().dat_get_extents(dat, disp, size);
+    return 0;
+  });
+}
+
+int ops_b200_dat_get_raw_pointer(int dat, int memspace, void **ptr, int *stride) {
+  return guarded([&] {
+    if (!ptr) throw opsb::Error(opsb::E_ARG, "ptr required");
+    if (memspace != OPS_B200_HOST && memspace != OPS_B200_DEVICE) throw opsb::Error(opsb::E_ARG, "bad memspace");
+    *ptr = rt().dat_get_raw_pointer(dat, memspace, stride);
+    return 0;
+  });
+}
+
+int ops_b200_dat_release_raw_data(int dat, int acc) {
+  return guarded([&] {
+    rt().dat_release_raw_data(dat, acc);
+    return 0;
+  });
+}
+
+int ops_b200_set_option(const char *name, int value) {
+  return guarded([&] {
+    std::string n = name ? name : "";
+    if (n == "graphs") rt().set_graphs(value);
+    else if (n == "fusion") rt().set_fusion(value);
+    else throw opsb::Error(opsb::E_ARG, "unknown option " + n);
+    return 0;
+  });
+}
+
+int ops_b200_counters(long long *kernels, long long *graphs, long long *loops) {
+  return guarded([&] {
+    opsb::Runtime &r = rt();
+    if (kernels) *kernels = r.kernels_launched();
+    if (graphs) *graphs = r.graphs_launched();
+    if (loops) *loops = r.loops_enqueued();
+    return 0;
+  });
+}
+
+int ops_b200_reset_counters(void) {
+  return guarded([&] {
+    rt().reset_counters();
+    return 0;
+  });
+}
+
+int ops_b200_set_kernel_timing(int on) {
+  return guarded([&] {
+    rt().set_timing(on);
+    return 0;
+  });
+}
+
+int ops_b200_kernel_time(const char *kernel, long long *launches, double *total_ms) {
+  return guarded([&] {
+    const auto &m = rt().kernel_times();
+    auto it = m.find(kernel ? kernel : "");
+    if (launches) *launches = it == m.end() ? 0 : it->second.launches;
+    if (total_ms) *total_ms = it == m.end() ? 0.0 : it->second.ms;
+    return 0;
+  });
+}
+
+int ops_b200_clear_kernel_timing(void) {
+  return guarded([&] {
+    rt().clear_timing();
+    return 0;
+  });
+}
+
+}  // extern "C"
+
+// App entry points are defined next to their drivers (apps_*.cpp) and use
+// this helper to share the error path.
+namespace opsb {
+int capi_guard(const std::function<int()> &f) { return guarded(f); }
+}  // namespace opsb

@@ -1,0 +1,337 @@
+// Device-side building blocks of the OPS-B200 loop backend.
+//
+// An OPS parallel loop (ops_par_loop, ops/c/include/ops_seq_v2.h:225-292 is
+// the semantic reference) applies a per-point kernel over an index range;
+// the kernel reaches neighbouring points of each dat through an accessor
+// (ACC<T>, ops/c/include/ops_lib_core.h:1357-2038) and receives global
+// arguments (ops_arg_gbl), reduction targets (ops_arg_reduce) and the
+// point's index (ops_arg_idx) through plain pointers.
+//
+// Here each loop kernel is a functor with a __device__ operator() taking the
+// same parameter list as the OPS kernel; ACC2/ACC3 play the role of ACC<T>.
+// exec_loop<K> (below) turns the functor into a grid: x is the fastest,
+// coalesced dimension, each thread walks several rows, reductions are folded
+// per thread, per warp (shuffles), per block (shared memory) and finally
+// across blocks by the last block to finish, in a fixed order, so results do
+// not depend on scheduling.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <float.h>
+#include <limits.h>
+#include <utility>
+#include <type_traits>
+
+#define OPSB_MAX_ARGS 24
+#define OPSB_MAX_RED_DIM 12
+#define OPSB_MAX_REDUCE_ARGS 8
+
+namespace opsb {
+
+enum ArgKind { ARG_GBL = 0, ARG_DAT = 1, ARG_IDX = 2, ARG_REDUCE = 3 };
+// Access modes keep the reference's numbering (ops/c/include/ops_lib_core.h:84-89).
+enum Access { ACC_READ = 0, ACC_WRITE = 1, ACC_RW = 2, ACC_INC = 3, ACC_MIN = 4, ACC_MAX = 5 };
+
+// The reference's min/max/sign macros (ops/c/include/ops_lib_core.h:559-571),
+// restated as functions with the same comparison order so that ties, signed
+// zeros and NaNs resolve exactly as on the CPU.
+template <class T> __host__ __device__ __forceinline__ T op_min(T a, T b) { return (a < b) ? a : b; }
+template <class T> __host__ __device__ __forceinline__ T op_max(T a, T b) { return (a > b) ? a : b; }
+__host__ __device__ __forceinline__ double op_sign(double a, double b) { return (b < 0.0) ? (a * (-1)) : a; }
+
+// 2D accessor: p points at the current point; (i, j) is a stencil offset.
+template <class T>
+struct ACC2 {
+  T *p;
+  int sx, sy;
+  ACC2() = default;
+  __device__ __forceinline__ ACC2(T *p_, int sx_, int sy_) : p(p_), sx(sx_), sy(sy_) {}
+  __device__ __forceinline__ T &operator()(int i, int j) const { return p[i * sx + j * sy]; }
+};
+
+// 3D accessor.
+template <class T>
+struct ACC3 {
+  T *p;
+  int sx, sy, sz;
+  ACC3() = default;
+  __device__ __forceinline__ ACC3(T *p_, int sx_, int sy_, int sz_) : p(p_), sx(sx_), sy(sy_), sz(sz_) {}
+  __device__ __forceinline__ T &operator()(int i, int j, int k) const {
+    return p[i * sx + (long long)j * sy + (long long)k * sz];
+  }
+};
+
+// One loop argument as the device sees it.
+struct ArgView {
+  char *ptr;        // DAT: logical origin of the dat; GBL: device copy; REDUCE: handle slot
+  int sx, sy, sz;   // element strides (0 along a dimension the stencil does not stride)
+  int kind;         // ArgKind
+  int acc;          // Access
+  int dim;          // components (reduction width for REDUCE)
+  int red_index;    // REDUCE: index among this loop's reduction args
+  int first;        // REDUCE: 1 when the handle starts from the identity in this loop
+  int pad_;
+};
+
+struct LoopParams {
+  int start[3], end[3];
+  int ndim;
+  int nargs;
+  int nred;           // number of REDUCE args
+  int rows_per_iter;  // unused by exec_loop, kept for fused kernels
+  char *red_scratch;  // per-block partials: [red_index][block][OPSB_MAX_RED_DIM] x 8 bytes
+  unsigned int *red_counter;  // blocks-done counter, reset to 0 by the last block
+  ArgView a[OPSB_MAX_ARGS];
+};
+
+// ----------------------------------------------------------------------------
+// Reduction identities and combine, by element type and access mode
+// (zero / +max / -max as ops/c/include/ops_internal2.h:67-97 defines them).
+// ----------------------------------------------------------------------------
+template <class T> struct RedTraits;
+template <> struct RedTraits<double> { __device__ static double big() { return DBL_MAX; } };
+template <> struct RedTraits<float> { __device__ static float big() { return FLT_MAX; } };
+template <> struct RedTraits<int> { __device__ static int big() { return INT_MAX; } };
+template <> struct RedTraits<long long> { __device__ static long long big() { return LLONG_MAX; } };
+
+template <class T>
+__device__ __forceinline__ T red_identity(int acc) {
+  if (acc == ACC_MIN) return RedTraits<T>::big();
+  if (acc == ACC_MAX) return -RedTraits<T>::big();
+  return T(0);
+}
+template <class T>
+__device__ __forceinline__ T red_combine(int acc, T a, T b) {
+  if (acc == ACC_MIN) return op_min(a, b);
+  if (acc == ACC_MAX) return op_max(a, b);
+  return a + b;
+}
+
+template <class T>
+__device__ __forceinline__ T shfl_down(T v, int o) { return __shfl_down_sync(0xffffffffu, v, o); }
+
+// Block-wide reduction of one value; result valid in thread 0.
+// smem must hold one T per warp.
+template <class T>
+__device__ __forceinline__ T block_reduce(T v, int acc, T *smem) {
+  const int lane = threadIdx.x & 31;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int warp = tid >> 5;
+  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = red_combine(acc, v, shfl_down(v, o));
+  __syncthreads();
+  if (lane == 0) smem[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = (lane < nwarps) ? smem[lane] : red_identity<T>(acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = red_combine(acc, v, shfl_down(v, o));
+  }
+  return v;
+}
+
+// ----------------------------------------------------------------------------
+// Per-parameter storage: how each kernel parameter is produced from an arg.
+// ----------------------------------------------------------------------------
+template <class P> struct Slot;
+
+template <class T>
+struct Slot<ACC2<T>> {
+  ACC2<T> acc;
+  __device__ __forceinline__ void init(const ArgView &) {}
+  __device__ __forceinline__ ACC2<T> &at(const ArgView &a, int x, int y, int) {
+    acc = ACC2<T>(reinterpret_cast<T *>(a.ptr) + (long long)x * a.sx + (long long)y * a.sy, a.sx, a.sy);
+    return acc;
+  }
+  template <class S> __device__ __forceinline__ void finish(const ArgView &, const LoopParams &, S *, int) {}
+};
+
+template <class T>
+struct Slot<ACC3<T>> {
+  ACC3<T> acc;
+  __device__ __forceinline__ void init(const ArgView &) {}
+  __device__ __forceinline__ ACC3<T> &at(const ArgView &a, int x, int y, int z) {
+    acc = ACC3<T>(reinterpret_cast<T *>(a.ptr) + (long long)x * a.sx + (long long)y * a.sy + (long long)z * a.sz,
+                  a.sx, a.sy, a.sz);
+    return acc;
+  }
+  template <class S> __device__ __forceinline__ void finish(const ArgView &, const LoopParams &, S *, int) {}
+};
+
+// Non-const pointer: a reduction target (thread-local accumulator), the
+// point's index (int only) or a read-write global.
+template <class T>
+struct Slot<T *> {
+  T red[OPSB_MAX_RED_DIM];
+  int idx[3];
+  __device__ __forceinline__ void init(const ArgView &a) {
+    if (a.kind == ARG_REDUCE) {
+      for (int d = 0; d < OPSB_MAX_RED_DIM; d++) red[d] = red_identity<T>(a.acc);
+    }
+  }
+  __device__ __forceinline__ T *at(const ArgView &a, int x, int y, int z) {
+    if (a.kind == ARG_REDUCE) return red;
+    if (a.kind == ARG_IDX) {
+      idx[0] = x; idx[1] = y; idx[2] = z;
+      return reinterpret_cast<T *>(idx);
+    }
+    return reinterpret_cast<T *>(a.ptr);
+  }
+  // Fold this thread's partial into the block's, then across blocks.
+  __device__ void finish(const ArgView &a, const LoopParams &lp, T *smem, int nblocks) {
+    if (a.kind != ARG_REDUCE) return;
+    const int bid = blockIdx.x + blockIdx.y * gridDim.x;
+    T *part = reinterpret_cast<T *>(lp.red_scratch) +
+              ((size_t)a.red_index * nblocks + bid) * OPSB_MAX_RED_DIM;
+    for (int d = 0; d < a.dim; d++) {
+      T v = block_reduce<T>(red[d], a.acc, smem);
+      if (threadIdx.x == 0 && threadIdx.y == 0) part[d] = v;
+    }
+  }
+};
+
+template <class T>
+struct Slot<const T *> {
+  int idx[3];
+  __device__ __forceinline__ void init(const ArgView &) {}
+  __device__ __forceinline__ const T *at(const ArgView &a, int x, int y, int z) {
+    if (a.kind == ARG_IDX) {
+      idx[0] = x; idx[1] = y; idx[2] = z;
+      return reinterpret_cast<const T *>(idx);
+    }
+    return reinterpret_cast<const T *>(a.ptr);
+  }
+  template <class S> __device__ __forceinline__ void finish(const ArgView &, const LoopParams &, S *, int) {}
+};
+
+// Minimal tuple of slots (device code, no std::tuple).
+template <size_t I, class T> struct Leaf { T v; };
+template <class Seq, class... T> struct SlotTuple;
+template <size_t... I, class... T>
+struct SlotTuple<std::index_sequence<I...>, T...> : Leaf<I, T>... {};
+template <size_t I, class T> __device__ __forceinline__ T &get_leaf(Leaf<I, T> &l) { return l.v; }
+
+// Reduction element type of a parameter (void when it cannot reduce).
+template <class P> struct RedElem { using type = void; };
+template <class T> struct RedElem<T *> { using type = T; };
+
+// Combine the per-block partials of every reduction arg (last block only).
+template <class T>
+__device__ void finish_grid_reduction(const ArgView &a, const LoopParams &lp, int nblocks, T *smem) {
+  T *part = reinterpret_cast<T *>(lp.red_scratch) + (size_t)a.red_index * nblocks * OPSB_MAX_RED_DIM;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nthr = blockDim.x * blockDim.y;
+  T *slot = reinterpret_cast<T *>(a.ptr);
+  for (int d = 0; d < a.dim; d++) {
+    T v = red_identity<T>(a.acc);
+    for (int b = tid; b < nblocks; b += nthr) v = red_combine(a.acc, v, part[(size_t)b * OPSB_MAX_RED_DIM + d]);
+    v = block_reduce<T>(v, a.acc, smem);
+    if (tid == 0) slot[d] = a.first ? v : red_combine(a.acc, slot[d], v);
+  }
+}
+
+template <class K, class Sig> struct Exec;
+
+template <class K, class... P>
+struct Exec<K, void (K::*)(P...) const> {
+  using Seq = std::index_sequence_for<P...>;
+  using Tup = SlotTuple<Seq, Slot<std::decay_t<P>>...>;
+
+  template <size_t... I>
+  __device__ static __forceinline__ void init_all(Tup &t, const LoopParams &lp, std::index_sequence<I...>) {
+    (get_leaf<I, Slot<std::decay_t<P>>>(t).init(lp.a[I]), ...);
+  }
+  template <size_t... I>
+  __device__ static __forceinline__ void call(const K &k, Tup &t, const LoopParams &lp, int x, int y, int z,
+                                              std::index_sequence<I...>) {
+    k(get_leaf<I, Slot<std::decay_t<P>>>(t).at(lp.a[I], x, y, z)...);
+  }
+  template <size_t... I>
+  __device__ static __forceinline__ void finish_all(Tup &t, const LoopParams &lp, double *smem, int nblocks,
+                                                    std::index_sequence<I...>) {
+    (finish_one<I>(t, lp, smem, nblocks), ...);
+  }
+  template <size_t I>
+  __device__ static __forceinline__ void finish_one(Tup &t, const LoopParams &lp, double *smem, int nblocks) {
+    using PT = std::decay_t<std::tuple_element_t<I, std::tuple<P...>>>;
+    using RT = typename RedElem<PT>::type;
+    if constexpr (!std::is_void<RT>::value && !std::is_const<RT>::value) {
+      get_leaf<I, Slot<PT>>(t).finish(lp.a[I], lp, reinterpret_cast<RT *>(smem), nblocks);
+    }
+  }
+  template <size_t... I>
+  __device__ static __forceinline__ void grid_finish_all(const LoopParams &lp, double *smem, int nblocks,
+                                                         std::index_sequence<I...>) {
+    (grid_finish_one<I>(lp, smem, nblocks), ...);
+  }
+  template <size_t I>
+  __device__ static __forceinline__ void grid_finish_one(const LoopParams &lp, double *smem, int nblocks) {
+    using PT = std::decay_t<std::tuple_element_t<I, std::tuple<P...>>>;
+    using RT = typename RedElem<PT>::type;
+    if constexpr (!std::is_void<RT>::value && !std::is_const<RT>::value) {
+      if (lp.a[I].kind == ARG_REDUCE) finish_grid_reduction<RT>(lp.a[I], lp, nblocks, reinterpret_cast<RT *>(smem));
+    }
+  }
+};
+
+// The generic loop kernel. blockDim = (BX, BY); blocks tile x exactly and
+// stride over the remaining (y, z) rows.
+template <class K>
+__global__ void __launch_bounds__(256) exec_loop(const __grid_constant__ LoopParams lp) {
+  using E = Exec<K, decltype(&K::operator())>;
+  typename E::Tup t;
+  E::init_all(t, lp, typename E::Seq{});
+  const K k{};
+  const int x = lp.start[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int ny = lp.end[1] - lp.start[1];
+  const int nz = lp.end[2] - lp.start[2];
+  const long long nrows = (long long)ny * nz;
+  if (x < lp.end[0]) {
+    for (long long r = (long long)blockIdx.y * blockDim.y + threadIdx.y; r < nrows;
+         r += (long long)gridDim.y * blockDim.y) {
+      const int y = lp.start[1] + (int)(r % ny);
+      const int z = lp.start[2] + (int)(r / ny);
+      E::call(k, t, lp, x, y, z, typename E::Seq{});
+    }
+  }
+  if (lp.nred == 0) return;
+  __shared__ double smem[32];
+  const int nblocks = gridDim.x * gridDim.y;
+  E::finish_all(t, lp, smem, nblocks, typename E::Seq{});
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    __threadfence();
+    unsigned int done = atomicAdd(lp.red_counter, 1u);
+    last = (done == (unsigned int)(nblocks - 1));
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  E::grid_finish_all(lp, smem, nblocks, typename E::Seq{});
+  if (threadIdx.x == 0 && threadIdx.y == 0) *lp.red_counter = 0u;
+}
+
+// Host-side description of a kernel's parameter list, used to validate args
+// at enqueue time: 'A' accessor, 'p' non-const pointer, 'c' const pointer;
+// elem is the element size in bytes.
+struct ParamInfo { char cls; int elem; int ndim; };
+
+template <class P> struct ParamDesc;
+template <class T> struct ParamDesc<ACC2<T>> { static ParamInfo get() { return {'A', (int)sizeof(T), 2}; } };
+template <class T> struct ParamDesc<ACC3<T>> { static ParamInfo get() { return {'A', (int)sizeof(T), 3}; } };
+template <class T> struct ParamDesc<T *> { static ParamInfo get() { return {'p', (int)sizeof(T), 0}; } };
+template <class T> struct ParamDesc<const T *> { static ParamInfo get() { return {'c', (int)sizeof(T), 0}; } };
+
+template <class Sig> struct SigInfo;
+template <class K, class... P>
+struct SigInfo<void (K::*)(P...) const> {
+  static constexpr int n = sizeof...(P);
+  static void fill(ParamInfo *out) {
+    ParamInfo tmp[] = {ParamDesc<std::decay_t<P>>::get()..., ParamInfo{0, 0, 0}};
+    for (int i = 0; i < (int)sizeof...(P); i++) out[i] = tmp[i];
+  }
+};
+
+}  // namespace opsb

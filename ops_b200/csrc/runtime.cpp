@@ -1,0 +1,670 @@
+// OPS-B200 host runtime (see runtime.h for the reference mapping).
+#include "runtime.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <sstream>
+
+namespace opsb {
+
+void cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    std::ostringstream os;
+    os << "CUDA error " << cudaGetErrorName(e) << " (" << cudaGetErrorString(e) << ") in " << what;
+    throw Error(E_CUDA, os.str());
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Registries (populated at static-initialisation time by the kernel modules).
+// ---------------------------------------------------------------------------
+namespace {
+struct Registry {
+  std::map<std::string, std::unique_ptr<LoopInfo>> loops;
+  struct ConstSlot { const void *symbol; size_t offset, bytes; };
+  std::multimap<std::string, ConstSlot> consts;
+  std::vector<ChainRule> chains;
+};
+Registry &registry() {
+  static Registry r;
+  return r;
+}
+Runtime *g_runtime = nullptr;
+
+inline uint64_t mix64(uint64_t h, uint64_t v) {
+  // FNV-1a style fold of 64-bit words.
+  h ^= v + 0x9E3779B97F4A7C15ULL + (h << 6) + (h >> 2);
+  return h * 0x100000001B3ULL;
+}
+
+constexpr size_t kGblCap = 1 << 20;
+}  // namespace
+
+void Runtime::register_loop(const LoopInfo &info) {
+  registry().loops[info.kernel] = std::make_unique<LoopInfo>(info);
+}
+const LoopInfo *Runtime::find_loop(const std::string &kernel) {
+  auto &m = registry().loops;
+  auto it = m.find(kernel);
+  return it == m.end() ? nullptr : it->second.get();
+}
+void Runtime::register_const(const std::string &name, const void *symbol, size_t offset, size_t bytes) {
+  registry().consts.insert({name, {symbol, offset, bytes}});
+}
+void Runtime::register_chain(const ChainRule &rule) { registry().chains.push_back(rule); }
+
+Runtime &Runtime::get() {
+  if (!g_runtime) g_runtime = new Runtime();
+  return *g_runtime;
+}
+bool Runtime::exists() { return g_runtime != nullptr && g_runtime->inited_; }
+void Runtime::destroy() {
+  delete g_runtime;
+  g_runtime = nullptr;
+}
+
+Runtime::~Runtime() {
+  if (!inited_) return;
+  cudaStreamSynchronize(stream_);
+  for (auto &p : pending_) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  for (auto e : event_pool_) cudaEventDestroy(e);
+  for (auto &kv : graphs_)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  for (auto &d : dats_)
+    if (d && d->data_d) cudaFree(d->data_d);
+  for (auto &r : reductions_)
+    if (r.slot_d) cudaFree(r.slot_d);
+  if (gbl_dev_) cudaFree(gbl_dev_);
+  if (red_scratch_) cudaFree(red_scratch_);
+  if (red_counters_) cudaFree(red_counters_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Runtime::init(int device, int diags) {
+  if (inited_) return;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    throw Error(E_CUDA, "ops_b200: no CUDA device available (the B200 backend has no CPU path)");
+  if (device < 0 || device >= n) throw Error(E_ARG, "ops_b200: device index out of range");
+  device_ = device;
+  diags_ = diags;
+  OPSB_CUDA(cudaSetDevice(device_));
+  OPSB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  OPSB_CUDA(cudaMalloc(&gbl_dev_, kGblCap));
+  gbl_host_.resize(kGblCap);
+  gbl_cap_ = kGblCap;
+  size_t scratch = (size_t)OPSB_MAX_REDUCE_ARGS * kMaxRedBlocks * OPSB_MAX_RED_DIM * sizeof(double);
+  OPSB_CUDA(cudaMalloc(&red_scratch_, scratch));
+  OPSB_CUDA(cudaMalloc(&red_counters_, kNumCounters * sizeof(unsigned int)));
+  OPSB_CUDA(cudaMemset(red_counters_, 0, kNumCounters * sizeof(unsigned int)));
+  const char *g = getenv("OPS_B200_GRAPHS");
+  if (g) graphs_on_ = atoi(g);
+  const char *f = getenv("OPS_B200_FUSION");
+  if (f) fusion_on_ = atoi(f);
+  inited_ = true;
+}
+
+static void require(bool cond, int code, const std::string &msg) {
+  if (!cond) throw Error(code, msg);
+}
+
+Dat &Runtime::dat(int i) {
+  require(i >= 0 && i < (int)dats_.size() && dats_[i], E_ARG, "invalid dat handle " + std::to_string(i));
+  return *dats_[i];
+}
+Stencil &Runtime::stencil(int i) {
+  require(i >= 0 && i < (int)stencils_.size(), E_ARG, "invalid stencil handle " + std::to_string(i));
+  return stencils_[i];
+}
+Reduction &Runtime::reduction(int i) {
+  require(i >= 0 && i < (int)reductions_.size(), E_ARG, "invalid reduction handle " + std::to_string(i));
+  return reductions_[i];
+}
+Block &Runtime::block(int i) {
+  require(i >= 0 && i < (int)blocks_.size(), E_ARG, "invalid block handle " + std::to_string(i));
+  return blocks_[i];
+}
+
+int Runtime::decl_block(int dims, const char *name) {
+  require(inited_, E_STATE, "ops_decl_block before ops_init");
+  require(dims >= 1 && dims <= 3, E_UNSUPPORTED, "blocks of 1 to 3 dimensions are supported");
+  Block b;
+  b.index = (int)blocks_.size();
+  b.dims = dims;
+  b.name = name ? name : "";
+  blocks_.push_back(b);
+  return b.index;
+}
+
+static int type_size_of(const char *type) {
+  std::string t = type ? type : "";
+  if (t == "double" || t == "long" || t == "long long" || t == "ll") return 8;
+  if (t == "float" || t == "int" || t == "unsigned int") return 4;
+  if (t == "short" || t == "half") return 2;
+  if (t == "char") return 1;
+  return 0;
+}
+
+int Runtime::decl_dat(int blk, int dim, const int *size, const int *base, const int *d_m, const int *d_p,
+                      const void *data, int type_size, const char *type, const char *name) {
+  require(inited_, E_STATE, "ops_decl_dat before ops_init");
+  Block &b = block(blk);
+  require(dim >= 1, E_ARG, "dat dim must be >= 1");
+  int ts = type_size > 0 ? type_size : type_size_of(type);
+  require(ts > 0, E_ARG, std::string("unknown dat type ") + (type ? type : "(null)"));
+  auto d = std::make_unique<Dat>();
+  d->index = (int)dats_.size();
+  d->block = blk;
+  d->dim = dim;
+  d->type_size = ts;
+  d->elem_size = ts * dim;
+  d->type = type ? type : "";
+  d->name = name ? name : "";
+  for (int i = 0; i < 3; i++) {
+    if (i < b.dims) {
+      require(d_m[i] <= 0 && d_p[i] >= 0, E_ARG, "halo depths must satisfy d_m <= 0 <= d_p");
+      require(size[i] >= 0, E_ARG, "negative dat size");
+      d->base[i] = base ? base[i] : 0;
+      d->d_m[i] = d_m[i];
+      d->d_p[i] = d_p[i];
+      // ops_dat_init_metadata_core (ops/c/src/core/ops_lib_core.cpp:469-474)
+      d->size[i] = size[i] - d_m[i] + d_p[i];
+    } else {
+      d->size[i] = 1;
+    }
+  }
+  // Logical index 0 of x starts on a 64-byte boundary; rows are 128-byte pitched.
+  const int e = d->elem_size;
+  int lead = -d->d_m[0] + d->base[0] * 0;  // columns before logical x = 0
+  int align_elems = (e <= 64 && 64 % e == 0) ? 64 / e : 1;
+  d->pad_front = (align_elems - (lead % align_elems)) % align_elems;
+  int row_align = (e <= 128 && 128 % e == 0) ? 128 / e : 1;
+  d->pitch = ((long long)(d->pad_front + d->size[0]) + row_align - 1) / row_align * row_align;
+  d->plane = d->pitch * d->size[1];
+  d->origin = d->pad_front + (long long)(-d->base[0] - d->d_m[0]) + (long long)(-d->base[1] - d->d_m[1]) * d->pitch +
+              (long long)(-d->base[2] - d->d_m[2]) * d->plane;
+  d->bytes = (size_t)d->plane * d->size[2] * e;
+  OPSB_CUDA(cudaMalloc(&d->data_d, d->bytes > 0 ? d->bytes : 256));
+  OPSB_CUDA(cudaMemsetAsync(d->data_d, 0, d->bytes, stream_));
+  int idx = d->index;
+  dats_.push_back(std::move(d));
+  if (data) {
+    const Dat &dd = *dats_[idx];
+    dat_set_data(idx, data, (size_t)dd.size[0] * dd.size[1] * dd.size[2] * dd.elem_size);
+  }
+  OPSB_CUDA(cudaStreamSynchronize(stream_));
+  return idx;
+}
+
+int Runtime::decl_stencil(int dims, int points, const int *offs, const int *stride, const char *name) {
+  require(inited_, E_STATE, "ops_decl_stencil before ops_init");
+  require(dims >= 1 && dims <= 3 && points >= 1, E_ARG, "bad stencil shape");
+  Stencil s;
+  s.index = (int)stencils_.size();
+  s.dims = dims;
+  s.points = points;
+  s.offs.assign(offs, offs + (size_t)dims * points);
+  for (int i = 0; i < 3; i++) s.stride[i] = (stride && i < dims) ? stride[i] : 1;
+  s.name = name ? name : "";
+  stencils_.push_back(s);
+  return s.index;
+}
+
+int Runtime::decl_reduction(int size, const char *type, const char *name) {
+  require(inited_, E_STATE, "ops_decl_reduction_handle before ops_init");
+  require(size > 0, E_ARG, "reduction size must be positive");
+  Reduction r;
+  r.index = (int)reductions_.size();
+  r.size = size;
+  r.type = type ? type : "double";
+  r.elem = type_size_of(r.type.c_str());
+  require(r.elem > 0, E_ARG, "unknown reduction type " + r.type);
+  r.name = name ? name : "";
+  OPSB_CUDA(cudaMalloc(&r.slot_d, std::max(size, 64)));
+  OPSB_CUDA(cudaMemset(r.slot_d, 0, std::max(size, 64)));
+  reductions_.push_back(r);
+  return r.index;
+}
+
+void Runtime::decl_const(const char *name, int dim, const char *type, const void *data) {
+  require(inited_, E_STATE, "ops_decl_const before ops_init");
+  execute();  // ops_update_const flushes the queue first (ops_lazy.cpp semantics)
+  auto range = registry().consts.equal_range(name ? name : "");
+  int ts = type_size_of(type);
+  bool any = false;
+  for (auto it = range.first; it != range.second; ++it) {
+    // Struct-typed constants (e.g. CloverLeaf's field_type) have no scalar
+    // type size; the registered slot size is used then.
+    size_t bytes = ts > 0 ? (size_t)ts * dim : it->second.bytes;
+    bytes = std::min(bytes, it->second.bytes);
+    OPSB_CUDA(cudaMemcpyToSymbolAsync(it->second.symbol, data, bytes, it->second.offset, cudaMemcpyHostToDevice,
+                                      stream_));
+    any = true;
+  }
+  if (any) OPSB_CUDA(cudaStreamSynchronize(stream_));
+}
+
+// ---------------------------------------------------------------------------
+// Loop enqueue (create_kerneldesc_and_enque, ops/c/src/core/ops_lazy.cpp:1403).
+// ---------------------------------------------------------------------------
+void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim, const int *range,
+                       const Arg *args, int nargs) {
+  require(inited_, E_STATE, "ops_par_loop before ops_init");
+  require(loop != nullptr, E_NOTFOUND, "unknown loop kernel");
+  Block &b = block(blk);
+  require(dim == b.dims, E_ARG, "ops_par_loop dim does not match the block");
+  require(nargs == loop->nparams, E_ARG,
+          "loop " + loop->kernel + " takes " + std::to_string(loop->nparams) + " args, got " + std::to_string(nargs));
+  require(nargs <= OPSB_MAX_ARGS, E_ARG, "too many loop args");
+  Desc d;
+  d.loop = loop;
+  d.name = name ? name : loop->kernel;
+  d.block = blk;
+  d.dim = dim;
+  for (int i = 0; i < 3; i++) {
+    d.range[2 * i] = i < dim ? range[2 * i] : 0;
+    d.range[2 * i + 1] = i < dim ? range[2 * i + 1] : 1;
+  }
+  d.args.assign(args, args + nargs);
+  d.red_first.assign(nargs, 0);
+  d.gbl_off.assign(nargs, 0);
+  int nred = 0;
+  for (int i = 0; i < nargs; i++) {
+    Arg &a = d.args[i];
+    const ParamInfo &p = loop->params[i];
+    switch (a.kind) {
+      case ARG_DAT: {
+        Dat &dt = dat(a.dat);
+        stencil(a.stencil);
+        require(p.cls == 'A', E_ARG, "loop " + loop->kernel + ": arg " + std::to_string(i) + " is a dat but the kernel expects a pointer");
+        require(p.elem == dt.type_size, E_ARG, "loop " + loop->kernel + ": dat " + dt.name + " element size mismatch");
+        require(dt.block == blk, E_ARG, "dat " + dt.name + " is declared on another block");
+        require(dt.locked == 0, E_STATE, "dat " + dt.name + " is used in a loop while its raw pointer is held (ops_lib_core.cpp:2321)");
+        if (a.acc != ACC_READ) dt.host.clear();
+        break;
+      }
+      case ARG_GBL:
+        require(p.cls == 'c' || p.cls == 'p', E_ARG, "loop " + loop->kernel + ": arg " + std::to_string(i) + " is a global but the kernel expects an accessor");
+        require(a.gbl.size() <= 4096, E_ARG, "global argument larger than 4 KiB");
+        break;
+      case ARG_REDUCE: {
+        Reduction &r = reduction(a.red);
+        require(p.cls == 'p', E_ARG, "loop " + loop->kernel + ": reduction arg must bind to a non-const pointer");
+        require(p.elem == r.elem, E_ARG, "reduction " + r.name + " type does not match the kernel parameter");
+        require(a.dim <= OPSB_MAX_RED_DIM && a.dim * r.elem <= r.size, E_ARG, "reduction " + r.name + " too wide");
+        require(nred < OPSB_MAX_REDUCE_ARGS, E_ARG, "too many reductions in one loop");
+        require(a.acc == ACC_INC || a.acc == ACC_MIN || a.acc == ACC_MAX, E_ARG, "reduction access must be INC, MIN or MAX");
+        // ops_arg_reduce_core (ops/c/src/core/ops_lib_core.cpp:856): the first use after a result restarts.
+        d.red_first[i] = r.initialized ? 0 : 1;
+        r.initialized = 1;
+        r.acc = a.acc;
+        a.elem = r.elem;
+        nred++;
+        break;
+      }
+      case ARG_IDX:
+        require(p.elem == 4 && p.cls != 'A', E_ARG, "ops_arg_idx must bind to an int pointer");
+        break;
+      default:
+        throw Error(E_ARG, "unknown arg kind");
+    }
+  }
+  queue_.push_back(std::move(d));
+  loops_enqueued_++;
+  if (queue_.size() >= 4096) execute();
+}
+
+void Runtime::launch_shape(const int *range, int dim, bool reduces, dim3 &grid, dim3 &block) {
+  (void)dim;
+  long long nx = std::max(0, range[1] - range[0]);
+  long long ny = std::max(0, range[3] - range[2]);
+  long long nz = std::max(0, range[5] - range[4]);
+  long long nrows = ny * nz;
+  int bx = nx >= 128 ? 128 : (nx >= 64 ? 64 : 32);
+  int by = 256 / bx;
+  long long gx = std::max(1LL, (nx + bx - 1) / bx);
+  long long target = 148LL * 16;
+  long long gy = std::max(1LL, std::min((nrows + by - 1) / by, std::max(1LL, target / gx)));
+  gy = std::min(gy, 65535LL);
+  if (reduces) {
+    while (gx * gy > kMaxRedBlocks && gy > 1) gy = (gy + 1) / 2;
+    if (gx * gy > kMaxRedBlocks) throw Error(E_UNSUPPORTED, "reduction loop too wide");
+  }
+  grid = dim3((unsigned)gx, (unsigned)gy, 1);
+  block = dim3(bx, by, 1);
+}
+
+void Runtime::build_params(const Desc &d, LoopParams &lp, int *nred_out) {
+  memset(&lp, 0, sizeof(lp));
+  for (int i = 0; i < 3; i++) {
+    lp.start[i] = d.range[2 * i];
+    lp.end[i] = d.range[2 * i + 1];
+  }
+  lp.ndim = d.dim;
+  lp.nargs = (int)d.args.size();
+  int nred = 0;
+  for (int i = 0; i < lp.nargs; i++) {
+    const Arg &a = d.args[i];
+    ArgView &v = lp.a[i];
+    v.kind = a.kind;
+    v.acc = a.acc;
+    v.dim = a.dim;
+    switch (a.kind) {
+      case ARG_DAT: {
+        const Dat &dt = *dats_[a.dat];
+        const Stencil &st = stencils_[a.stencil];
+        v.ptr = a.opt ? dt.origin_ptr() : nullptr;
+        v.sx = st.stride[0] ? dt.dim : 0;
+        v.sy = st.stride[1] ? (int)(dt.pitch * dt.dim) : 0;
+        v.sz = st.stride[2] ? (int)(dt.plane * dt.dim) : 0;
+        break;
+      }
+      case ARG_GBL:
+        v.ptr = gbl_dev_ + d.gbl_off[i];
+        break;
+      case ARG_REDUCE:
+        v.ptr = reductions_[a.red].slot_d;
+        v.red_index = nred++;
+        v.first = d.red_first[i];
+        break;
+      default:
+        break;
+    }
+  }
+  lp.nred = nred;
+  lp.red_scratch = red_scratch_;
+  lp.red_counter = red_counters_;
+  if (nred_out) *nred_out = nred;
+}
+
+uint64_t Runtime::queue_key(const std::vector<Desc> &q) const {
+  uint64_t h = 0xCBF29CE484222325ULL;
+  for (const Desc &d : q) {
+    h = mix64(h, (uint64_t)(uintptr_t)d.loop);
+    for (int i = 0; i < 6; i++) h = mix64(h, (uint64_t)(uint32_t)d.range[i]);
+    for (size_t i = 0; i < d.args.size(); i++) {
+      const Arg &a = d.args[i];
+      h = mix64(h, ((uint64_t)a.kind << 56) ^ ((uint64_t)a.acc << 48) ^ ((uint64_t)a.opt << 40) ^
+                       ((uint64_t)(a.dim & 0xff) << 32) ^ (uint64_t)(uint32_t)a.stencil);
+      if (a.kind == ARG_DAT) h = mix64(h, (uint64_t)(uintptr_t)dats_[a.dat]->data_d);
+      if (a.kind == ARG_REDUCE) h = mix64(h, ((uint64_t)a.red << 1) | (uint64_t)d.red_first[i]);
+      if (a.kind == ARG_GBL) h = mix64(h, (uint64_t)d.gbl_off[i] ^ ((uint64_t)a.gbl.size() << 40));
+    }
+  }
+  return h;
+}
+
+void Runtime::set_timing(int on) {
+  collect_timing();
+  timing_on_ = on;
+}
+
+void Runtime::timed_launch_begin(const std::string &name) {
+  if (!timing_on_) return;
+  if (event_pool_.empty()) {
+    for (int i = 0; i < 64; i++) {
+      cudaEvent_t e;
+      OPSB_CUDA(cudaEventCreate(&e));
+      event_pool_.push_back(e);
+    }
+  }
+  cur_ev_ = event_pool_.back();
+  event_pool_.pop_back();
+  cur_name_ = name;
+  OPSB_CUDA(cudaEventRecord(cur_ev_, stream_));
+}
+
+void Runtime::timed_launch_end() {
+  if (!timing_on_ || !cur_ev_) return;
+  if (event_pool_.empty()) {
+    for (int i = 0; i < 64; i++) {
+      cudaEvent_t e;
+      OPSB_CUDA(cudaEventCreate(&e));
+      event_pool_.push_back(e);
+    }
+  }
+  cudaEvent_t e = event_pool_.back();
+  event_pool_.pop_back();
+  OPSB_CUDA(cudaEventRecord(e, stream_));
+  pending_.push_back({cur_name_, cur_ev_, e});
+  cur_ev_ = nullptr;
+  if (pending_.size() > 4096) collect_timing();
+}
+
+void Runtime::collect_timing() {
+  if (pending_.empty()) return;
+  OPSB_CUDA(cudaStreamSynchronize(stream_));
+  for (auto &p : pending_) {
+    float ms = 0.f;
+    OPSB_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+    KTime &k = ktimes_[p.name];
+    k.launches++;
+    k.ms += ms;
+    event_pool_.push_back(p.a);
+    event_pool_.push_back(p.b);
+  }
+  pending_.clear();
+}
+
+void Runtime::launch_items(std::vector<Desc> &q) {
+  auto &chains = registry().chains;
+  size_t i = 0;
+  while (i < q.size()) {
+    if (q[i].loop->internal) {
+      timed_launch_begin(q[i].loop->kernel);
+      launch_swap_outside(q[i], stream_);
+      timed_launch_end();
+      i++;
+      continue;
+    }
+    if (fusion_on_) {
+      bool fused = false;
+      for (auto &rule : chains) {
+        int n = rule.match(q, i);
+        if (n > 0) {
+          timed_launch_begin(rule.name);
+          rule.launch(q, i, n, stream_);
+          timed_launch_end();
+          i += n;
+          fused = true;
+          break;
+        }
+      }
+      if (fused) continue;
+    }
+    const Desc &d = q[i];
+    LoopParams lp;
+    int nred = 0;
+    build_params(d, lp, &nred);
+    lp.red_counter = red_counters_ + (i % kNumCounters);
+    dim3 g, b;
+    launch_shape(d.range, d.dim, nred > 0, g, b);
+    long long nx = (long long)d.range[1] - d.range[0];
+    long long nr = (long long)(d.range[3] - d.range[2]) * (d.range[5] - d.range[4]);
+    if ((nx > 0 && nr > 0) || nred > 0) {
+      timed_launch_begin(d.loop->kernel);
+      d.loop->launch(lp, g, b, stream_);
+      OPSB_CUDA(cudaGetLastError());
+      timed_launch_end();
+      kernels_launched_++;
+    }
+    i++;
+  }
+}
+
+void Runtime::run_queue(std::vector<Desc> &q) {
+  elide_copies(q);
+  // Stage the READ globals of the whole flush into the device arena.
+  gbl_used_ = 0;
+  for (Desc &d : q) {
+    for (size_t i = 0; i < d.args.size(); i++) {
+      const Arg &a = d.args[i];
+      if (a.kind != ARG_GBL) continue;
+      size_t off = (gbl_used_ + 15) & ~(size_t)15;
+      require(off + a.gbl.size() <= gbl_cap_, E_UNSUPPORTED, "global argument arena exhausted in one flush");
+      memcpy(gbl_host_.data() + off, a.gbl.data(), a.gbl.size());
+      d.gbl_off[i] = off;
+      gbl_used_ = off + a.gbl.size();
+    }
+  }
+  if (gbl_used_ > 0)
+    OPSB_CUDA(cudaMemcpyAsync(gbl_dev_, gbl_host_.data(), gbl_used_, cudaMemcpyHostToDevice, stream_));
+
+  if (!graphs_on_ || timing_on_ || q.size() < 2) {
+    launch_items(q);
+    return;
+  }
+  uint64_t key = queue_key(q);
+  GraphEntry &ge = graphs_[key];
+  ge.seen++;
+  if (ge.exec) {
+    OPSB_CUDA(cudaGraphLaunch(ge.exec, stream_));
+    graphs_launched_++;
+    kernels_launched_ += ge.kernels;
+    return;
+  }
+  if (ge.seen < 2) {
+    launch_items(q);
+    return;
+  }
+  // Second sighting of this queue structure: capture it once, replay from now on.
+  cudaGraph_t graph = nullptr;
+  long long before = kernels_launched_;
+  OPSB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  try {
+    launch_items(q);
+  } catch (...) {
+    cudaStreamEndCapture(stream_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  OPSB_CUDA(cudaStreamEndCapture(stream_, &graph));
+  ge.kernels = kernels_launched_ - before;
+  kernels_launched_ = before;
+  OPSB_CUDA(cudaGraphInstantiate(&ge.exec, graph, 0));
+  cudaGraphDestroy(graph);
+  OPSB_CUDA(cudaGraphLaunch(ge.exec, stream_));
+  graphs_launched_++;
+  kernels_launched_ += ge.kernels;
+}
+
+void Runtime::execute() {
+  if (!inited_ || queue_.empty()) return;
+  std::vector<Desc> q;
+  q.swap(queue_);
+  run_queue(q);
+}
+
+void Runtime::reduction_result(int handle, void *out) {
+  Reduction &r = reduction(handle);
+  execute();
+  OPSB_CUDA(cudaMemcpyAsync(out, r.slot_d, r.size, cudaMemcpyDeviceToHost, stream_));
+  OPSB_CUDA(cudaStreamSynchronize(stream_));
+  r.initialized = 0;  // ops_reduction_result_char resets the handle (ops_lib_core.cpp:1143)
+}
+
+// ---------------------------------------------------------------------------
+// Data access.
+// ---------------------------------------------------------------------------
+void Runtime::dat_set_data(int di, const void *host, size_t bytes) {
+  execute();
+  Dat &d = dat(di);
+  require(d.locked == 0, E_STATE, "ops_dat_set_data on a dat whose raw pointer is held");
+  size_t row = (size_t)d.size[0] * d.elem_size;
+  size_t rows = (size_t)d.size[1] * d.size[2];
+  require(bytes == row * rows, E_ARG, "ops_dat_set_data: buffer size does not match the dat extent");
+  OPSB_CUDA(cudaMemcpy2DAsync(d.data_d + (size_t)d.pad_front * d.elem_size, (size_t)d.pitch * d.elem_size, host, row,
+                              row, rows, cudaMemcpyHostToDevice, stream_));
+  OPSB_CUDA(cudaStreamSynchronize(stream_));
+  d.host.clear();
+}
+
+void Runtime::dat_fetch_data(int di, void *host, size_t bytes) {
+  execute();
+  Dat &d = dat(di);
+  size_t row = (size_t)d.size[0] * d.elem_size;
+  size_t rows = (size_t)d.size[1] * d.size[2];
+  require(bytes == row * rows, E_ARG, "ops_dat_fetch_data: buffer size does not match the dat extent");
+  OPSB_CUDA(cudaMemcpy2DAsync(host, row, d.data_d + (size_t)d.pad_front * d.elem_size, (size_t)d.pitch * d.elem_size,
+                              row, rows, cudaMemcpyDeviceToHost, stream_));
+  OPSB_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Runtime::dat_get_extents(int di, int *disp, int *size) {
+  Dat &d = dat(di);
+  int nd = blocks_[d.block].dims;
+  for (int i = 0; i < nd; i++) {
+    if (disp) disp[i] = 0;
+    if (size) size[i] = d.size[i];
+  }
+}
+
+// memspace: 1 = host, 2 = device (ops_memspace, ops/c/include/ops_lib_core.h).
+char *Runtime::dat_get_raw_pointer(int di, int memspace, int *stride_elems) {
+  execute();
+  Dat &d = dat(di);
+  require(d.locked == 0, E_STATE, "raw pointer already held for dat " + d.name);
+  if (stride_elems) {
+    stride_elems[0] = (int)d.pitch;
+    stride_elems[1] = d.size[1];
+    stride_elems[2] = d.size[2];
+  }
+  if (memspace == 2) {
+    OPSB_CUDA(cudaStreamSynchronize(stream_));
+    d.locked = 2;
+    return d.origin_ptr();
+  }
+  d.host.resize(d.bytes);
+  OPSB_CUDA(cudaMemcpyAsync(d.host.data(), d.data_d, d.bytes, cudaMemcpyDeviceToHost, stream_));
+  OPSB_CUDA(cudaStreamSynchronize(stream_));
+  d.locked = 1;
+  return d.host.data() + d.origin * d.elem_size;
+}
+
+void Runtime::dat_release_raw_data(int di, int acc) {
+  Dat &d = dat(di);
+  require(d.locked != 0, E_STATE, "ops_dat_release_raw_data without a matching ops_dat_get_raw_pointer");
+  if (d.locked == 1 && acc != ACC_READ) {
+    OPSB_CUDA(cudaMemcpyAsync(d.data_d, d.host.data(), d.bytes, cudaMemcpyHostToDevice, stream_));
+    OPSB_CUDA(cudaStreamSynchronize(stream_));
+  }
+  d.locked = 0;
+}
+
+void Runtime::release_to(const Mark &m) {
+  execute();
+  OPSB_CUDA(cudaStreamSynchronize(stream_));
+  // Cached graphs may reference storage about to be freed.
+  for (auto &kv : graphs_)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  graphs_.clear();
+  while (dats_.size() > m.dats) {
+    if (dats_.back() && dats_.back()->data_d) cudaFree(dats_.back()->data_d);
+    dats_.pop_back();
+  }
+  while (reductions_.size() > m.reductions) {
+    if (reductions_.back().slot_d) cudaFree(reductions_.back().slot_d);
+    reductions_.pop_back();
+  }
+  stencils_.resize(std::min(stencils_.size(), m.stencils));
+  blocks_.resize(std::min(blocks_.size(), m.blocks));
+}
+
+void Runtime::dat_swap(int a, int b) {
+  execute();
+  Dat &x = dat(a);
+  Dat &y = dat(b);
+  require(x.bytes == y.bytes && x.pitch == y.pitch && x.origin == y.origin && x.elem_size == y.elem_size, E_ARG,
+          "dat_swap needs two dats of identical layout");
+  std::swap(x.data_d, y.data_d);
+  x.host.clear();
+  y.host.clear();
+}
+
+}  // namespace opsb

@@ -1,0 +1,318 @@
+// OPS-B200 host runtime: declarations, device data, lazy loop queue,
+// reductions, constants and the launch of registered loop kernels.
+//
+// Semantics follow the reference runtime:
+//   dats            ops/c/src/core/ops_lib_core.cpp:445-548 (metadata),
+//                   ops/c/src/core/ops_device_singlenode_common.cpp:44-107
+//   stencils        ops/c/src/core/ops_lib_core.cpp:640-832
+//   args            ops/c/src/core/ops_lib_core.cpp:856,1047-1118
+//   lazy queue      ops/c/src/core/ops_lazy.cpp:186-275 (enqueue),
+//                   :1248-1377 (ops_execute), :1403-1440 (descriptor + hash)
+//   reductions      ops/c/src/core/ops_lib_core.cpp:1119-1143
+//   raw data access ops/c/src/core/ops_dummy_singlenode.cpp:662-850
+// The B200 design differs where the hardware asks for it: dat rows are
+// pitched to 128 bytes in HBM, reductions finish on the device and stay
+// there until a result is requested, a flushed queue is replayed as a CUDA
+// graph once its structure repeats, and registered chain kernels replace
+// runs of queued loops they cover exactly (fusion).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <initializer_list>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "ops_b200_device.cuh"
+
+namespace opsb {
+
+// Error codes of the C-ABI (include/ops_b200.h).
+enum ErrCode { E_OK = 0, E_ARG = -1, E_CUDA = -2, E_STATE = -3, E_NOTFOUND = -4, E_TIMEOUT = -5, E_UNSUPPORTED = -6 };
+
+struct Error {
+  int code;
+  std::string msg;
+  Error(int c, std::string m) : code(c), msg(std::move(m)) {}
+};
+
+void cuda_check(cudaError_t e, const char *what);
+#define OPSB_CUDA(call) ::opsb::cuda_check((call), #call)
+
+struct Block {
+  int index = 0, dims = 0;
+  std::string name;
+};
+
+struct Dat {
+  int index = 0, block = 0, dim = 1, type_size = 8, elem_size = 8;
+  int size[3] = {1, 1, 1};  // extent including halos (ops_dat_core::size)
+  int base[3] = {0, 0, 0}, d_m[3] = {0, 0, 0}, d_p[3] = {0, 0, 0};
+  int pad_front = 0;        // elements before logical column d_m[0]
+  long long pitch = 0;      // elements per x row (>= size[0] + pad_front)
+  long long plane = 0;      // elements per xy plane
+  long long origin = 0;     // element offset of logical index (0,0,0)
+  char *data_d = nullptr;   // device allocation
+  size_t bytes = 0;
+  std::string type, name;
+  int locked = 0;           // 0 free, 1 host raw pointer out, 2 device raw pointer out
+  std::vector<char> host;   // host mirror for host raw pointers
+  char *origin_ptr() const { return data_d + origin * elem_size; }
+};
+
+struct Stencil {
+  int index = 0, dims = 0, points = 0;
+  std::vector<int> offs;   // points*dims
+  int stride[3] = {1, 1, 1};
+  std::string name;
+};
+
+struct Reduction {
+  int index = 0, size = 0;  // size in bytes
+  int elem = 8;
+  std::string type, name;
+  char *slot_d = nullptr;   // device slot holding the running value
+  int initialized = 0;      // ops_reduction_core::initialized
+  int acc = -1;
+};
+
+// A loop argument as the host sees it (ops_arg, ops/c/include/ops_lib_core.h:509).
+struct Arg {
+  int kind = ARG_DAT;
+  int dat = -1, stencil = -1, dim = 1, acc = ACC_READ, opt = 1, red = -1;
+  int elem = 8;             // GBL/REDUCE element size in bytes
+  std::vector<char> gbl;    // GBL payload, copied at enqueue like ops_lazy.cpp:1434-1438
+};
+
+struct LoopInfo {
+  std::string kernel;       // registered name
+  int nparams = 0;
+  ParamInfo params[OPSB_MAX_ARGS];
+  int ndim = 2;             // accessor dimensionality (0 when the kernel has none)
+  int copy_dst = -1, copy_src = -1;  // pure copy kernels: which args are dst/src
+  int internal = 0;         // runtime-internal item (not launched through exec_loop)
+  void (*launch)(const LoopParams &, dim3, dim3, cudaStream_t) = nullptr;
+};
+
+// A queued loop (ops_kernel_descriptor, ops/c/include/ops_internal2.h:141-157).
+struct Desc {
+  const LoopInfo *loop = nullptr;
+  std::string name;
+  int block = 0, dim = 2;
+  int range[6] = {0, 1, 0, 1, 0, 1};
+  std::vector<Arg> args;
+  std::vector<int> red_first;  // per arg: 1 if the reduction handle restarts here
+  std::vector<size_t> gbl_off; // per arg: offset of its GBL payload in the arena
+  uint64_t hash = 0;
+};
+
+// A fused replacement for a run of queued loops. `match` inspects the queue
+// from position i and returns how many descriptors it covers (0 = no match);
+// `launch` enqueues the replacement work on the stream.
+struct ChainRule {
+  std::string name;
+  std::function<int(const std::vector<Desc> &, size_t)> match;
+  std::function<void(const std::vector<Desc> &, size_t, int, cudaStream_t)> launch;
+};
+
+struct LoopStats {
+  long long count = 0;
+};
+
+class Runtime {
+ public:
+  static Runtime &get();
+  static bool exists();
+  static void destroy();
+
+  void init(int device, int diags);
+  bool initialized() const { return inited_; }
+
+  int decl_block(int dims, const char *name);
+  int decl_dat(int block, int dim, const int *size, const int *base, const int *d_m, const int *d_p,
+               const void *data, int type_size, const char *type, const char *name);
+  int decl_stencil(int dims, int points, const int *offs, const int *stride, const char *name);
+  int decl_reduction(int size, const char *type, const char *name);
+  void decl_const(const char *name, int dim, const char *type, const void *data);
+
+  void par_loop(const LoopInfo *loop, const char *name, int block, int dim, const int *range,
+                const Arg *args, int nargs);
+  void execute();
+  void reduction_result(int handle, void *out);
+
+  // Data access (ops_dat_* in ops/c/src/core/ops_dummy_singlenode.cpp:611-850).
+  void dat_set_data(int dat, const void *host, size_t bytes);
+  void dat_fetch_data(int dat, void *host, size_t bytes);
+  void dat_get_extents(int dat, int *disp, int *size);
+  char *dat_get_raw_pointer(int dat, int memspace, int *stride_elems);
+  void dat_release_raw_data(int dat, int acc);
+  void dat_swap(int a, int b);  // exchange device storage of two same-shape dats
+
+  Dat &dat(int i);
+  Stencil &stencil(int i);
+  Reduction &reduction(int i);
+  Block &block(int i);
+  int ndats() const { return (int)dats_.size(); }
+  cudaStream_t stream() const { return stream_; }
+
+  // Registry of loops (by kernel name) and of named device constants.
+  static void register_loop(const LoopInfo &info);
+  static const LoopInfo *find_loop(const std::string &kernel);
+  // A named constant (ops_decl_const / ops_update_const) maps to `bytes` at
+  // `offset` inside a __constant__ symbol; one name may feed several modules.
+  static void register_const(const std::string &name, const void *symbol, size_t offset, size_t bytes);
+  static void register_chain(const ChainRule &rule);
+
+  // Build the device-side view of a queued loop.
+  void build_params(const Desc &d, LoopParams &lp, int *nred_out);
+  static void launch_shape(const int *range, int dim, bool reduces, dim3 &grid, dim3 &block);
+
+  // Counters.
+  long long kernels_launched() const { return kernels_launched_; }
+  long long graphs_launched() const { return graphs_launched_; }
+  long long loops_enqueued() const { return loops_enqueued_; }
+  void count_kernels(long long n) { kernels_launched_ += n; }
+  void set_graphs(int on) { graphs_on_ = on; }
+  // Per-kernel CUDA-event timing (launches are bracketed by events on the
+  // runtime stream; graphs are bypassed while it is on).
+  void set_timing(int on);
+  void collect_timing();
+  struct KTime { long long launches = 0; double ms = 0.0; };
+  const std::map<std::string, KTime> &kernel_times() { collect_timing(); return ktimes_; }
+  void clear_timing() { collect_timing(); ktimes_.clear(); }
+  void timed_launch_begin(const std::string &name);
+  void timed_launch_end();
+  void set_fusion(int on) { fusion_on_ = on; }
+  int fusion_enabled() const { return fusion_on_; }
+  int diags() const { return diags_; }
+  void reset_counters() { kernels_launched_ = graphs_launched_ = loops_enqueued_ = 0; }
+  char *red_scratch() const { return red_scratch_; }
+  unsigned int *red_counters() const { return red_counters_; }
+  static constexpr int kMaxRedBlocks = 65536;
+  static constexpr int kNumCounters = 256;
+
+  // Declarations made by one app call are released when it returns.
+  struct Mark { size_t blocks, dats, stencils, reductions; };
+  Mark mark() const { return {blocks_.size(), dats_.size(), stencils_.size(), reductions_.size()}; }
+  void release_to(const Mark &m);
+
+  ~Runtime();
+
+ private:
+  Runtime() = default;
+  void run_queue(std::vector<Desc> &q);
+  void elide_copies(std::vector<Desc> &q);
+  void launch_swap_outside(const Desc &d, cudaStream_t s);
+  void launch_items(std::vector<Desc> &q);
+  uint64_t queue_key(const std::vector<Desc> &q) const;
+
+  bool inited_ = false;
+  int device_ = 0, diags_ = 0;
+  cudaStream_t stream_ = nullptr;
+  std::vector<Block> blocks_;
+  std::vector<std::unique_ptr<Dat>> dats_;
+  std::vector<Stencil> stencils_;
+  std::vector<Reduction> reductions_;
+  std::vector<Desc> queue_;
+
+  // GBL arena: host staging and its device copy, refilled per flush.
+  std::vector<char> gbl_host_;
+  char *gbl_dev_ = nullptr;
+  size_t gbl_cap_ = 0;
+  size_t gbl_used_ = 0;
+
+  char *red_scratch_ = nullptr;
+  unsigned int *red_counters_ = nullptr;
+
+  struct GraphEntry {
+    int seen = 0;
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;
+  };
+  std::unordered_map<uint64_t, GraphEntry> graphs_;
+  int graphs_on_ = 1;
+  int timing_on_ = 0;
+  struct PendingTime { std::string name; cudaEvent_t a, b; };
+  std::vector<PendingTime> pending_;
+  std::vector<cudaEvent_t> event_pool_;
+  std::map<std::string, KTime> ktimes_;
+  std::string cur_name_;
+  cudaEvent_t cur_ev_ = nullptr;
+  int fusion_on_ = 1;
+  long long kernels_launched_ = 0, graphs_launched_ = 0, loops_enqueued_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// C++ convenience API used by the app drivers (mirrors ops_arg_* and
+// ops_par_loop of ops/c/include/ops_lib_core.h / ops_seq_v2.h).
+// ---------------------------------------------------------------------------
+inline Arg arg_dat(int dat, int dim, int stencil, int acc) {
+  Arg a; a.kind = ARG_DAT; a.dat = dat; a.dim = dim; a.stencil = stencil; a.acc = acc; return a;
+}
+inline Arg arg_dat_opt(int dat, int dim, int stencil, int acc, int flag) {
+  Arg a = arg_dat(dat, dim, stencil, acc); a.opt = flag ? 1 : 0; return a;
+}
+inline Arg arg_gbl(const void *data, int dim, int elem, int acc) {
+  Arg a; a.kind = ARG_GBL; a.dim = dim; a.elem = elem; a.acc = acc;
+  a.gbl.assign((const char *)data, (const char *)data + (size_t)dim * elem);
+  return a;
+}
+inline Arg arg_reduce(int handle, int dim, int acc) {
+  Arg a; a.kind = ARG_REDUCE; a.red = handle; a.dim = dim; a.acc = acc; return a;
+}
+inline Arg arg_idx() { Arg a; a.kind = ARG_IDX; a.dim = 1; a.elem = 4; return a; }
+
+template <class K>
+void launch_exec(const LoopParams &lp, dim3 g, dim3 b, cudaStream_t s) {
+  exec_loop<K><<<g, b, 0, s>>>(lp);
+}
+
+template <class K, class = void>
+struct CopyTrait { static constexpr int dst = -1, src = -1; };
+template <class K>
+struct CopyTrait<K, std::void_t<decltype(K::copy_dst)>> { static constexpr int dst = K::copy_dst, src = K::copy_src; };
+
+template <class K>
+LoopInfo make_loop_info(const char *kernel) {
+  LoopInfo li;
+  li.kernel = kernel;
+  using S = SigInfo<decltype(&K::operator())>;
+  li.nparams = S::n;
+  S::fill(li.params);
+  li.ndim = 0;
+  for (int i = 0; i < li.nparams; i++)
+    if (li.params[i].cls == 'A') li.ndim = li.params[i].ndim;
+  li.copy_dst = CopyTrait<K>::dst;
+  li.copy_src = CopyTrait<K>::src;
+  li.launch = &launch_exec<K>;
+  return li;
+}
+
+// Registers K under `kernel` at static-initialisation time.
+// Registers K under K::kname at static-initialisation time so that the
+// C-ABI can launch it by name.
+template <class K>
+struct LoopRegistrar {
+  LoopRegistrar() { Runtime::register_loop(make_loop_info<K>(K::kname)); }
+};
+#define OPSB_REGISTER_LOOP(K) static ::opsb::LoopRegistrar<K> opsb_reg_##K
+
+// ops_par_loop(kernel, name, block, dim, range, args...) for a functor K.
+template <class K>
+void par_loop(const char *name, int block, int dim, const int *range, std::initializer_list<Arg> args) {
+  static const LoopInfo *li = nullptr;
+  if (!li) {
+    li = Runtime::find_loop(K::kname);
+    if (!li) {
+      static LoopInfo own = make_loop_info<K>(K::kname);
+      li = &own;
+    }
+  }
+  Runtime::get().par_loop(li, name, block, dim, range, args.begin(), (int)args.size());
+}
+
+}  // namespace opsb

@@ -1,0 +1,223 @@
+"""Python mirror of the OPS C/C++ API over the OPS-B200 C-ABI.
+
+Names, argument order and meaning follow ops/c/include/ops_lib_core.h and
+ops_seq_v2.h; failures raise OpsError (the reference throws OPSException,
+ops/c/include/ops_exceptions.h:46-77). Kernels are the registered sm_100a
+loop kernels, named "<app>/<kernel>" where <kernel> is the reference's kernel
+function name (e.g. "laplace2d/apply_stencil").
+
+    ops_init(0)
+    grid = ops_decl_block(2, "grid")
+    A = ops_decl_dat(grid, 1, [nx, ny], [0, 0], [-1, -1], [1, 1], None, "double", "A")
+    ...
+    ops_par_loop("laplace2d/apply_stencil", "apply stencil", grid, 2, [0, nx, 0, ny],
+                 ops_arg_dat(A, 1, S5, "double", OPS_READ),
+                 ops_arg_dat(Anew, 1, S0, "double", OPS_WRITE),
+                 ops_arg_reduce(h_err, 1, "double", OPS_MAX))
+    err = ops_reduction_result(h_err)
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import OpsError, check, lib
+
+OPS_READ, OPS_WRITE, OPS_RW, OPS_INC, OPS_MIN, OPS_MAX = 0, 1, 2, 3, 4, 5
+OPS_HOST, OPS_DEVICE = 1, 2
+
+_TYPES = {"double": (np.float64, 8), "float": (np.float32, 4), "int": (np.int32, 4),
+          "long long": (np.int64, 8), "ll": (np.int64, 8)}
+
+
+class ops_block:
+    def __init__(self, h, dims, name):
+        self.index, self.dims, self.name = h, dims, name
+
+
+class ops_dat:
+    def __init__(self, h, block, dim, size, d_m, d_p, type_, name):
+        self.index, self.block, self.dim, self.type, self.name = h, block, dim, type_, name
+        self.d_m, self.d_p = list(d_m), list(d_p)
+        # Full extent including halos (ops_dat_core::size).
+        self.size = [s - m + p for s, m, p in zip(size, d_m, d_p)]
+
+    @property
+    def dtype(self):
+        return _TYPES[self.type][0]
+
+    def extent_shape(self):
+        """numpy shape of the full extent, slowest dimension first."""
+        shp = list(reversed(self.size))
+        if self.dim > 1:
+            shp.append(self.dim)
+        return tuple(shp)
+
+
+class ops_stencil:
+    def __init__(self, h, dims, points, name):
+        self.index, self.dims, self.points, self.name = h, dims, points, name
+
+
+class ops_reduction:
+    def __init__(self, h, size, type_, name):
+        self.index, self.size, self.type, self.name = h, size, type_, name
+
+
+def _iarr(v):
+    a = (ctypes.c_int * len(v))(*[int(x) for x in v])
+    return a
+
+
+def ops_init(device=0, diags=0):
+    check(lib().ops_b200_init(device, diags))
+
+
+def ops_exit():
+    check(lib().ops_b200_exit())
+
+
+def ops_decl_block(dims, name):
+    return ops_block(check(lib().ops_b200_decl_block(dims, name.encode())), dims, name)
+
+
+def ops_decl_dat(block, dim, size, base, d_m, d_p, data, type_, name):
+    """ops_decl_dat; `data` (numpy array or None) holds the full extent."""
+    dtype, ts = _TYPES[type_]
+    buf = None
+    if data is not None:
+        buf = np.ascontiguousarray(data, dtype=dtype)
+    h = check(lib().ops_b200_decl_dat(block.index, dim, _iarr(size), _iarr(base), _iarr(d_m), _iarr(d_p),
+                                      buf.ctypes.data if buf is not None else None, ts, type_.encode(),
+                                      name.encode()))
+    return ops_dat(h, block, dim, size, d_m, d_p, type_, name)
+
+
+def ops_decl_stencil(dims, points, sten, name):
+    return ops_stencil(check(lib().ops_b200_decl_stencil(dims, points, _iarr(sten), name.encode())), dims,
+                       points, name)
+
+
+def ops_decl_strided_stencil(dims, points, sten, stride, name):
+    return ops_stencil(check(lib().ops_b200_decl_strided_stencil(dims, points, _iarr(sten), _iarr(stride),
+                                                                 name.encode())), dims, points, name)
+
+
+def ops_decl_reduction_handle(size, type_, name):
+    return ops_reduction(check(lib().ops_b200_decl_reduction_handle(size, type_.encode(), name.encode())), size,
+                         type_, name)
+
+
+def ops_decl_const(name, dim, type_, data):
+    arr = np.ascontiguousarray(np.atleast_1d(data), dtype=_TYPES[type_][0]) if type_ in _TYPES else data
+    check(lib().ops_b200_decl_const(name.encode(), dim, type_.encode(),
+                                    arr.ctypes.data if isinstance(arr, np.ndarray) else ctypes.addressof(arr)))
+
+
+ops_update_const = ops_decl_const
+
+
+def ops_arg_dat(dat, dim, stencil, type_, acc):
+    return _lib.Arg(_lib.ARG_DAT, dat.index, stencil.index, dim, acc, 1, -1, 0, None), None
+
+
+def ops_arg_dat_opt(dat, dim, stencil, type_, acc, flag):
+    return _lib.Arg(_lib.ARG_DAT, dat.index, stencil.index, dim, acc, 1 if flag else 0, -1, 0, None), None
+
+
+def ops_arg_gbl(data, dim, type_, acc):
+    arr = np.ascontiguousarray(np.atleast_1d(data), dtype=_TYPES[type_][0])
+    return _lib.Arg(_lib.ARG_GBL, -1, -1, dim, acc, 1, -1, arr.itemsize, arr.ctypes.data), arr
+
+
+def ops_arg_reduce(handle, dim, type_, acc):
+    return _lib.Arg(_lib.ARG_REDUCE, -1, -1, dim, acc, 1, handle.index, 0, None), None
+
+
+def ops_arg_idx():
+    return _lib.Arg(_lib.ARG_IDX, -1, -1, 1, OPS_READ, 1, -1, 4, None), None
+
+
+def ops_par_loop(kernel, name, block, dim, rng, *args):
+    """Queue one loop; `kernel` is a registered kernel name."""
+    arr = (_lib.Arg * max(1, len(args)))()
+    keep = []
+    for i, (a, k) in enumerate(args):
+        arr[i] = a
+        keep.append(k)
+    check(lib().ops_b200_par_loop(kernel.encode(), name.encode(), block.index, dim, _iarr(rng), len(args), arr))
+
+
+def ops_execute():
+    check(lib().ops_b200_execute())
+
+
+def ops_reduction_result(handle, count=None):
+    """Returns the reduced value(s) as a numpy array (or a scalar for width 1)."""
+    dtype, ts = _TYPES[handle.type]
+    n = handle.size // ts
+    out = np.zeros(n, dtype=dtype)
+    check(lib().ops_b200_reduction_result(handle.index, out.ctypes.data))
+    return out[0] if n == 1 else out
+
+
+def ops_dat_set_data(dat, data):
+    buf = np.ascontiguousarray(data, dtype=dat.dtype)
+    check(lib().ops_b200_dat_set_data(dat.index, buf.ctypes.data, buf.nbytes))
+
+
+def ops_dat_fetch_data(dat):
+    out = np.zeros(dat.extent_shape(), dtype=dat.dtype)
+    check(lib().ops_b200_dat_fetch_data(dat.index, out.ctypes.data, out.nbytes))
+    return out
+
+
+def ops_dat_get_extents(dat):
+    nd = dat.block.dims
+    disp = (ctypes.c_int * nd)()
+    size = (ctypes.c_int * nd)()
+    check(lib().ops_b200_dat_get_extents(dat.index, disp, size))
+    return list(disp), list(size)
+
+
+def ops_dat_get_raw_pointer(dat, memspace):
+    ptr = ctypes.c_void_p()
+    stride = (ctypes.c_int * 3)()
+    check(lib().ops_b200_dat_get_raw_pointer(dat.index, memspace, ctypes.byref(ptr), stride))
+    return ptr.value, list(stride)
+
+
+def ops_dat_release_raw_data(dat, acc):
+    check(lib().ops_b200_dat_release_raw_data(dat.index, acc))
+
+
+def set_option(name, value):
+    check(lib().ops_b200_set_option(name.encode(), int(value)))
+
+
+def counters():
+    k, g, l = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    check(lib().ops_b200_counters(ctypes.byref(k), ctypes.byref(g), ctypes.byref(l)))
+    return {"kernels": k.value, "graphs": g.value, "loops": l.value}
+
+
+def set_kernel_timing(on):
+    check(lib().ops_b200_set_kernel_timing(int(on)))
+
+
+def kernel_time(kernel):
+    n, ms = ctypes.c_longlong(), ctypes.c_double()
+    check(lib().ops_b200_kernel_time(kernel.encode(), ctypes.byref(n), ctypes.byref(ms)))
+    return n.value, ms.value
+
+
+def clear_kernel_timing():
+    check(lib().ops_b200_clear_kernel_timing())
+
+
+def reset_counters():
+    check(lib().ops_b200_reset_counters())
+
+
+__all__ = [n for n in dir() if n.startswith("ops_")] + ["OpsError", "set_option", "counters", "reset_counters",
+                                                          "set_kernel_timing", "kernel_time", "clear_kernel_timing"]

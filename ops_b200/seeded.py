@@ -1,0 +1,41 @@
+"""Seeded synthetic inputs (counter-based SplitMix64, numpy uint64).
+
+The k-th output of the stream `seed` is mix(seed + (k+1) * GAMMA) with the
+SplitMix64 finaliser (Steele, Lea, Flood, OOPSLA 2014); uniform doubles take
+its top 53 bits. Identical bit for bit to the C definition used on the
+reference side (oracle/src/seeded_rng.h), which a CPU test checks.
+"""
+import numpy as np
+
+GAMMA = np.uint64(0x9E3779B97F4A7C15)
+M1 = np.uint64(0xBF58476D1CE4E5B9)
+M2 = np.uint64(0x94D049BB133111EB)
+
+
+def sm64_at(seed, k):
+    """Raw 64-bit outputs for counter array k (any integer array)."""
+    k = np.asarray(k, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (k + np.uint64(1)) * GAMMA
+        z = (z ^ (z >> np.uint64(30))) * M1
+        z = (z ^ (z >> np.uint64(27))) * M2
+        return z ^ (z >> np.uint64(31))
+
+
+def u01(seed, k):
+    """Uniform doubles in [0, 1)."""
+    return (sm64_at(seed, k) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def uniform(seed, k, lo, hi):
+    return lo + (hi - lo) * u01(seed, k)
+
+
+def laplace_field(imax, jmax, seed):
+    """Laplace initial field: full (jmax+2) x (imax+2) extent, zero interior,
+    ring cell (x, y) = u01(seed, (y+1)*(imax+2) + (x+1))."""
+    W, H = imax + 2, jmax + 2
+    k = np.arange(W * H, dtype=np.uint64).reshape(H, W)
+    A = u01(seed, k)
+    A[1:-1, 1:-1] = 0.0
+    return np.ascontiguousarray(A)
