@@ -139,6 +139,16 @@ int ops_b200_reset_counters(void);
 int ops_b200_set_kernel_timing(int on);
 int ops_b200_kernel_time(const char *kernel, long long *launches, double *total_ms);
 int ops_b200_clear_kernel_timing(void);
+/* All timed kernels: up to `max` entries of name (NUL-terminated, at most 95
+ * characters), launches, total milliseconds and total compulsory bytes
+ * (each dat argument's points once; read-write twice). Returns the count. */
+typedef struct ops_b200_kernel_stat {
+  char name[96];
+  long long launches;
+  double total_ms;
+  double alg_bytes;
+} ops_b200_kernel_stat;
+int ops_b200_kernel_stats(ops_b200_kernel_stat *out, int max);
 
 /* ---- apps ----------------------------------------------------------------
  * Reference app drivers restated in C++ on the runtime above; they issue the
@@ -152,6 +162,34 @@ int ops_b200_clear_kernel_timing(void);
  * device seconds (CUDA events) of the last `iters` iterations. */
 int ops_b200_app_laplace2d(int imax, int jmax, int warmup, int iters, const double *field_in, double *field_out,
                            double *err_per_iter, double *device_seconds);
+
+/* CloverLeaf 2D hydro (apps/c/CloverLeaf/clover_leaf.cpp:161-214). The deck
+ * holds the values the reference reads from clover.in
+ * (apps/c/CloverLeaf/read_input.cpp:36-276). */
+typedef struct ops_b200_clover_state {
+  double density, energy, xvel, yvel;
+  int geometry;                           /* 1 rectangle, 2 circle, 3 point    */
+  double xmin, xmax, ymin, ymax, radius;
+} ops_b200_clover_state;
+
+typedef struct ops_b200_clover_deck {
+  int x_cells, y_cells;
+  double xmin, ymin, xmax, ymax;
+  double initial_timestep, timestep_rise, max_timestep, end_time;
+  int end_step, summary_frequency;
+  int number_of_states;                   /* 1..16; state 0 is the background */
+  ops_b200_clover_state states[16];
+} ops_b200_clover_deck;
+
+/* Runs the deck to completion. Every field summary (the set-up one, one per
+ * summary_frequency steps and the final one) is written to `summaries` as 8
+ * doubles {step, time, volume, mass, internal energy, kinetic energy,
+ * pressure sum, dt} (up to max_summaries rows; *n_summaries gets the count).
+ * device_seconds: CUDA-event time of the cycles after the first
+ * `warmup_steps`. dump_dir (may be NULL): every dat's full extent is written
+ * to <dump_dir>/<name>.bin at the end. */
+int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int warmup_steps, double *summaries,
+                            int max_summaries, int *n_summaries, double *device_seconds, const char *dump_dir);
 
 #ifdef __cplusplus
 }

@@ -31,6 +31,27 @@ class Arg(ctypes.Structure):
                 ("reduction", ctypes.c_int), ("elem_size", ctypes.c_int), ("gbl", ctypes.c_void_p)]
 
 
+class KernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 96), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double),
+                ("alg_bytes", ctypes.c_double)]
+
+
+class CloverState(ctypes.Structure):
+    _fields_ = [("density", ctypes.c_double), ("energy", ctypes.c_double), ("xvel", ctypes.c_double),
+                ("yvel", ctypes.c_double), ("geometry", ctypes.c_int), ("xmin", ctypes.c_double),
+                ("xmax", ctypes.c_double), ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
+                ("radius", ctypes.c_double)]
+
+
+class CloverDeck(ctypes.Structure):
+    _fields_ = [("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int), ("xmin", ctypes.c_double),
+                ("ymin", ctypes.c_double), ("xmax", ctypes.c_double), ("ymax", ctypes.c_double),
+                ("initial_timestep", ctypes.c_double), ("timestep_rise", ctypes.c_double),
+                ("max_timestep", ctypes.c_double), ("end_time", ctypes.c_double), ("end_step", ctypes.c_int),
+                ("summary_frequency", ctypes.c_int), ("number_of_states", ctypes.c_int),
+                ("states", CloverState * 16)]
+
+
 _lib = None
 
 
@@ -80,7 +101,9 @@ def _declare(L):
         "ops_b200_set_kernel_timing": ([i], i),
         "ops_b200_kernel_time": ([cp, P, P], i),
         "ops_b200_clear_kernel_timing": ([], i),
+        "ops_b200_kernel_stats": ([P, i], i),
         "ops_b200_app_laplace2d": ([i, i, i, i, P, P, P, P], i),
+        "ops_b200_app_cloverleaf": ([P, i, P, i, P, P, cp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

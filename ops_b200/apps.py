@@ -24,3 +24,72 @@ def laplace2d(field, iters, warmup=0, return_errors=True):
     check(lib().ops_b200_app_laplace2d(imax, jmax, warmup, iters, _ptr(field), _ptr(out), _ptr(errs),
                                        ctypes.byref(secs)))
     return out, (errs[:warmup + iters] if errs is not None else None), secs.value
+
+
+# ---------------------------------------------------------------------------
+# CloverLeaf
+# ---------------------------------------------------------------------------
+# read_input.cpp:46-68 defaults, overridden by the deck.
+CLOVER_DEFAULTS = dict(x_cells=10, y_cells=10, xmin=0.0, ymin=0.0, xmax=100.0, ymax=100.0, initial_timestep=0.1,
+                       timestep_rise=1.5, max_timestep=1.0, end_time=10.0, end_step=640000, summary_frequency=10)
+GEOMETRY = {"rectangle": 1, "circle": 2, "point": 3}
+
+
+def clover_deck(**kw):
+    """Build a deck from keyword values; `states` is a list of dicts with
+    density, energy and optionally xvel, yvel, geometry, xmin..ymax, radius."""
+    from ._lib import CloverDeck
+    d = CloverDeck()
+    vals = dict(CLOVER_DEFAULTS)
+    vals.update({k: v for k, v in kw.items() if k != "states"})
+    for k, v in vals.items():
+        setattr(d, k, v)
+    states = kw["states"]
+    d.number_of_states = len(states)
+    for i, s in enumerate(states):
+        st = d.states[i]
+        st.density, st.energy = s["density"], s["energy"]
+        st.xvel, st.yvel = s.get("xvel", 0.0), s.get("yvel", 0.0)
+        g = s.get("geometry", 0)
+        st.geometry = GEOMETRY.get(g, g) if isinstance(g, str) else g
+        for k in ("xmin", "xmax", "ymin", "ymax", "radius"):
+            setattr(st, k, s.get(k, 0.0))
+    return d
+
+
+def clover_deck_text(deck):
+    """The same deck as clover.in text (17 significant digits, so the
+    reference's atof reads back identical doubles)."""
+    g = lambda v: repr(float(v))
+    lines = ["*clover"]
+    for i in range(deck.number_of_states):
+        s = deck.states[i]
+        line = f" state {i + 1} density={g(s.density)} energy={g(s.energy)}"
+        if s.xvel != 0.0:
+            line += f" xvel={g(s.xvel)}"
+        if s.yvel != 0.0:
+            line += f" yvel={g(s.yvel)}"
+        if i > 0:
+            geo = {1: "rectangle", 2: "circle", 3: "point"}[s.geometry]
+            line += f" geometry={geo} xmin={g(s.xmin)} xmax={g(s.xmax)} ymin={g(s.ymin)} ymax={g(s.ymax)}"
+            if s.geometry == 2:
+                line += f" radius={g(s.radius)}"
+        lines.append(line)
+    lines += [f" x_cells={deck.x_cells}", f" y_cells={deck.y_cells}", f" xmin={g(deck.xmin)}", f" ymin={g(deck.ymin)}",
+              f" xmax={g(deck.xmax)}", f" ymax={g(deck.ymax)}", f" initial_timestep={g(deck.initial_timestep)}",
+              f" timestep_rise={g(deck.timestep_rise)}", f" max_timestep={g(deck.max_timestep)}",
+              f" end_time={g(deck.end_time)}", f" end_step={deck.end_step}",
+              f" summary_frequency={deck.summary_frequency}", "*endclover", ""]
+    return "\n".join(lines)
+
+
+def cloverleaf(deck, warmup_steps=0, dump_dir=None, max_summaries=100000):
+    """Runs a CloverLeaf deck on the GPU. Returns (summaries[n, 8], device_seconds);
+    columns: step, time, volume, mass, internal energy, kinetic energy, pressure sum, dt."""
+    out = np.zeros((max_summaries, 8))
+    n = ctypes.c_int(0)
+    secs = ctypes.c_double(0.0)
+    check(lib().ops_b200_app_cloverleaf(ctypes.byref(deck), warmup_steps, out.ctypes.data, max_summaries,
+                                        ctypes.byref(n), ctypes.byref(secs),
+                                        dump_dir.encode() if dump_dir else None))
+    return out[:n.value].copy(), secs.value

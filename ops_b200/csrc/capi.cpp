@@ -1,6 +1,7 @@
 // extern "C" entry points of include/ops_b200.h over the C++ runtime.
 #include "../../include/ops_b200.h"
 
+#include <cstring>
 #include <string>
 
 #include "runtime.h"
@@ -225,6 +226,24 @@ int ops_b200_kernel_time(const char *kernel, long long *launches, double *total_
     if (launches) *launches = it == m.end() ? 0 : it->second.launches;
     if (total_ms) *total_ms = it == m.end() ? 0.0 : it->second.ms;
     return 0;
+  });
+}
+
+int ops_b200_kernel_stats(ops_b200_kernel_stat *out, int max) {
+  return guarded([&] {
+    const auto &m = rt().kernel_times();
+    int n = 0;
+    for (const auto &kv : m) {
+      if (out && n < max) {
+        strncpy(out[n].name, kv.first.c_str(), sizeof(out[n].name) - 1);
+        out[n].name[sizeof(out[n].name) - 1] = 0;
+        out[n].launches = kv.second.launches;
+        out[n].total_ms = kv.second.ms;
+        out[n].alg_bytes = kv.second.bytes;
+      }
+      n++;
+    }
+    return n;
   });
 }
 

@@ -33,21 +33,21 @@ struct copy {
 
 struct left_bndcon {
   static constexpr const char *kname = "laplace2d/left_bndcon";
-  __device__ void operator()(ACC2<double> &A, const int *idx) const {
+  __device__ void operator()(ACC2<double> &A, const IDX &idx) const {
     A(0, 0) = sin(c_lap.pi * (idx[1] + 1) / (c_lap.jmax + 1));
   }
 };
 
 struct right_bndcon {
   static constexpr const char *kname = "laplace2d/right_bndcon";
-  __device__ void operator()(ACC2<double> &A, const int *idx) const {
+  __device__ void operator()(ACC2<double> &A, const IDX &idx) const {
     A(0, 0) = sin(c_lap.pi * (idx[1] + 1) / (c_lap.jmax + 1)) * exp(-c_lap.pi);
   }
 };
 
 struct apply_stencil {
   static constexpr const char *kname = "laplace2d/apply_stencil";
-  __device__ void operator()(const ACC2<double> &A, ACC2<double> &Anew, double *error) const {
+  __device__ void operator()(const ACC2<double> &A, ACC2<double> &Anew, RED<double> &error) const {
     Anew(0, 0) = 0.25f * (A(1, 0) + A(-1, 0) + A(0, -1) + A(0, 1));
     *error = fmax(*error, fabs(Anew(0, 0) - A(0, 0)));
   }

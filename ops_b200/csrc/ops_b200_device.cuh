@@ -46,7 +46,9 @@ struct ACC2 {
   int sx, sy;
   ACC2() = default;
   __device__ __forceinline__ ACC2(T *p_, int sx_, int sy_) : p(p_), sx(sx_), sy(sy_) {}
-  __device__ __forceinline__ T &operator()(int i, int j) const { return p[i * sx + j * sy]; }
+  __device__ __forceinline__ T &operator()(int i, int j) { return p[i * sx + j * sy]; }
+  // Read-only view (the kernel's const ACC<T>& arguments): non-coherent loads.
+  __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (i * sx + j * sy)); }
 };
 
 // 3D accessor.
@@ -56,9 +58,28 @@ struct ACC3 {
   int sx, sy, sz;
   ACC3() = default;
   __device__ __forceinline__ ACC3(T *p_, int sx_, int sy_, int sz_) : p(p_), sx(sx_), sy(sy_), sz(sz_) {}
-  __device__ __forceinline__ T &operator()(int i, int j, int k) const {
+  __device__ __forceinline__ T &operator()(int i, int j, int k) {
     return p[i * sx + (long long)j * sy + (long long)k * sz];
   }
+  __device__ __forceinline__ T operator()(int i, int j, int k) const {
+    return __ldg(p + (i * sx + (long long)j * sy + (long long)k * sz));
+  }
+};
+
+// Reduction target of a kernel (the reference passes a T*): a thread-local
+// accumulator of N components kept in registers; *r and r[i] read like the
+// reference's pointer.
+template <class T, int N = 1>
+struct RED {
+  T v[N];
+  __device__ __forceinline__ T &operator*() { return v[0]; }
+  __device__ __forceinline__ T &operator[](int i) { return v[i]; }
+};
+
+// The point's index (ops_arg_idx; the reference passes const int*).
+struct IDX {
+  int v[3];
+  __device__ __forceinline__ int operator[](int i) const { return v[i]; }
 };
 
 // One loop argument as the device sees it.
@@ -159,50 +180,41 @@ struct Slot<ACC3<T>> {
   template <class S> __device__ __forceinline__ void finish(const ArgView &, const LoopParams &, S *, int) {}
 };
 
-// Non-const pointer: a reduction target (thread-local accumulator), the
-// point's index (int only) or a read-write global.
-template <class T>
-struct Slot<T *> {
-  T red[OPSB_MAX_RED_DIM];
-  int idx[3];
+template <class T, int N>
+struct Slot<RED<T, N>> {
+  RED<T, N> r;
   __device__ __forceinline__ void init(const ArgView &a) {
-    if (a.kind == ARG_REDUCE) {
-      for (int d = 0; d < OPSB_MAX_RED_DIM; d++) red[d] = red_identity<T>(a.acc);
-    }
+#pragma unroll
+    for (int d = 0; d < N; d++) r.v[d] = red_identity<T>(a.acc);
   }
-  __device__ __forceinline__ T *at(const ArgView &a, int x, int y, int z) {
-    if (a.kind == ARG_REDUCE) return red;
-    if (a.kind == ARG_IDX) {
-      idx[0] = x; idx[1] = y; idx[2] = z;
-      return reinterpret_cast<T *>(idx);
-    }
-    return reinterpret_cast<T *>(a.ptr);
-  }
-  // Fold this thread's partial into the block's, then across blocks.
+  __device__ __forceinline__ RED<T, N> &at(const ArgView &, int, int, int) { return r; }
+  // Fold this thread's partial into the block's and store the block partial.
   __device__ void finish(const ArgView &a, const LoopParams &lp, T *smem, int nblocks) {
-    if (a.kind != ARG_REDUCE) return;
     const int bid = blockIdx.x + blockIdx.y * gridDim.x;
-    T *part = reinterpret_cast<T *>(lp.red_scratch) +
-              ((size_t)a.red_index * nblocks + bid) * OPSB_MAX_RED_DIM;
-    for (int d = 0; d < a.dim; d++) {
-      T v = block_reduce<T>(red[d], a.acc, smem);
-      if (threadIdx.x == 0 && threadIdx.y == 0) part[d] = v;
+    T *part = reinterpret_cast<T *>(lp.red_scratch) + ((size_t)a.red_index * nblocks + bid) * OPSB_MAX_RED_DIM;
+#pragma unroll
+    for (int d = 0; d < N; d++) {
+      T v = block_reduce<T>(r.v[d], a.acc, smem);
+      if (threadIdx.x == 0 && threadIdx.y == 0 && d < a.dim) part[d] = v;
     }
   }
 };
 
-template <class T>
-struct Slot<const T *> {
-  int idx[3];
+template <>
+struct Slot<IDX> {
+  IDX i;
   __device__ __forceinline__ void init(const ArgView &) {}
-  __device__ __forceinline__ const T *at(const ArgView &a, int x, int y, int z) {
-    if (a.kind == ARG_IDX) {
-      idx[0] = x; idx[1] = y; idx[2] = z;
-      return reinterpret_cast<const T *>(idx);
-    }
-    return reinterpret_cast<const T *>(a.ptr);
+  __device__ __forceinline__ IDX &at(const ArgView &, int x, int y, int z) {
+    i.v[0] = x; i.v[1] = y; i.v[2] = z;
+    return i;
   }
-  template <class S> __device__ __forceinline__ void finish(const ArgView &, const LoopParams &, S *, int) {}
+};
+
+// Pointer parameters are globals (ops_arg_gbl): READ as const T*, RW as T*.
+template <class T>
+struct Slot<T *> {
+  __device__ __forceinline__ void init(const ArgView &) {}
+  __device__ __forceinline__ T *at(const ArgView &a, int, int, int) { return reinterpret_cast<T *>(a.ptr); }
 };
 
 // Minimal tuple of slots (device code, no std::tuple).
@@ -214,7 +226,7 @@ template <size_t I, class T> __device__ __forceinline__ T &get_leaf(Leaf<I, T> &
 
 // Reduction element type of a parameter (void when it cannot reduce).
 template <class P> struct RedElem { using type = void; };
-template <class T> struct RedElem<T *> { using type = T; };
+template <class T, int N> struct RedElem<RED<T, N>> { using type = T; };
 
 // Combine the per-block partials of every reduction arg (last block only).
 template <class T>
@@ -233,8 +245,8 @@ __device__ void finish_grid_reduction(const ArgView &a, const LoopParams &lp, in
 
 template <class K, class Sig> struct Exec;
 
-template <class K, class... P>
-struct Exec<K, void (K::*)(P...) const> {
+template <class K, class C, class... P>
+struct Exec<K, void (C::*)(P...) const> {
   using Seq = std::index_sequence_for<P...>;
   using Tup = SlotTuple<Seq, Slot<std::decay_t<P>>...>;
 
@@ -256,7 +268,7 @@ struct Exec<K, void (K::*)(P...) const> {
   __device__ static __forceinline__ void finish_one(Tup &t, const LoopParams &lp, double *smem, int nblocks) {
     using PT = std::decay_t<std::tuple_element_t<I, std::tuple<P...>>>;
     using RT = typename RedElem<PT>::type;
-    if constexpr (!std::is_void<RT>::value && !std::is_const<RT>::value) {
+    if constexpr (!std::is_void<RT>::value) {
       get_leaf<I, Slot<PT>>(t).finish(lp.a[I], lp, reinterpret_cast<RT *>(smem), nblocks);
     }
   }
@@ -269,8 +281,8 @@ struct Exec<K, void (K::*)(P...) const> {
   __device__ static __forceinline__ void grid_finish_one(const LoopParams &lp, double *smem, int nblocks) {
     using PT = std::decay_t<std::tuple_element_t<I, std::tuple<P...>>>;
     using RT = typename RedElem<PT>::type;
-    if constexpr (!std::is_void<RT>::value && !std::is_const<RT>::value) {
-      if (lp.a[I].kind == ARG_REDUCE) finish_grid_reduction<RT>(lp.a[I], lp, nblocks, reinterpret_cast<RT *>(smem));
+    if constexpr (!std::is_void<RT>::value) {
+      finish_grid_reduction<RT>(lp.a[I], lp, nblocks, reinterpret_cast<RT *>(smem));
     }
   }
 };
@@ -288,11 +300,17 @@ __global__ void __launch_bounds__(256) exec_loop(const __grid_constant__ LoopPar
   const int nz = lp.end[2] - lp.start[2];
   const long long nrows = (long long)ny * nz;
   if (x < lp.end[0]) {
-    for (long long r = (long long)blockIdx.y * blockDim.y + threadIdx.y; r < nrows;
-         r += (long long)gridDim.y * blockDim.y) {
-      const int y = lp.start[1] + (int)(r % ny);
-      const int z = lp.start[2] + (int)(r / ny);
-      E::call(k, t, lp, x, y, z, typename E::Seq{});
+    if (nz == 1) {
+#pragma unroll 2
+      for (int y = lp.start[1] + blockIdx.y * blockDim.y + threadIdx.y; y < lp.end[1]; y += gridDim.y * blockDim.y)
+        E::call(k, t, lp, x, y, lp.start[2], typename E::Seq{});
+    } else {
+      for (long long r = (long long)blockIdx.y * blockDim.y + threadIdx.y; r < nrows;
+           r += (long long)gridDim.y * blockDim.y) {
+        const int y = lp.start[1] + (int)(r % ny);
+        const int z = lp.start[2] + (int)(r / ny);
+        E::call(k, t, lp, x, y, z, typename E::Seq{});
+      }
     }
   }
   if (lp.nred == 0) return;
@@ -314,19 +332,21 @@ __global__ void __launch_bounds__(256) exec_loop(const __grid_constant__ LoopPar
 }
 
 // Host-side description of a kernel's parameter list, used to validate args
-// at enqueue time: 'A' accessor, 'p' non-const pointer, 'c' const pointer;
-// elem is the element size in bytes.
+// at enqueue time: 'A' accessor, 'R' reduction (ndim = width), 'I' index,
+// 'p' non-const pointer, 'c' const pointer; elem is the element size in bytes.
 struct ParamInfo { char cls; int elem; int ndim; };
 
 template <class P> struct ParamDesc;
 template <class T> struct ParamDesc<ACC2<T>> { static ParamInfo get() { return {'A', (int)sizeof(T), 2}; } };
 template <class T> struct ParamDesc<ACC3<T>> { static ParamInfo get() { return {'A', (int)sizeof(T), 3}; } };
 template <class T> struct ParamDesc<T *> { static ParamInfo get() { return {'p', (int)sizeof(T), 0}; } };
+template <class T, int N> struct ParamDesc<RED<T, N>> { static ParamInfo get() { return {'R', (int)sizeof(T), N}; } };
+template <> struct ParamDesc<IDX> { static ParamInfo get() { return {'I', 4, 0}; } };
 template <class T> struct ParamDesc<const T *> { static ParamInfo get() { return {'c', (int)sizeof(T), 0}; } };
 
 template <class Sig> struct SigInfo;
-template <class K, class... P>
-struct SigInfo<void (K::*)(P...) const> {
+template <class C, class... P>
+struct SigInfo<void (C::*)(P...) const> {
   static constexpr int n = sizeof...(P);
   static void fill(ParamInfo *out) {
     ParamInfo tmp[] = {ParamDesc<std::decay_t<P>>::get()..., ParamInfo{0, 0, 0}};

@@ -295,7 +295,8 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         break;
       case ARG_REDUCE: {
         Reduction &r = reduction(a.red);
-        require(p.cls == 'p', E_ARG, "loop " + loop->kernel + ": reduction arg must bind to a non-const pointer");
+        require(p.cls == 'R', E_ARG, "loop " + loop->kernel + ": reduction arg must bind to a RED<> parameter");
+        require(a.dim <= p.ndim, E_ARG, "reduction " + r.name + " wider than the kernel's accumulator");
         require(p.elem == r.elem, E_ARG, "reduction " + r.name + " type does not match the kernel parameter");
         require(a.dim <= OPSB_MAX_RED_DIM && a.dim * r.elem <= r.size, E_ARG, "reduction " + r.name + " too wide");
         require(nred < OPSB_MAX_REDUCE_ARGS, E_ARG, "too many reductions in one loop");
@@ -309,7 +310,7 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         break;
       }
       case ARG_IDX:
-        require(p.elem == 4 && p.cls != 'A', E_ARG, "ops_arg_idx must bind to an int pointer");
+        require(p.cls == 'I', E_ARG, "ops_arg_idx must bind to an IDX parameter");
         break;
       default:
         throw Error(E_ARG, "unknown arg kind");
@@ -405,8 +406,23 @@ void Runtime::set_timing(int on) {
   timing_on_ = on;
 }
 
-void Runtime::timed_launch_begin(const std::string &name) {
+double Runtime::alg_bytes(const Desc &d) const {
+  double total = 0.0;
+  for (const Arg &a : d.args) {
+    if (a.kind != ARG_DAT || !a.opt) continue;
+    const Dat &dt = *dats_[a.dat];
+    const Stencil &st = stencils_[a.stencil];
+    double pts = 1.0;
+    for (int k = 0; k < d.dim; k++)
+      if (st.stride[k]) pts *= std::max(0, d.range[2 * k + 1] - d.range[2 * k]);
+    total += pts * dt.elem_size * ((a.acc == ACC_RW || a.acc == ACC_INC) ? 2 : 1);
+  }
+  return total;
+}
+
+void Runtime::timed_launch_begin(const std::string &name, double bytes) {
   if (!timing_on_) return;
+  cur_bytes_ = bytes;
   if (event_pool_.empty()) {
     for (int i = 0; i < 64; i++) {
       cudaEvent_t e;
@@ -432,7 +448,7 @@ void Runtime::timed_launch_end() {
   cudaEvent_t e = event_pool_.back();
   event_pool_.pop_back();
   OPSB_CUDA(cudaEventRecord(e, stream_));
-  pending_.push_back({cur_name_, cur_ev_, e});
+  pending_.push_back({cur_name_, cur_ev_, e, cur_bytes_});
   cur_ev_ = nullptr;
   if (pending_.size() > 4096) collect_timing();
 }
@@ -446,6 +462,7 @@ void Runtime::collect_timing() {
     KTime &k = ktimes_[p.name];
     k.launches++;
     k.ms += ms;
+    k.bytes += p.bytes;
     event_pool_.push_back(p.a);
     event_pool_.push_back(p.b);
   }
@@ -488,7 +505,7 @@ void Runtime::launch_items(std::vector<Desc> &q) {
     long long nx = (long long)d.range[1] - d.range[0];
     long long nr = (long long)(d.range[3] - d.range[2]) * (d.range[5] - d.range[4]);
     if ((nx > 0 && nr > 0) || nred > 0) {
-      timed_launch_begin(d.loop->kernel);
+      timed_launch_begin(d.loop->kernel, timing_on_ ? alg_bytes(d) : 0.0);
       d.loop->launch(lp, g, b, stream_);
       OPSB_CUDA(cudaGetLastError());
       timed_launch_end();

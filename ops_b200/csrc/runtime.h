@@ -181,10 +181,12 @@ class Runtime {
   // runtime stream; graphs are bypassed while it is on).
   void set_timing(int on);
   void collect_timing();
-  struct KTime { long long launches = 0; double ms = 0.0; };
+  struct KTime { long long launches = 0; double ms = 0.0; double bytes = 0.0; };
   const std::map<std::string, KTime> &kernel_times() { collect_timing(); return ktimes_; }
   void clear_timing() { collect_timing(); ktimes_.clear(); }
-  void timed_launch_begin(const std::string &name);
+  void timed_launch_begin(const std::string &name, double alg_bytes = 0.0);
+  // Compulsory bytes of one loop: each dat arg's points once, RW/INC twice.
+  double alg_bytes(const Desc &d) const;
   void timed_launch_end();
   void set_fusion(int on) { fusion_on_ = on; }
   int fusion_enabled() const { return fusion_on_; }
@@ -236,11 +238,12 @@ class Runtime {
   std::unordered_map<uint64_t, GraphEntry> graphs_;
   int graphs_on_ = 1;
   int timing_on_ = 0;
-  struct PendingTime { std::string name; cudaEvent_t a, b; };
+  struct PendingTime { std::string name; cudaEvent_t a, b; double bytes; };
   std::vector<PendingTime> pending_;
   std::vector<cudaEvent_t> event_pool_;
   std::map<std::string, KTime> ktimes_;
   std::string cur_name_;
+  double cur_bytes_ = 0.0;
   cudaEvent_t cur_ev_ = nullptr;
   int fusion_on_ = 1;
   long long kernels_launched_ = 0, graphs_launched_ = 0, loops_enqueued_ = 0;
@@ -300,6 +303,15 @@ struct LoopRegistrar {
   LoopRegistrar() { Runtime::register_loop(make_loop_info<K>(K::kname)); }
 };
 #define OPSB_REGISTER_LOOP(K) static ::opsb::LoopRegistrar<K> opsb_reg_##K
+
+// ops_par_loop by registered kernel name (what translated app code and the
+// C++ app drivers call; no template instantiation at the call site).
+inline void par_loop_named(const char *kernel, const char *name, int block, int dim, const int *range,
+                           std::initializer_list<Arg> args) {
+  const LoopInfo *li = Runtime::find_loop(kernel);
+  if (!li) throw Error(E_NOTFOUND, std::string("no registered loop kernel named ") + kernel);
+  Runtime::get().par_loop(li, name, block, dim, range, args.begin(), (int)args.size());
+}
 
 // ops_par_loop(kernel, name, block, dim, range, args...) for a functor K.
 template <class K>

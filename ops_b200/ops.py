@@ -211,6 +211,14 @@ def kernel_time(kernel):
     return n.value, ms.value
 
 
+def kernel_stats():
+    """{kernel name: (launches, total_ms, alg_bytes)} of the timed kernels."""
+    n = check(lib().ops_b200_kernel_stats(None, 0))
+    arr = (_lib.KernelStat * max(n, 1))()
+    check(lib().ops_b200_kernel_stats(arr, n))
+    return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms, arr[i].alg_bytes) for i in range(n)}
+
+
 def clear_kernel_timing():
     check(lib().ops_b200_clear_kernel_timing())
 

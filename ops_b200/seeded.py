@@ -39,3 +39,26 @@ def laplace_field(imax, jmax, seed):
     A = u01(seed, k)
     A[1:-1, 1:-1] = 0.0
     return np.ascontiguousarray(A)
+
+
+def clover_rectangles(x_cells, y_cells, seed, n=4, xmin=0.0, xmax=10.0, ymin=0.0, ymax=10.0):
+    """n seeded rectangles with corners on grid lines, density U[0.5, 2] and
+    energy U[1, 3]: rectangle i draws counters 8i..8i+5 of stream `seed`."""
+    states = []
+    for i in range(n):
+        u = u01(seed, np.arange(8 * i, 8 * i + 6, dtype=np.uint64))
+        w = max(1, int(x_cells * (0.05 + 0.25 * u[0])))
+        h = max(1, int(y_cells * (0.05 + 0.25 * u[1])))
+        x0 = int(u[2] * (x_cells - w))
+        y0 = int(u[3] * (y_cells - h))
+        dx = (xmax - xmin) / x_cells
+        dy = (ymax - ymin) / y_cells
+        states.append(dict(density=float(0.5 + 1.5 * u[4]), energy=float(1.0 + 2.0 * u[5]), geometry="rectangle",
+                           xmin=xmin + x0 * dx, xmax=xmin + (x0 + w) * dx, ymin=ymin + y0 * dy,
+                           ymax=ymin + (y0 + h) * dy))
+    return states
+
+
+def clover_config2_states(x_cells, y_cells, seed=2):
+    """Background rho=0.2, e=1.0 plus four seeded rectangles."""
+    return [dict(density=0.2, energy=1.0)] + clover_rectangles(x_cells, y_cells, seed)

@@ -48,5 +48,64 @@ def laplace():
         print("wrote", name)
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and len(sys.argv) == 1:
     laplace()
+
+
+# CloverLeaf decks: (name, x_cells, y_cells, end_step, rectangle seed)
+CLOVER_CASES = [
+    ("clover_64x64_s30", 64, 64, 30, 2),
+    ("clover_100x70_s25", 100, 70, 25, 5),
+]
+DUMP_FIELDS = ["density0", "density1", "energy0", "energy1", "pressure", "viscosity", "soundspeed", "xvel0",
+               "xvel1", "yvel0", "yvel1", "vol_flux_x", "vol_flux_y", "mass_flux_x", "mass_flux_y"]
+
+
+def run_reference_clover(deck_text, dump=False, threads=1, timeout=600):
+    """Runs the reference CloverLeaf build on a deck; returns (summaries, dts, dumps)."""
+    exe = oracle.reference_binary("cloverleaf")
+    if exe is None:
+        raise SystemExit("oracle/_ref/bin/cloverleaf missing: run oracle/build_ref.sh")
+    with tempfile.TemporaryDirectory() as td:
+        with open(os.path.join(td, "clover.in"), "w") as f:
+            f.write(deck_text)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        if dump:
+            env["ORACLE_DUMP_DIR"] = td
+        r = subprocess.run([exe], cwd=td, capture_output=True, text=True, timeout=timeout, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
+        out = open(os.path.join(td, "clover.out")).read()
+        summ = []
+        for line in out.splitlines():
+            if line.strip().startswith("step:"):
+                v = line.split()
+                summ.append([float(x) for x in v[1:9]])
+        dts = [float(l.split()[7]) for l in r.stdout.splitlines() if l.strip().startswith("Step ")]
+        dumps = {}
+        if dump:
+            for name in DUMP_FIELDS:
+                meta = open(os.path.join(td, name + ".meta")).read().split("\n")
+                size = [int(x) for x in meta[1].split()[1:]]
+                xpad = int(meta[4].split()[1])
+                a = np.fromfile(os.path.join(td, name + ".bin"), dtype=np.float64).reshape(size[1], size[0])
+                dumps[name] = a[:, :size[0] - xpad]
+    # columns: step, vol, mass, density, pressure, ie, ke, total
+    return np.array(summ), np.array(dts), dumps
+
+
+def clover():
+    from ops_b200 import apps, seeded
+    for name, nx, ny, steps, seed in CLOVER_CASES:
+        deck = apps.clover_deck(x_cells=nx, y_cells=ny, xmin=0.0, ymin=0.0, xmax=10.0, ymax=10.0,
+                                initial_timestep=0.04, timestep_rise=1.5, max_timestep=0.04, end_step=steps,
+                                summary_frequency=1, states=seeded.clover_config2_states(nx, ny, seed))
+        text = apps.clover_deck_text(deck)
+        summ, dts, dumps = run_reference_clover(text, dump=True)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, deck=text, summaries=summ, dts=dts, **{"f_" + k: v for k, v in dumps.items()})
+        print("wrote", path, summ.shape, len(dts))
+
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "clover":
+    clover()
