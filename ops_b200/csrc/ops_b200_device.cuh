@@ -290,7 +290,7 @@ struct Exec<K, void (C::*)(P...) const> {
 // The generic loop kernel. blockDim = (BX, BY); blocks tile x exactly and
 // stride over the remaining (y, z) rows.
 template <class K>
-__global__ void __launch_bounds__(256) exec_loop(const __grid_constant__ LoopParams lp) {
+__global__ void __launch_bounds__(256, 3) exec_loop(const __grid_constant__ LoopParams lp) {
   using E = Exec<K, decltype(&K::operator())>;
   typename E::Tup t;
   E::init_all(t, lp, typename E::Seq{});
