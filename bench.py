@@ -289,13 +289,14 @@ def bench_clover(args, world, rank, local, pg):
 
     peaks, peak_kind = load_peaks()
     O.ops_init(local, 0)
-    cells = CL_N * CL_N
+    N = args.grid or CL_N
+    cells = N * N
     K, W = args.steps, args.warmup
 
     barrier(pg, local)
     O.reset_counters()
     with ClockSampler(local) as cs:
-        summ, secs = apps.cloverleaf(clover_deck(W + K), warmup_steps=W)
+        summ, secs = apps.cloverleaf(clover_deck(W + K, N), warmup_steps=W)
     clocks = cs.summary()
     c = O.counters()
     barrier(pg, local)
@@ -305,7 +306,7 @@ def bench_clover(args, world, rank, local, pg):
     kp = min(K, 10)
     O.set_kernel_timing(1)
     O.clear_kernel_timing()
-    apps.cloverleaf(clover_deck(kp))
+    apps.cloverleaf(clover_deck(kp, N))
     stats = O.kernel_stats()
     O.set_kernel_timing(0)
     launches_per_step = sum(v[0] for v in stats.values()) / kp
@@ -317,7 +318,7 @@ def bench_clover(args, world, rank, local, pg):
     # e2e: the public C-ABI call from the host deck to host summaries, wall clock.
     barrier(pg, local)
     t0 = time.perf_counter()
-    summ_e2e, _ = apps.cloverleaf(clover_deck(K))
+    summ_e2e, _ = apps.cloverleaf(clover_deck(K, N))
     t1 = time.perf_counter()
     e2e_s = max_over_ranks(pg, t1 - t0, local)
 
@@ -334,7 +335,7 @@ def bench_clover(args, world, rank, local, pg):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (background rho=0.2 e=1.0 + 4 SplitMix64-seeded rectangles, seed 2)",
-        "config": {"workload": "cloverleaf2d_3840x3840_fp64", "grid": [CL_N, CL_N], "gamma": 1.4,
+        "config": {"workload": f"cloverleaf2d_{N}x{N}_fp64", "grid": [N, N], "gamma": 1.4,
                    "cell_update": "one cell advanced one hydro timestep",
                    "step": "timestep (ideal_gas, viscosity, CFL dt) + PdV + accelerate + flux_calc + advection"
                            " + reset_field + field_summary (5 FP64 sums read back)",
@@ -394,6 +395,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clover")
     ap.add_argument("--cpu-iters", type=int, default=100)
     ap.add_argument("--cpu-clover-steps", type=int, default=5)
+    ap.add_argument("--grid", type=int, default=None, help="clover grid edge (default 3840; smaller for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:
