@@ -191,6 +191,29 @@ typedef struct ops_b200_clover_deck {
 int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int warmup_steps, double *summaries,
                             int max_summaries, int *n_summaries, double *device_seconds, const char *dump_dir);
 
+/* ---- allocation-free sweep ----------------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory where they need a sweep (inside another
+ * framework's memory pool or arena, inside a stream capture that must not
+ * gain allocation nodes, or in latency-critical loops).
+ *
+ * One Jacobi sweep of the Laplace 5-point stencil, the arithmetic of loop
+ * kernel "laplace2d/apply_stencil": Anew = 0.25 * (A(+1,0) + A(-1,0) +
+ * A(0,-1) + A(0,+1)) over x in [0, imax), y in [0, jmax), and the maximum
+ * |Anew - A| written to *max_delta. A and Anew are device pointers to
+ * logical index (0,0) of fields with a one-cell halo and a row pitch of
+ * `pitch` doubles (>= imax + 2); max_delta is a device pointer; stream is a
+ * cudaStream_t (NULL = default stream). Nothing is allocated: the scratch is
+ * a fixed ~32 KiB __device__ array that every GPU loading this library holds
+ * until exit. imax and jmax above 65536 are rejected (OPS_B200_ERR_ARG).
+ * All calls share that array, so calls that can overlap on the GPU race and
+ * must be serialised by the caller. The first call on each device looks up
+ * the array's device address; make it before any stream capture. Errors are
+ * described by ops_b200_noalloc_last_error(). */
+int ops_b200_laplace_sweep_noalloc(int imax, int jmax, const double *A, double *Anew, long long pitch,
+                                   double *max_delta, void *stream);
+const char *ops_b200_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
