@@ -383,7 +383,150 @@ def reference_clover(args, world, rank):
     }
 
 
-WORKLOADS = {"laplace": (bench_laplace, reference_laplace), "clover": (bench_clover, reference_clover)}
+# ---------------------------------------------------------------------------
+# Batched tridiagonal ADI sweeps (ops_tridMultiDimBatch)
+# ---------------------------------------------------------------------------
+ADI_N = 256
+
+
+def adi_batch_shapes(seed=3, nblocks=64, lo=32, hi=192):
+    """64 blocks, each edge log-uniform in [32, 192] (numpy order z, y, x)."""
+    import numpy as np
+
+    from ops_b200 import seeded
+    u = seeded.u01(seed, np.arange(3 * nblocks, dtype=np.uint64)).reshape(nblocks, 3)
+    return [tuple(int(round(lo * (hi / lo) ** v)) for v in row) for row in u]
+
+
+def bench_adi(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    from ops_b200 import ops as O
+    from ops_b200 import seeded
+
+    peaks, peak_kind = load_peaks()
+    O.ops_init(local, 0)
+    dt = np.float64 if args.precision == "fp64" else np.float32
+    es = np.dtype(dt).itemsize
+    shapes = [(ADI_N,) * 3] if args.adi_case == "cube" else adi_batch_shapes()
+    sets = []
+    for i, shp in enumerate(shapes):
+        a, b, c, d = seeded.trid_system(shp, 0, 3 + i, dt)
+        t = [torch.from_numpy(v).cuda(local) for v in (a, b, c, d)] + [torch.zeros(shp, dtype=torch.from_numpy(a).dtype,
+                                                                               device=f"cuda:{local}")]
+        sets.append((shp, t))
+    unknowns = sum(int(np.prod(s)) for s, _ in sets)
+
+    def systems(inc):
+        out = []
+        for shp, t in sets:
+            out.append(dict(a=t[0].data_ptr(), b=t[1].data_ptr(), c=t[2].data_ptr(), d=t[3].data_ptr(),
+                            u=t[4].data_ptr() if inc else None, dims=list(reversed(shp)), pads=list(reversed(shp))))
+        return out
+
+    sx, sy, sz = systems(False), systems(False), systems(True)
+    stream = torch.cuda.current_stream(local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    sweep_ms = [0.0, 0.0, 0.0]
+
+    def step(timed=False):
+        if timed:
+            ev[0].record(stream)
+        O.trid_batch(es, 0, sx, stream.cuda_stream)
+        if timed:
+            ev[1].record(stream)
+        O.trid_batch(es, 1, sy, stream.cuda_stream)
+        if timed:
+            ev[2].record(stream)
+        O.trid_batch(es, 2, sz, stream.cuda_stream)
+        if timed:
+            ev[3].record(stream)
+
+    K, W = args.steps, args.warmup
+    for _ in range(W):
+        step()
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    O.reset_counters()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as cs:
+        t0.record(stream)
+        for _ in range(K):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize(local)
+    clocks = cs.summary()
+    launches = O.counters()["kernels"]
+    secs = max_over_ranks(pg, t0.elapsed_time(t1) * 1e-3, local)
+    # per-sweep event timing (separate pass)
+    for _ in range(min(K, 5)):
+        step(timed=True)
+        torch.cuda.synchronize(local)
+        for j in range(3):
+            sweep_ms[j] += ev[j].elapsed_time(ev[j + 1]) / min(K, 5)
+    dom = int(np.argmax(sweep_ms))
+    byt = [40.0 * es / 8, 40.0 * es / 8, 48.0 * es / 8]
+    achieved = byt[dom] * unknowns / (sweep_ms[dom] * 1e-3) / 1e9
+    # e2e: host arrays in, three sweeps, solution out
+    host = [(shp, [x.cpu().numpy() for x in t]) for shp, t in sets]
+    barrier(pg, local)
+    te0 = time.perf_counter()
+    for shp, hv in host:
+        dev = [torch.from_numpy(v).cuda(local) for v in hv]
+        s1 = [dict(a=dev[0].data_ptr(), b=dev[1].data_ptr(), c=dev[2].data_ptr(), d=dev[3].data_ptr(), u=None,
+                   dims=list(reversed(shp)), pads=list(reversed(shp)))]
+        s3 = [dict(s1[0], u=dev[4].data_ptr())]
+        O.trid_batch(es, 0, s1, stream.cuda_stream)
+        O.trid_batch(es, 1, s1, stream.cuda_stream)
+        O.trid_batch(es, 2, s3, stream.cuda_stream)
+        dev[4].cpu()
+    torch.cuda.synchronize(local)
+    e2e_s = max_over_ranks(pg, time.perf_counter() - te0, local)
+    h2d = sum(4 * int(np.prod(s)) * es for s, _ in host)
+    name = f"adi_{args.adi_case}_{args.precision}"
+    line = {
+        "metric": "cell-solves/s", "value": world * 3 * unknowns * K / secs, "unit": "unknowns solved/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": secs * 1e3 / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.precision.replace("fp", "f"),
+        "data": "synthetic (a=c=-lam, b=1+2lam, lam~U[0.1,1] per line, d~N(0,1))",
+        "config": {"workload": name, "blocks": len(shapes), "unknowns": unknowns,
+                   "step": "x sweep + y sweep + z sweep (_Inc into u)", "l2": "inputs larger than L2"
+                   if unknowns * es * 4 > 126e6 else "inputs fit in L2 (batch case)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": f"sweep {'xyz'[dom]}",
+                     "sweep_ms": sweep_ms, "alg_bytes_per_unknown": byt, "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": world * 3 * unknowns / e2e_s, "unit": "unknowns solved/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": unknowns * es},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import ctypes
+
+        import oracle
+        L = oracle.lib()
+        f = L.oracle_trid_batch_d if dt == np.float64 else L.oracle_trid_batch_s
+        tc = time.perf_counter()
+        for shp, hv in host:
+            dims = (ctypes.c_int * 3)(*reversed(shp))
+            a, b, c, d, u = [np.ascontiguousarray(v) for v in hv]
+            for sd, uu in ((0, None), (1, None), (2, u)):
+                f(a.ctypes.data, b.ctypes.data, c.ctypes.data, d.ctypes.data, None if uu is None else uu.ctypes.data,
+                  3, sd, dims, dims)
+        cs_ = time.perf_counter() - tc
+        line["cpu_baseline"] = {"value": 3 * unknowns / cs_, "unit": "unknowns solved/s", "cores": os.cpu_count(),
+                                "kind": "port", "sample": f"oracle Thomas (OpenMP over lines), one x+y+z step, {cs_:.2f} s"}
+    return line
+
+
+def reference_adi(args, world, rank):
+    return {"impl": "reference", "unavailable": "the reference's tridiagonal solver is the external Tridsolver"
+                                                " library, which is not vendored with the reference"}
+
+
+WORKLOADS = {"laplace": (bench_laplace, reference_laplace), "clover": (bench_clover, reference_clover),
+             "adi": (bench_adi, reference_adi)}
 
 
 def main():
@@ -396,10 +539,12 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=100)
     ap.add_argument("--cpu-clover-steps", type=int, default=5)
     ap.add_argument("--grid", type=int, default=None, help="clover grid edge (default 3840; smaller for profiling)")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64", help="adi workload precision")
+    ap.add_argument("--adi-case", choices=["cube", "batch"], default="cube", help="adi: 256^3 block or 64 uneven blocks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 200 if args.workload in ("laplace", "clover") else 20
+        args.steps = {"laplace": 200, "clover": 200, "adi": 50}.get(args.workload, 20)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_setup(args)

@@ -191,6 +191,37 @@ typedef struct ops_b200_clover_deck {
 int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int warmup_steps, double *summaries,
                             int max_summaries, int *n_summaries, double *device_seconds, const char *dump_dir);
 
+/* ---- batched tridiagonal solves ------------------------------------------
+ * ops_tridMultiDimBatch / ops_tridMultiDimBatch_Inc
+ * (ops/c/include/ops_tridiag.h, ops/c/src/tridiag/ops_tridiag.cpp:78-249):
+ * solve a_i x_{i-1} + b_i x_i + c_i x_{i+1} = d_i along dimension `solvedim`
+ * for every line of `range` (2*ndim entries). The plain form overwrites d
+ * with x; _Inc adds x to u and leaves d untouched. a, b, c, d (and u) are dat
+ * handles of one type ("double" or "float") and one shape. The reference's
+ * ops_tridsolver_params only steer the MPI strategies and are not needed on
+ * one GPU. Queued loops are flushed first. */
+int ops_b200_tridMultiDimBatch(int ndim, int solvedim, const int *range, int a, int b, int c, int d);
+int ops_b200_tridMultiDimBatch_Inc(int ndim, int solvedim, const int *range, int a, int b, int c, int d, int u);
+
+/* One strided system set, as Tridsolver's trid{D,S}mtsvStridedBatch[Inc]
+ * takes it (call sites ops/c/src/tridiag/ops_tridiag.cpp:126,140,219,236):
+ * device pointers to the first solved element, the solved extents `dims`
+ * and the allocated extents `pads` (element (i,j,k) at
+ * i + j*pads[0] + k*pads[0]*pads[1]); u != NULL selects the Inc form. */
+typedef struct ops_b200_trid_system {
+  const void *a, *b, *c;
+  void *d, *u;
+  int ndim;
+  int dims[3];
+  int pads[3];
+} ops_b200_trid_system;
+
+/* Solves all lines along `solvedim` of `nsys` system sets, of any shapes, in
+ * one persistent launch (elem_size 8 = double, 4 = float) on `stream`
+ * (cudaStream_t, NULL = default stream). Lines along x up to 512 points and
+ * along y/z up to 256 points are supported. */
+int ops_b200_trid_batch(int elem_size, int solvedim, int nsys, const ops_b200_trid_system *systems, void *stream);
+
 /* ---- allocation-free sweep ----------------------------------------------
  * No counterpart in the reference: an extra entry point for callers that
  * cannot allocate device memory where they need a sweep (inside another

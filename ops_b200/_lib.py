@@ -31,6 +31,12 @@ class Arg(ctypes.Structure):
                 ("reduction", ctypes.c_int), ("elem_size", ctypes.c_int), ("gbl", ctypes.c_void_p)]
 
 
+class TridSystem(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("c", ctypes.c_void_p), ("d", ctypes.c_void_p),
+                ("u", ctypes.c_void_p), ("ndim", ctypes.c_int), ("dims", ctypes.c_int * 3),
+                ("pads", ctypes.c_int * 3)]
+
+
 class KernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 96), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double),
                 ("alg_bytes", ctypes.c_double)]
@@ -104,6 +110,9 @@ def _declare(L):
         "ops_b200_kernel_stats": ([P, i], i),
         "ops_b200_app_laplace2d": ([i, i, i, i, P, P, P, P], i),
         "ops_b200_app_cloverleaf": ([P, i, P, i, P, P, cp], i),
+        "ops_b200_tridMultiDimBatch": ([i, i, P, i, i, i, i], i),
+        "ops_b200_tridMultiDimBatch_Inc": ([i, i, P, i, i, i, i, i], i),
+        "ops_b200_trid_batch": ([i, i, i, P, P], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

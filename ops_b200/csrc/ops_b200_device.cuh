@@ -40,29 +40,30 @@ template <class T> __host__ __device__ __forceinline__ T op_max(T a, T b) { retu
 __host__ __device__ __forceinline__ double op_sign(double a, double b) { return (b < 0.0) ? (a * (-1)) : a; }
 
 // 2D accessor: p points at the current point; (i, j) is a stencil offset.
+// As in the reference's ACC<T> (ops/c/include/ops_lib_core.h:1525-1556) an
+// offset is i + j * (row pitch) whatever the stencil's stride: a dat that is
+// one point wide along a dimension is only ever offset along the other.
 template <class T>
 struct ACC2 {
   T *p;
-  int sx, sy;
+  int sy;
   ACC2() = default;
-  __device__ __forceinline__ ACC2(T *p_, int sx_, int sy_) : p(p_), sx(sx_), sy(sy_) {}
-  __device__ __forceinline__ T &operator()(int i, int j) { return p[i * sx + j * sy]; }
+  __device__ __forceinline__ ACC2(T *p_, int sy_) : p(p_), sy(sy_) {}
+  __device__ __forceinline__ T &operator()(int i, int j) { return p[i + j * sy]; }
   // Read-only view (the kernel's const ACC<T>& arguments): non-coherent loads.
-  __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (i * sx + j * sy)); }
+  __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (i + j * sy)); }
 };
 
 // 3D accessor.
 template <class T>
 struct ACC3 {
   T *p;
-  int sx, sy, sz;
+  int sy, sz;
   ACC3() = default;
-  __device__ __forceinline__ ACC3(T *p_, int sx_, int sy_, int sz_) : p(p_), sx(sx_), sy(sy_), sz(sz_) {}
-  __device__ __forceinline__ T &operator()(int i, int j, int k) {
-    return p[i * sx + (long long)j * sy + (long long)k * sz];
-  }
+  __device__ __forceinline__ ACC3(T *p_, int sy_, int sz_) : p(p_), sy(sy_), sz(sz_) {}
+  __device__ __forceinline__ T &operator()(int i, int j, int k) { return p[i + j * sy + (long long)k * sz]; }
   __device__ __forceinline__ T operator()(int i, int j, int k) const {
-    return __ldg(p + (i * sx + (long long)j * sy + (long long)k * sz));
+    return __ldg(p + (i + j * sy + (long long)k * sz));
   }
 };
 
@@ -85,13 +86,13 @@ struct IDX {
 // One loop argument as the device sees it.
 struct ArgView {
   char *ptr;        // DAT: logical origin of the dat; GBL: device copy; REDUCE: handle slot
-  int sx, sy, sz;   // element strides (0 along a dimension the stencil does not stride)
+  int sx, sy, sz;   // element strides of the point's base (0 where the stencil does not stride)
+  int ay, az;       // accessor strides: row pitch and plane size of the dat
   int kind;         // ArgKind
   int acc;          // Access
   int dim;          // components (reduction width for REDUCE)
   int red_index;    // REDUCE: index among this loop's reduction args
   int first;        // REDUCE: 1 when the handle starts from the identity in this loop
-  int pad_;
 };
 
 struct LoopParams {
@@ -162,7 +163,7 @@ struct Slot<ACC2<T>> {
   ACC2<T> acc;
   __device__ __forceinline__ void init(const ArgView &) {}
   __device__ __forceinline__ ACC2<T> &at(const ArgView &a, int x, int y, int) {
-    acc = ACC2<T>(reinterpret_cast<T *>(a.ptr) + (long long)x * a.sx + (long long)y * a.sy, a.sx, a.sy);
+    acc = ACC2<T>(reinterpret_cast<T *>(a.ptr) + (x * a.sx + y * a.sy), a.ay);
     return acc;
   }
   template <class S> __device__ __forceinline__ void finish(const ArgView &, const LoopParams &, S *, int) {}
@@ -173,8 +174,7 @@ struct Slot<ACC3<T>> {
   ACC3<T> acc;
   __device__ __forceinline__ void init(const ArgView &) {}
   __device__ __forceinline__ ACC3<T> &at(const ArgView &a, int x, int y, int z) {
-    acc = ACC3<T>(reinterpret_cast<T *>(a.ptr) + (long long)x * a.sx + (long long)y * a.sy + (long long)z * a.sz,
-                  a.sx, a.sy, a.sz);
+    acc = ACC3<T>(reinterpret_cast<T *>(a.ptr) + (x * a.sx + y * a.sy + (long long)z * a.sz), a.ay, a.az);
     return acc;
   }
   template <class S> __device__ __forceinline__ void finish(const ArgView &, const LoopParams &, S *, int) {}
@@ -290,7 +290,7 @@ struct Exec<K, void (C::*)(P...) const> {
 // The generic loop kernel. blockDim = (BX, BY); blocks tile x exactly and
 // stride over the remaining (y, z) rows.
 template <class K>
-__global__ void __launch_bounds__(256, 3) exec_loop(const __grid_constant__ LoopParams lp) {
+__global__ void __launch_bounds__(256) exec_loop(const __grid_constant__ LoopParams lp) {
   using E = Exec<K, decltype(&K::operator())>;
   typename E::Tup t;
   E::init_all(t, lp, typename E::Seq{});

@@ -284,6 +284,8 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         stencil(a.stencil);
         require(p.cls == 'A', E_ARG, "loop " + loop->kernel + ": arg " + std::to_string(i) + " is a dat but the kernel expects a pointer");
         require(p.elem == dt.type_size, E_ARG, "loop " + loop->kernel + ": dat " + dt.name + " element size mismatch");
+        require(dt.dim == 1, E_UNSUPPORTED, "dat " + dt.name + ": multi-component dats are not supported by loop kernels");
+        require(dt.plane < (1LL << 31), E_UNSUPPORTED, "dat " + dt.name + " has a plane of 2^31 elements or more");
         require(dt.block == blk, E_ARG, "dat " + dt.name + " is declared on another block");
         require(dt.locked == 0, E_STATE, "dat " + dt.name + " is used in a loop while its raw pointer is held (ops_lib_core.cpp:2321)");
         if (a.acc != ACC_READ) dt.host.clear();
@@ -361,9 +363,11 @@ void Runtime::build_params(const Desc &d, LoopParams &lp, int *nred_out) {
         const Dat &dt = *dats_[a.dat];
         const Stencil &st = stencils_[a.stencil];
         v.ptr = a.opt ? dt.origin_ptr() : nullptr;
-        v.sx = st.stride[0] ? dt.dim : 0;
-        v.sy = st.stride[1] ? (int)(dt.pitch * dt.dim) : 0;
-        v.sz = st.stride[2] ? (int)(dt.plane * dt.dim) : 0;
+        v.sx = st.stride[0] ? 1 : 0;
+        v.sy = st.stride[1] ? (int)dt.pitch : 0;
+        v.sz = st.stride[2] ? (int)dt.plane : 0;
+        v.ay = (int)dt.pitch;
+        v.az = (int)dt.plane;
         break;
       }
       case ARG_GBL:

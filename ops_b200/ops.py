@@ -229,3 +229,29 @@ def reset_counters():
 
 __all__ = [n for n in dir() if n.startswith("ops_")] + ["OpsError", "set_option", "counters", "reset_counters",
                                                           "set_kernel_timing", "kernel_time", "clear_kernel_timing"]
+
+
+def ops_tridMultiDimBatch(ndim, solvedim, rng, a, b, c, d, params=None):
+    """ops_tridMultiDimBatch: solve along `solvedim` over `rng`, result in d."""
+    check(lib().ops_b200_tridMultiDimBatch(ndim, solvedim, _iarr(rng), a.index, b.index, c.index, d.index))
+
+
+def ops_tridMultiDimBatch_Inc(ndim, solvedim, rng, a, b, c, d, u, params=None):
+    """ops_tridMultiDimBatch_Inc: solve along `solvedim` over `rng`, add the result to u."""
+    check(lib().ops_b200_tridMultiDimBatch_Inc(ndim, solvedim, _iarr(rng), a.index, b.index, c.index, d.index,
+                                               u.index))
+
+
+def trid_batch(elem_size, solvedim, systems, stream=None):
+    """Raw strided batch over device pointers; `systems` is a list of dicts with
+    a, b, c, d, u (ints, u may be None), dims and pads (lists)."""
+    arr = (_lib.TridSystem * max(1, len(systems)))()
+    for i, s in enumerate(systems):
+        t = arr[i]
+        t.a, t.b, t.c, t.d = s["a"], s["b"], s["c"], s["d"]
+        t.u = s.get("u")
+        t.ndim = len(s["dims"])
+        for k in range(3):
+            t.dims[k] = s["dims"][k] if k < t.ndim else 1
+            t.pads[k] = s["pads"][k] if k < t.ndim else 1
+    check(lib().ops_b200_trid_batch(elem_size, solvedim, len(systems), arr, stream))

@@ -62,3 +62,28 @@ def clover_rectangles(x_cells, y_cells, seed, n=4, xmin=0.0, xmax=10.0, ymin=0.0
 def clover_config2_states(x_cells, y_cells, seed=2):
     """Background rho=0.2, e=1.0 plus four seeded rectangles."""
     return [dict(density=0.2, energy=1.0)] + clover_rectangles(x_cells, y_cells, seed)
+
+
+def normal(seed, k):
+    """Standard normal doubles (Box-Muller on counter pairs 2k, 2k+1)."""
+    k = np.asarray(k, dtype=np.uint64)
+    u1 = u01(seed, 2 * k)
+    u2 = u01(seed, 2 * k + np.uint64(1))
+    return np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * np.pi * u2)
+
+
+def trid_system(shape, solvedim, seed, dtype=np.float64):
+    """ADI test systems (config 3): per line a = c = -lam, b = 1 + 2 lam with
+    lam ~ U[0.1, 1], d ~ N(0, 1). `shape` is numpy order (z, y, x)."""
+    nd = len(shape)
+    ax = nd - 1 - solvedim                      # numpy axis of the solve dimension
+    lshape = list(shape)
+    lshape[ax] = 1
+    nlines = int(np.prod(lshape))
+    lam = uniform(seed, np.arange(nlines, dtype=np.uint64), 0.1, 1.0).reshape(lshape)
+    lam = np.broadcast_to(lam, shape)
+    a = (-lam).astype(dtype)
+    c = (-lam).astype(dtype)
+    b = (1.0 + 2.0 * lam).astype(dtype)
+    d = normal(seed + 1, np.arange(int(np.prod(shape)), dtype=np.uint64)).reshape(shape).astype(dtype)
+    return np.ascontiguousarray(a), np.ascontiguousarray(b), np.ascontiguousarray(c), np.ascontiguousarray(d)

@@ -86,5 +86,9 @@ def _declare(L):
             f.restype = res
 
 
-# Declarations added by the other oracle modules: (name, argtypes, restype).
-_EXTRA_DECLS = []
+# Declarations of the other oracle modules: (name, argtypes, restype).
+_P = ctypes.c_void_p
+_EXTRA_DECLS = [
+    ("oracle_trid_batch_d", [_P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int, _P, _P], None),
+    ("oracle_trid_batch_s", [_P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int, _P, _P], None),
+]

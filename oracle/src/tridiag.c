@@ -47,13 +47,20 @@ static long line_offset(int ndim, int solvedim, const int *dims, const int *pads
   return off;
 }
 
+/* Lines are independent: OpenMP splits them over the host threads (the
+ * CPU baseline uses all cores; tests run it single-threaded or not, with
+ * identical results since each line is solved by one thread). */
 #define THOMAS_BODY(T)                                                                     \
   long stride, nlines;                                                                     \
   line_geometry(ndim, solvedim, dims, pads, &stride, &nlines);                             \
   const int n = dims[solvedim];                                                            \
+  _Pragma("omp parallel")                                                                  \
+  {                                                                                        \
   T *cp = (T *)malloc(sizeof(T) * (n > 0 ? n : 1));                                        \
   T *dp = (T *)malloc(sizeof(T) * (n > 0 ? n : 1));                                        \
-  for (long l = 0; l < nlines && n > 0; l++) {                                             \
+  _Pragma("omp for schedule(static)")                                                      \
+  for (long l = 0; l < nlines; l++) {                                                      \
+    if (n <= 0) continue;                                                                  \
     const long o = line_offset(ndim, solvedim, dims, pads, l);                             \
     cp[0] = c[o] / b[o];                                                                   \
     dp[0] = d[o] / b[o];                                                                   \
@@ -71,7 +78,8 @@ static long line_offset(int ndim, int solvedim, const int *dims, const int *pads
     }                                                                                      \
   }                                                                                        \
   free(cp);                                                                                \
-  free(dp);
+  free(dp);                                                                                \
+  }
 
 /* tridDmtsvStridedBatch / tridDmtsvStridedBatchInc (u != NULL). */
 void oracle_trid_batch_d(const double *a, const double *b, const double *c, double *d, double *u, int ndim,
