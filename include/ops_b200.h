@@ -191,6 +191,31 @@ typedef struct ops_b200_clover_deck {
 int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int warmup_steps, double *summaries,
                             int max_summaries, int *n_summaries, double *device_seconds, const char *dump_dir);
 
+/* TeaLeaf 2D implicit heat conduction (apps/c/TeaLeaf/diffuse.cpp:78-148,
+ * tea_solve.cpp:37-418). The deck holds the tea.in values the reference
+ * reads (apps/c/TeaLeaf/read_input.cpp:70-378); states use the CloverLeaf
+ * state record (velocities ignored). solver: 0 Jacobi, 1 CG;
+ * preconditioner: 0 none, 1 Jacobi diagonal (jac_diag); coefficient:
+ * 1 conductivity = density, 2 reciprocal density. */
+typedef struct ops_b200_tea_deck {
+  int x_cells, y_cells;
+  double xmin, ymin, xmax, ymax;
+  double initial_timestep, end_time;
+  int end_step, summary_frequency;
+  int max_iters;
+  double eps;
+  int coefficient, preconditioner, solver, reflective_boundary, check_result;
+  int number_of_states;                   /* 1..24; state 0 is the background */
+  ops_b200_clover_state states[24];
+} ops_b200_tea_deck;
+
+/* Runs the deck. summaries: 6 doubles per field summary {step, time, volume,
+ * mass, internal energy, temperature}; solves: 4 doubles per timestep solve
+ * {iterations, initial residual, final error / initial residual, exact
+ * residual ratio or -1}. dump_dir as for CloverLeaf. */
+int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summaries, int max_summaries, int *n_summaries,
+                         double *solves, int max_solves, int *n_solves, double *device_seconds, const char *dump_dir);
+
 /* ---- batched tridiagonal solves ------------------------------------------
  * ops_tridMultiDimBatch / ops_tridMultiDimBatch_Inc
  * (ops/c/include/ops_tridiag.h, ops/c/src/tridiag/ops_tridiag.cpp:78-249):

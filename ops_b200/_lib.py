@@ -58,6 +58,16 @@ class CloverDeck(ctypes.Structure):
                 ("states", CloverState * 16)]
 
 
+class TeaDeck(ctypes.Structure):
+    _fields_ = [("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int), ("xmin", ctypes.c_double),
+                ("ymin", ctypes.c_double), ("xmax", ctypes.c_double), ("ymax", ctypes.c_double),
+                ("initial_timestep", ctypes.c_double), ("end_time", ctypes.c_double), ("end_step", ctypes.c_int),
+                ("summary_frequency", ctypes.c_int), ("max_iters", ctypes.c_int), ("eps", ctypes.c_double),
+                ("coefficient", ctypes.c_int), ("preconditioner", ctypes.c_int), ("solver", ctypes.c_int),
+                ("reflective_boundary", ctypes.c_int), ("check_result", ctypes.c_int),
+                ("number_of_states", ctypes.c_int), ("states", CloverState * 24)]
+
+
 _lib = None
 
 
@@ -110,6 +120,7 @@ def _declare(L):
         "ops_b200_kernel_stats": ([P, i], i),
         "ops_b200_app_laplace2d": ([i, i, i, i, P, P, P, P], i),
         "ops_b200_app_cloverleaf": ([P, i, P, i, P, P, cp], i),
+        "ops_b200_app_tealeaf": ([P, P, i, P, P, i, P, P, cp], i),
         "ops_b200_tridMultiDimBatch": ([i, i, P, i, i, i, i], i),
         "ops_b200_tridMultiDimBatch_Inc": ([i, i, P, i, i, i, i, i], i),
         "ops_b200_trid_batch": ([i, i, i, P, P], i),

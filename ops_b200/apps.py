@@ -93,3 +93,75 @@ def cloverleaf(deck, warmup_steps=0, dump_dir=None, max_summaries=100000):
                                         ctypes.byref(n), ctypes.byref(secs),
                                         dump_dir.encode() if dump_dir else None))
     return out[:n.value].copy(), secs.value
+
+
+# ---------------------------------------------------------------------------
+# TeaLeaf
+# ---------------------------------------------------------------------------
+# read_input.cpp:70-103 defaults (Jacobi, no preconditioner, conductivity).
+TEA_DEFAULTS = dict(x_cells=10, y_cells=10, xmin=0.0, ymin=0.0, xmax=100.0, ymax=100.0, initial_timestep=0.1,
+                    end_time=10.0, end_step=640000, summary_frequency=10, max_iters=1000, eps=1e-10,
+                    coefficient=1, preconditioner=0, solver=0, reflective_boundary=0, check_result=0)
+
+
+def tea_deck(**kw):
+    from ._lib import TeaDeck
+    d = TeaDeck()
+    vals = dict(TEA_DEFAULTS)
+    vals.update({k: v for k, v in kw.items() if k != "states"})
+    for k, v in vals.items():
+        setattr(d, k, v)
+    states = kw["states"]
+    d.number_of_states = len(states)
+    for i, s in enumerate(states):
+        st = d.states[i]
+        st.density, st.energy = s["density"], s["energy"]
+        g = s.get("geometry", 0)
+        st.geometry = GEOMETRY.get(g, g) if isinstance(g, str) else g
+        for k in ("xmin", "xmax", "ymin", "ymax", "radius"):
+            setattr(st, k, s.get(k, 0.0))
+    return d
+
+
+def tea_deck_text(deck):
+    """The deck as tea.in text for the reference build."""
+    g = lambda v: repr(float(v))
+    lines = ["*tea"]
+    for i in range(deck.number_of_states):
+        s = deck.states[i]
+        line = f" state {i + 1} density={g(s.density)} energy={g(s.energy)}"
+        if i > 0:
+            geo = {1: "rectangle", 2: "circle", 3: "point"}[s.geometry]
+            line += f" geometry={geo} xmin={g(s.xmin)} xmax={g(s.xmax)} ymin={g(s.ymin)} ymax={g(s.ymax)}"
+            if s.geometry == 2:
+                line += f" radius={g(s.radius)}"
+        lines.append(line)
+    lines += [f" x_cells={deck.x_cells}", f" y_cells={deck.y_cells}", f" xmin={g(deck.xmin)}", f" ymin={g(deck.ymin)}",
+              f" xmax={g(deck.xmax)}", f" ymax={g(deck.ymax)}", f" initial_timestep={g(deck.initial_timestep)}",
+              f" end_time={g(deck.end_time)}", f" end_step={deck.end_step}",
+              f" summary_frequency={deck.summary_frequency}", f" tl_max_iters={deck.max_iters}",
+              f" tl_eps={deck.eps!r}"]
+    lines.append(" tl_use_cg" if deck.solver == 1 else " tl_use_jacobi")
+    if deck.preconditioner == 1:
+        lines.append(" tl_preconditioner_type=jac_diag")
+    lines.append(" tl_coefficient_inverse_density" if deck.coefficient == 2 else " tl_coefficient_density")
+    if deck.reflective_boundary:
+        lines.append(" reflective_boundary")
+    if deck.check_result:
+        lines.append(" tl_check_result=1")
+    lines += ["*endtea", ""]
+    return "\n".join(lines)
+
+
+def tealeaf(deck, dump_dir=None, max_rows=100000):
+    """Runs a TeaLeaf deck. Returns (summaries[n, 6], solves[m, 4], device_seconds):
+    summaries: step, time, volume, mass, internal energy, temperature;
+    solves: iterations, initial residual, error ratio, exact residual ratio."""
+    out = np.zeros((max_rows, 6))
+    sv = np.zeros((max_rows, 4))
+    n, ns = ctypes.c_int(0), ctypes.c_int(0)
+    secs = ctypes.c_double(0.0)
+    check(lib().ops_b200_app_tealeaf(ctypes.byref(deck), out.ctypes.data, max_rows, ctypes.byref(n), sv.ctypes.data,
+                                     max_rows, ctypes.byref(ns), ctypes.byref(secs),
+                                     dump_dir.encode() if dump_dir else None))
+    return out[:n.value].copy(), sv[:ns.value].copy(), secs.value

@@ -73,7 +73,7 @@ struct Clover {
     dtinit = d.initial_timestep; dtmax = d.max_timestep; dtrise = d.timestep_rise;
     end_time = d.end_time; end_step = d.end_step; summary_frequency = d.summary_frequency;
     number_of_states = d.number_of_states;
-    if (number_of_states < 1 || number_of_states > kMaxStates) throw Error(E_ARG, "1..16 states are supported");
+    if (number_of_states < 1 || number_of_states > 16) throw Error(E_ARG, "1..16 states are supported");
     for (int i = 0; i < number_of_states; i++) {
       const ops_b200_clover_state &s = d.states[i];
       states[i].defined = 1;

@@ -16,7 +16,7 @@ enum {
 };
 
 enum { G_RECT = 1, G_CIRC = 2, G_POINT = 3 };
-constexpr int kMaxStates = 16;
+constexpr int kMaxStates = 24;
 
 struct state_type {
   int defined;

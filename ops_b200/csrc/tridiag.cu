@@ -42,28 +42,75 @@ struct Work {
   int sys, l0, l1;  // system, first line along dim 0, line index along dim 1
 };
 
+// Reciprocal by Newton-Raphson refinement (Newton's method for 1/x,
+// e = 1 - x r, r' = r + r e, which doubles the correct bits per step) from a
+// hardware approximation. It is accurate to about 1 ulp without the
+// out-of-line slow path of IEEE division, whose call would force the
+// per-thread coefficient arrays out of registers. Valid for finite normal
+// pivots with 2^-1000 < |x| < 2^1000; the solver's tolerance is relative
+// (1e-12 in FP64), not bit-exact.
+__device__ __forceinline__ float recip(float x) {
+  float r = __fdividef(1.0f, x);
+  const float e = fmaf(-x, r, 1.0f);
+  return fmaf(r, e, r);
+}
+__device__ __forceinline__ double recip(double x) {
+  // Scale x to [1, 2) by its exponent so the single-precision seed never
+  // over- or underflows, refine twice, then undo the scaling.
+  const long long bits = __double_as_longlong(x);
+  const long long ex = (bits >> 52) & 0x7ff;
+  const double m = __longlong_as_double((bits & ~(0x7ffLL << 52)) | (1023LL << 52));
+  double r = (double)__fdividef(1.0f, (float)m);
+  double e = fma(-m, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-m, r, 1.0);
+  r = fma(r, e, r);
+  return r * __longlong_as_double((2046LL - ex) << 52);
+}
+
 // Modified Thomas on rows [r0, r0+m) of one line (m >= 2): afterwards row i
 // reads  aa_i x_first + x_i + cc_i x_last = dd_i  for 0 < i < m-1, and the
 // end rows keep their outside couplings:
 //   aa_0 x_prev_last + x_first + cc_0 x_last   = dd_0
 //   aa_{m-1} x_first + x_last + cc_{m-1} x_next_first = dd_{m-1}
+// The last row's coefficients are returned in la, lc, ld as they are
+// produced (row m-1 is final after the forward sweep); reading them back
+// from the arrays with a run-time index would move the arrays to local memory.
 template <class T, int M>
 __device__ __forceinline__ void chunk_eliminate(const T *a, const T *b, const T *c, const T *d, long long ss, int m,
-                                                T (&aa)[M], T (&cc)[M], T (&dd)[M]) {
+                                                T (&aa)[M], T (&cc)[M], T (&dd)[M], T &la, T &lc, T &ld) {
+  // All of the chunk's loads are issued before any arithmetic, so each
+  // thread keeps 4*m independent requests in flight.
+  T bb[M];
 #pragma unroll
   for (int i = 0; i < M; i++) {
     if (i < m) {
-      const T ai = __ldg(a + i * ss), bi = __ldg(b + i * ss), ci = __ldg(c + i * ss), di = __ldg(d + i * ss);
+      aa[i] = __ldg(a + i * ss);
+      bb[i] = __ldg(b + i * ss);
+      cc[i] = __ldg(c + i * ss);
+      dd[i] = __ldg(d + i * ss);
+    }
+  }
+  // Forward sweep in place: (a_i, c_i, d_i) become (aa_i, cc_i, dd_i).
+#pragma unroll
+  for (int i = 0; i < M; i++) {
+    if (i < m) {
       if (i < 2) {
-        const T r = T(1) / bi;
-        aa[i] = ai * r;
-        cc[i] = ci * r;
-        dd[i] = di * r;
+        const T r = recip(bb[i]);
+        aa[i] = aa[i] * r;
+        cc[i] = cc[i] * r;
+        dd[i] = dd[i] * r;
       } else {
-        const T r = T(1) / (bi - ai * cc[i - 1]);
-        dd[i] = r * (di - ai * dd[i - 1]);
+        const T ai = aa[i];
+        const T r = recip(bb[i] - ai * cc[i - 1]);
+        dd[i] = r * (dd[i] - ai * dd[i - 1]);
         aa[i] = -r * ai * aa[i - 1];
-        cc[i] = r * ci;
+        cc[i] = r * cc[i];
+      }
+      if (i == m - 1) {
+        la = aa[i];
+        lc = cc[i];
+        ld = dd[i];
       }
     }
   }
@@ -76,7 +123,7 @@ __device__ __forceinline__ void chunk_eliminate(const T *a, const T *b, const T 
     }
   }
   if (m > 2) {
-    const T r = T(1) / (T(1) - cc[0] * aa[1]);
+    const T r = recip(T(1) - cc[0] * aa[1]);
     dd[0] = r * (dd[0] - cc[0] * dd[1]);
     aa[0] = r * aa[0];
     cc[0] = -r * cc[0] * cc[1];
@@ -93,7 +140,7 @@ __device__ __forceinline__ void reduced_solve(T *A, T *C, T *D, int n, int strid
   C[0] = cp;
   for (int k = 1; k < n; k++) {
     const T ak = A[k * stride];
-    const T r = T(1) / (T(1) - ak * cp);
+    const T r = recip(T(1) - ak * cp);
     cp = C[k * stride] * r;
     dp = (D[k * stride] - ak * dp) * r;
     C[k * stride] = cp;
@@ -115,14 +162,15 @@ __device__ __forceinline__ void chunk_store(T *d, T *u, long long ss, int m, con
   }
 }
 
-constexpr int kChunksStrided = 8;    // warps per CTA = chunks per line
 constexpr int kLinesContig = 8;      // warps per CTA = lines per CTA (lane = chunk)
 
-// Lines along y or z: threadIdx.x = line (neighbouring x), threadIdx.y = chunk.
-template <class T, int M>
+// Lines along y or z: threadIdx.x = line (neighbouring x), threadIdx.y =
+// chunk. L lines x K chunks = 256 threads: FP64 uses 16 x 16 so that a chunk
+// of a 256-point line (16 rows, three coefficient arrays) stays in registers.
+template <class T, int M, int L, int K>
 __global__ void __launch_bounds__(256) trid_strided_kernel(const Sys *__restrict__ sys, const Work *__restrict__ work,
                                                            int nwork) {
-  __shared__ T A[2 * kChunksStrided][32], C[2 * kChunksStrided][32], Dv[2 * kChunksStrided][32];
+  __shared__ T A[2 * K][L], C[2 * K][L], Dv[2 * K][L];
   const int lane = threadIdx.x, chunk = threadIdx.y;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const Work wk = work[w];
@@ -130,7 +178,7 @@ __global__ void __launch_bounds__(256) trid_strided_kernel(const Sys *__restrict
     const int line = wk.l0 + lane;
     const bool active = line < s.nl0;
     const int n = s.n;
-    const int kact = n >= 2 * kChunksStrided ? kChunksStrided : (n / 2 > 0 ? n / 2 : 1);
+    const int kact = n >= 2 * K ? K : (n / 2 > 0 ? n / 2 : 1);
     const int r0 = chunk * n / kact, r1 = (chunk + 1) * n / kact, m = r1 - r0;
     const long long off = (long long)line * s.s0 + (long long)wk.l1 * s.s1 + (long long)r0 * s.ss;
     const T *a = reinterpret_cast<const T *>(s.a) + off;
@@ -141,22 +189,23 @@ __global__ void __launch_bounds__(256) trid_strided_kernel(const Sys *__restrict
     T aa[M], cc[M], dd[M];
     const bool mine = active && chunk < kact;
     if (mine && n == 1) {
-      const T x = __ldg(d) / __ldg(b);
+      const T x = __ldg(d) * recip(__ldg(b));
       if (u) *u += x;
       else *d = x;
     }
     const bool work_here = mine && n > 1;
     if (work_here) {
-      chunk_eliminate<T, M>(a, b, c, d, s.ss, m, aa, cc, dd);
+      T la = T(0), lc = T(0), ld = T(0);
+      chunk_eliminate<T, M>(a, b, c, d, s.ss, m, aa, cc, dd, la, lc, ld);
       A[2 * chunk][lane] = chunk == 0 ? T(0) : aa[0];
       C[2 * chunk][lane] = cc[0];
       Dv[2 * chunk][lane] = dd[0];
-      A[2 * chunk + 1][lane] = aa[m - 1];
-      C[2 * chunk + 1][lane] = chunk == kact - 1 ? T(0) : cc[m - 1];
-      Dv[2 * chunk + 1][lane] = dd[m - 1];
+      A[2 * chunk + 1][lane] = la;
+      C[2 * chunk + 1][lane] = chunk == kact - 1 ? T(0) : lc;
+      Dv[2 * chunk + 1][lane] = ld;
     }
     __syncthreads();
-    if (chunk == 0 && active && n > 1) reduced_solve<T>(&A[0][lane], &C[0][lane], &Dv[0][lane], 2 * kact, 32);
+    if (chunk == 0 && active && n > 1) reduced_solve<T>(&A[0][lane], &C[0][lane], &Dv[0][lane], 2 * kact, L);
     __syncthreads();
     if (work_here) chunk_store<T, M>(d, u, s.ss, m, aa, cc, dd, Dv[2 * chunk][lane], Dv[2 * chunk + 1][lane]);
     __syncthreads();
@@ -186,19 +235,20 @@ __global__ void __launch_bounds__(256) trid_contig_kernel(const Sys *__restrict_
     T aa[M], cc[M], dd[M];
     const bool mine = active && chunk < kact;
     if (mine && n == 1) {
-      const T x = __ldg(d) / __ldg(b);
+      const T x = __ldg(d) * recip(__ldg(b));
       if (u) *u += x;
       else *d = x;
     }
     const bool work_here = mine && n > 1;
     if (work_here) {
-      chunk_eliminate<T, M>(a, b, c, d, s.ss, m, aa, cc, dd);
+      T la = T(0), lc = T(0), ld = T(0);
+      chunk_eliminate<T, M>(a, b, c, d, s.ss, m, aa, cc, dd, la, lc, ld);
       A[wl][2 * chunk] = chunk == 0 ? T(0) : aa[0];
       C[wl][2 * chunk] = cc[0];
       Dv[wl][2 * chunk] = dd[0];
-      A[wl][2 * chunk + 1] = aa[m - 1];
-      C[wl][2 * chunk + 1] = chunk == kact - 1 ? T(0) : cc[m - 1];
-      Dv[wl][2 * chunk + 1] = dd[m - 1];
+      A[wl][2 * chunk + 1] = la;
+      C[wl][2 * chunk + 1] = chunk == kact - 1 ? T(0) : lc;
+      Dv[wl][2 * chunk + 1] = ld;
     }
     __syncwarp();
     if (chunk == 0 && active && n > 1) reduced_solve<T>(&A[wl][0], &C[wl][0], &Dv[wl][0], 2 * kact, 1);
@@ -229,7 +279,7 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
   for (int i = 0; i < (int)systems.size(); i++) {
     const Sys &s = systems[i];
     if (s.n == 0) continue;
-    const int g = contig ? kLinesContig : 32;
+    const int g = contig ? kLinesContig : 16;
     for (int l1 = 0; l1 < s.nl1; l1++)
       for (int l0 = 0; l0 < s.nl0; l0 += g) work.push_back({i, l0, l1});
   }
@@ -253,17 +303,20 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
     // 32 chunks per line for n >= 64 (ceil(n/32) rows each), else n/2 chunks of at most 3 rows.
     const int need = std::max(3, (maxn + 31) / 32);
     dim3 blk(32, kLinesContig);
-    if (need <= 4) trid_contig_kernel<T, 4><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
-    else if (need <= 8) trid_contig_kernel<T, 8><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
+    // (no 4-row variant: with arrays that small the compiler turns the
+    // unrolled selects back into indexed accesses and spills them to local memory)
+    if (need <= 8) trid_contig_kernel<T, 8><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
     else if (need <= 16) trid_contig_kernel<T, 16><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
     else throw Error(E_UNSUPPORTED, "tridiagonal lines along x longer than 512 are not supported");
   } else {
-    // 8 chunks per line for n >= 16 (ceil(n/8) rows each), else n/2 chunks of at most 3 rows.
-    const int need = std::max(3, (maxn + kChunksStrided - 1) / kChunksStrided);
-    dim3 blk(32, kChunksStrided);
-    if (need <= 8) trid_strided_kernel<T, 8><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
-    else if (need <= 16) trid_strided_kernel<T, 16><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
-    else if (need <= 32) trid_strided_kernel<T, 32><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
+    // 16 lines x 16 chunks: a chunk of a 256-point line holds 16 rows, whose
+    // four coefficient arrays stay in registers. A chunk holds ceil(n/K) rows
+    // for n >= 2K, else at most 3.
+    constexpr int L = 16, K = 16;
+    const int need = std::max(3, (maxn + K - 1) / K);
+    dim3 blk(L, K);
+    if (need <= 8) trid_strided_kernel<T, 8, L, K><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
+    else if (need <= 16) trid_strided_kernel<T, 16, L, K><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
     else throw Error(E_UNSUPPORTED, "tridiagonal lines along y/z longer than 256 are not supported");
   }
   OPSB_CUDA(cudaGetLastError());

@@ -87,3 +87,23 @@ def trid_system(shape, solvedim, seed, dtype=np.float64):
     b = (1.0 + 2.0 * lam).astype(dtype)
     d = normal(seed + 1, np.arange(int(np.prod(shape)), dtype=np.uint64)).reshape(shape).astype(dtype)
     return np.ascontiguousarray(a), np.ascontiguousarray(b), np.ascontiguousarray(c), np.ascontiguousarray(d)
+
+
+def tea_config4_states(x_cells, y_cells, seed=4, n=16, xmin=0.0, xmax=10.0, ymin=0.0, ymax=10.0):
+    """Implicit-heat problem: background rho=1 with energy U[0,1] plus n
+    seeded rectangles (corners on grid lines) with rho log-uniform in
+    [0.1, 100] and energy U[0,1]; rectangle i draws counters 8i..8i+5."""
+    bg = float(u01(seed, np.array([10 ** 6], dtype=np.uint64))[0])
+    states = [dict(density=1.0, energy=bg)]
+    for i in range(n):
+        u = u01(seed, np.arange(8 * i, 8 * i + 6, dtype=np.uint64))
+        w = max(1, int(x_cells * (0.05 + 0.25 * u[0])))
+        h = max(1, int(y_cells * (0.05 + 0.25 * u[1])))
+        x0 = int(u[2] * (x_cells - w))
+        y0 = int(u[3] * (y_cells - h))
+        dx = (xmax - xmin) / x_cells
+        dy = (ymax - ymin) / y_cells
+        states.append(dict(density=float(10.0 ** (-1.0 + 3.0 * u[4])), energy=float(u[5]), geometry="rectangle",
+                           xmin=xmin + x0 * dx, xmax=xmin + (x0 + w) * dx, ymin=ymin + y0 * dy,
+                           ymax=ymin + (y0 + h) * dy))
+    return states

@@ -109,3 +109,80 @@ def clover():
 
 if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "clover":
     clover()
+
+
+# TeaLeaf decks: (name, deck keywords)
+TEA_CASES = [
+    ("tea_kat_jacobi", dict(x_cells=10, y_cells=10, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=10,
+                            max_iters=1000, eps=1e-15, solver=0, summary_frequency=10,
+                            states="tea.in")),
+    ("tea_cg_jacdiag_64", dict(x_cells=64, y_cells=64, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=2,
+                               max_iters=5000, eps=1e-10, solver=1, preconditioner=1, summary_frequency=1,
+                               states=("seeded", 64, 64, 4))),
+    ("tea_cg_plain_100x70", dict(x_cells=100, y_cells=70, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=1,
+                                 max_iters=5000, eps=1e-10, solver=1, preconditioner=0, summary_frequency=1,
+                                 states=("seeded", 100, 70, 7))),
+]
+TEA_DUMP = ["u", "energy1", "density"]
+
+
+def tea_states(spec):
+    from ops_b200 import seeded
+    if spec == "tea.in":  # apps/c/TeaLeaf/tea.in
+        return [dict(density=100.0, energy=0.0001),
+                dict(density=0.1, energy=25.0, geometry="rectangle", xmin=0.0, xmax=1.0, ymin=1.0, ymax=2.0),
+                dict(density=0.1, energy=0.1, geometry="rectangle", xmin=1.0, xmax=6.0, ymin=1.0, ymax=2.0),
+                dict(density=0.1, energy=0.1, geometry="rectangle", xmin=5.0, xmax=6.0, ymin=1.0, ymax=8.0),
+                dict(density=0.1, energy=0.1, geometry="rectangle", xmin=5.0, xmax=10.0, ymin=7.0, ymax=8.0)]
+    _, nx, ny, seed = spec
+    return seeded.tea_config4_states(nx, ny, seed)
+
+
+def run_reference_tea(deck_text, dump=False, threads=1, timeout=900):
+    exe = oracle.reference_binary("tealeaf")
+    if exe is None:
+        raise SystemExit("oracle/_ref/bin/tealeaf missing: run oracle/build_ref.sh")
+    with tempfile.TemporaryDirectory() as td:
+        with open(os.path.join(td, "tea.in"), "w") as f:
+            f.write(deck_text)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        if dump:
+            env["ORACLE_DUMP_DIR"] = td
+        r = subprocess.run([exe], cwd=td, capture_output=True, text=True, timeout=timeout, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
+        out = open(os.path.join(td, "tea.out")).read()
+        summ = [[float(x) for x in l.split()[1:7]] for l in out.splitlines() if l.strip().startswith("step:")]
+        iters = [int(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Iteration count")]
+        errs = [float(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Conduction error")]
+        dumps = {}
+        if dump:
+            # the reference pads TeaLeaf dat names with blanks (build_field.cpp:55-73)
+            files = {f[:-5].strip(): f[:-5] for f in os.listdir(td) if f.endswith(".meta")}
+            for name in TEA_DUMP:
+                fn = files[name]
+                meta = open(os.path.join(td, fn + ".meta")).read().split("\n")
+                size = [int(x) for x in meta[1].split()[1:]]
+                xpad = int(meta[4].split()[1])
+                a = np.fromfile(os.path.join(td, fn + ".bin"), dtype=np.float64).reshape(size[1], size[0])
+                dumps[name] = a[:, :size[0] - xpad]
+    # summary columns: step, vol, mass, density, ie, temp
+    return np.array(summ), np.array(iters), np.array(errs), dumps
+
+
+def tea():
+    from ops_b200 import apps
+    for name, kw in TEA_CASES:
+        kw = dict(kw)
+        kw["states"] = tea_states(kw["states"])
+        deck = apps.tea_deck(**kw)
+        text = apps.tea_deck_text(deck)
+        summ, iters, errs, dumps = run_reference_tea(text, dump=True)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, deck=text, summaries=summ, iters=iters, errors=errs,
+                            **{"f_" + k: v for k, v in dumps.items()})
+        print("wrote", path, summ.shape, iters, errs)
+
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "tea":
+    tea()
