@@ -10,6 +10,13 @@ configurations with synthetic seeded inputs:
   laplace  2D Laplace Jacobi, single block 4096x4096 FP64, 5-point stencil,
            seeded U[0,1) Dirichlet ring, interior 0; a step is one iteration
            (apply_stencil + max|delta| reduction read back + copy).
+  adi      batched tridiagonal x/y/z sweeps (ops_tridMultiDimBatch), one
+           256^3 block or 64 uneven blocks, FP64 or FP32; a step is the three
+           sweeps.
+  tea      implicit heat conduction (TeaLeaf CG, Jacobi preconditioner) on
+           4096x4096 with 16 seeded density rectangles; a step is one implicit
+           timestep solved to residual 1e-10, FP64 PCG beside FP32-inner /
+           FP64-refinement PCG; the metric is time to solution.
 
 `value` is device-timed (CUDA events on the runtime stream) with inputs
 resident in HBM; `e2e` times the same work through the public C-ABI call
@@ -24,6 +31,7 @@ host cores for the same workload and metric (rank 0 only).
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -525,8 +533,161 @@ def reference_adi(args, world, rank):
                                                 " library, which is not vendored with the reference"}
 
 
+# ---------------------------------------------------------------------------
+# Implicit heat conduction (TeaLeaf CG, jac_diag), 4096^2, eps 1e-10
+# ---------------------------------------------------------------------------
+TEA_N = 4096
+TEA_BYTES_FP64 = 120.0   # per cell-iteration: k_w 32 + k_ur 64 + k_p 24 (FP64 words)
+TEA_BYTES_FP32 = 60.0
+
+
+def tea_deck(steps, n=TEA_N, max_iters=200000, **kw):
+    from ops_b200 import apps, seeded
+    return apps.tea_deck(x_cells=n, y_cells=n, xmin=0.0, ymin=0.0, xmax=10.0, ymax=10.0, initial_timestep=0.004,
+                         end_step=steps, summary_frequency=0, max_iters=max_iters, eps=1e-10, solver=1,
+                         preconditioner=1, states=seeded.tea_config4_states(n, n, 4), **kw)
+
+
+def cpu_reference_tea(iters, threads, n=TEA_N):
+    """Seconds per CG iteration of the reference OpenMP TeaLeaf on the same
+    deck: two runs capped at 2 and 2 + iters iterations, wall-time difference."""
+    import oracle
+    from ops_b200 import apps
+    exe = oracle.reference_binary("tealeaf")
+    if exe is None:
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+    wall = []
+    for m in (2, 2 + iters):
+        with tempfile.TemporaryDirectory() as td:
+            with open(os.path.join(td, "tea.in"), "w") as f:
+                f.write(apps.tea_deck_text(tea_deck(1, n, max_iters=m)))
+            r = subprocess.run([exe], cwd=td, capture_output=True, text=True, env=env, timeout=1800, check=True)
+        wall.append([float(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Total Wall time")][-1])
+    return (wall[1] - wall[0]) / iters, wall
+
+
+def bench_tea(args, world, rank, local, pg):
+    import numpy as np
+
+    from ops_b200 import apps
+    from ops_b200 import ops as O
+
+    peaks, peak_kind = load_peaks()
+    O.ops_init(local, 0)
+    N = args.grid or TEA_N
+    cells = N * N
+    K, W = args.steps, args.warmup
+    td = tempfile.mkdtemp(prefix="tea_bench_")
+    barrier(pg, local)
+
+    def run(tag, **kw):
+        O.reset_counters()
+        with ClockSampler(local) as cs:
+            _, sv, _ = apps.tealeaf(tea_deck(W + K, N, **kw), dump_dir=os.path.join(td, tag))
+        return sv[W:], cs.summary(), O.counters()["kernels"]
+
+    os.makedirs(os.path.join(td, "plain"))
+    os.makedirs(os.path.join(td, "mixed"))
+    sp, clk_p, launches_p = run("plain", fused=1, true_residual_stop=1)
+    sm, clk_m, launches_m = run("mixed", fused=1, mixed=1, reliable_delta=args.reliable_delta)
+    up = np.fromfile(os.path.join(td, "plain", "u.bin"))
+    um = np.fromfile(os.path.join(td, "mixed", "u.bin"))
+    err_vs_fp64 = float(np.linalg.norm(um - up) / np.linalg.norm(up))
+    shutil.rmtree(td, ignore_errors=True)
+
+    t_plain = max_over_ranks(pg, float(np.median(sp[:, 6])), local)
+    t_mixed = max_over_ranks(pg, float(np.median(sm[:, 6])), local)
+    it_p = float(np.mean(sp[:, 0]))
+    it_m = float(np.mean(sm[:, 0]))
+    # roofline of the dominant chain: the FP32 inner iteration (k_w + k_ur + k_p)
+    per_it_m = t_mixed / max(it_m, 1.0)
+    per_it_p = t_plain / max(it_p, 1.0)
+    ach_m = TEA_BYTES_FP32 * cells / per_it_m / 1e9
+    ach_p = TEA_BYTES_FP64 * cells / per_it_p / 1e9
+
+    # e2e: one public C-ABI call (deck in, device set-up, one solve, summaries back), wall clock
+    barrier(pg, local)
+    te0 = time.perf_counter()
+    _, sv_e2e, _ = apps.tealeaf(tea_deck(1, N, fused=1, mixed=1, reliable_delta=args.reliable_delta))
+    e2e_s = max_over_ranks(pg, time.perf_counter() - te0, local)
+
+    line = {
+        "metric": "time to 1e-10 residual",
+        "value": t_mixed,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": t_mixed * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 outer / f32 inner",
+        "data": "synthetic (rho=1 background + 16 SplitMix64-seeded rectangles, rho log-uniform [0.1,100],"
+                " energy U[0,1], seed 4)",
+        "config": {"workload": f"tealeaf2d_cg_jacdiag_{N}x{N}", "grid": [N, N], "eps": 1e-10,
+                   "step": "one implicit timestep: coefficient set-up + solve to ||u0 - A u|| < 1e-10 ||r0|| +"
+                           " finalise", "l2": "inputs larger than L2 (fields of 134 MB FP64 / 67 MB FP32 x 8)",
+                   "reliable_delta": args.reliable_delta, "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": ach_m, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": ach_m / peaks["hbm_gbs"], "traffic": None,
+                     "kernel": "FP32 inner PCG iteration (k_w + k_ur + k_p)",
+                     "alg_bytes_per_cell_iteration": TEA_BYTES_FP32, "avg_iteration_ms": per_it_m * 1e3,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "fp64_iteration": {"achieved": ach_p, "frac": ach_p / peaks["hbm_gbs"],
+                                        "alg_bytes_per_cell_iteration": TEA_BYTES_FP64,
+                                        "avg_iteration_ms": per_it_p * 1e3}},
+        "plain_fp64_pcg": {"seconds": t_plain, "iterations": it_p,
+                           "tealeaf_stop_ratio": float(np.max(sp[:, 2])), "true_residual_ratio": float(np.max(sp[:, 4])),
+                           "cell_iterations_per_s": cells * it_p / t_plain, "gpu_launches": launches_p},
+        "mixed_pcg": {"seconds": t_mixed, "inner_iterations": it_m, "reliable_updates": float(np.mean(sm[:, 5])),
+                      "true_residual_ratio": float(np.max(sm[:, 4])), "rel_l2_error_vs_fp64_solution": err_vs_fp64,
+                      "speedup_vs_plain": t_plain / t_mixed},
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 13 * 8,
+                "note": "one C-ABI call: deck in, device set-up (generate), one mixed-precision solve, summaries back",
+                "solve_seconds": float(sv_e2e[0, 6])},
+        "gpu_launches": int(round(launches_m / (W + K))),
+        "clocks": clk_m,
+        "clocks_plain": clk_p,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        base = cpu_reference_tea(args.cpu_tea_iters, threads, N)
+        if base:
+            per_it = base[0]
+            line["cpu_baseline"] = {
+                "value": cells / per_it, "unit": "cell-iterations/s", "cores": threads, "kind": "reference",
+                "sample": f"reference TeaLeaf OpenMP build, same {N}^2 deck, CG capped at 2 and"
+                          f" {2 + args.cpu_tea_iters} iterations (wall {base[1][0]:.2f} s / {base[1][1]:.2f} s)",
+                "est_time_to_solution_s": per_it * it_p}
+    return line
+
+
+def reference_tea(args, world, rank):
+    threads = os.cpu_count() or 1
+    N = args.grid or TEA_N
+    base = cpu_reference_tea(args.cpu_tea_iters, threads, N)
+    if base is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/bin/tealeaf was not built"}
+    per_it, wall = base
+    v = per_it * args.tea_ref_iters
+    return {
+        "impl": "reference", "metric": "time to 1e-10 residual", "value": v, "unit": "s", "n_gpus": world,
+        "steps": 1, "warmup": 0, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (rho=1 background + 16 SplitMix64-seeded rectangles, seed 4)",
+        "config": {"workload": f"tealeaf2d_cg_jacdiag_{N}x{N}", "grid": [N, N], "eps": 1e-10},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference",
+                         "sample": f"reference OpenMP TeaLeaf, CG capped at 2 and {2 + args.cpu_tea_iters} iterations;"
+                                   f" seconds per iteration x {args.tea_ref_iters} iterations (the FP64 PCG"
+                                   f" count at this size)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 WORKLOADS = {"laplace": (bench_laplace, reference_laplace), "clover": (bench_clover, reference_clover),
-             "adi": (bench_adi, reference_adi)}
+             "adi": (bench_adi, reference_adi), "tea": (bench_tea, reference_tea)}
 
 
 def main():
@@ -541,10 +702,14 @@ def main():
     ap.add_argument("--grid", type=int, default=None, help="clover grid edge (default 3840; smaller for profiling)")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64", help="adi workload precision")
     ap.add_argument("--adi-case", choices=["cube", "batch"], default="cube", help="adi: 256^3 block or 64 uneven blocks")
+    ap.add_argument("--reliable-delta", type=float, default=0.1,
+                    help="tea: FP32 residual decrease between FP64 reliable updates")
+    ap.add_argument("--cpu-tea-iters", type=int, default=100, help="tea: CG iterations in the CPU sample")
+    ap.add_argument("--tea-ref-iters", type=int, default=0, help="tea: FP64 PCG iterations to solution (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"laplace": 200, "clover": 200, "adi": 50}.get(args.workload, 20)
+        args.steps = {"laplace": 200, "clover": 200, "adi": 50, "tea": 3}.get(args.workload, 20)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_setup(args)

@@ -196,7 +196,16 @@ int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int warmup_steps, 
  * reads (apps/c/TeaLeaf/read_input.cpp:70-378); states use the CloverLeaf
  * state record (velocities ignored). solver: 0 Jacobi, 1 CG;
  * preconditioner: 0 none, 1 Jacobi diagonal (jac_diag); coefficient:
- * 1 conductivity = density, 2 reciprocal density. */
+ * 1 conductivity = density, 2 reciprocal density.
+ * Beyond tea.in (no reference counterpart): fused = 1 runs each CG solve as
+ * the device-resident three-kernel iteration (alpha, beta and the stop test
+ * stay on the GPU; same per-cell arithmetic and stopping rule as the loop
+ * chain, which fused = 0 keeps); true_residual_stop = 1 (with fused) stops on
+ * ||r|| < eps * ||r0|| instead of TeaLeaf's sqrt|r.z|; mixed = 1 (with fused)
+ * runs the iteration in FP32 under FP64 reliable updates (the FP32 residual
+ * is replaced by u0 - A u computed in FP64 each time it has fallen by
+ * reliable_delta, search direction kept) and stops when the FP64 residual
+ * ||u0 - A u|| < eps * ||r0||. Fused solves need reflective_boundary = 0. */
 typedef struct ops_b200_tea_deck {
   int x_cells, y_cells;
   double xmin, ymin, xmax, ymax;
@@ -207,12 +216,19 @@ typedef struct ops_b200_tea_deck {
   int coefficient, preconditioner, solver, reflective_boundary, check_result;
   int number_of_states;                   /* 1..24; state 0 is the background */
   ops_b200_clover_state states[24];
+  int fused, mixed, true_residual_stop;
+  double reliable_delta;
 } ops_b200_tea_deck;
 
 /* Runs the deck. summaries: 6 doubles per field summary {step, time, volume,
- * mass, internal energy, temperature}; solves: 4 doubles per timestep solve
- * {iterations, initial residual, final error / initial residual, exact
- * residual ratio or -1}. dump_dir as for CloverLeaf. */
+ * mass, internal energy, temperature}; solves: OPS_B200_TEA_SOLVE_COLS
+ * doubles per timestep solve {iterations (as tea_solve.cpp:386 prints them),
+ * initial residual, final stopping quantity / initial residual, exact residual
+ * ratio (tl_check_result) or -1, true FP64 residual ratio ||u0 - A u|| / ||r0||
+ * at exit or -1 (fused solves compute it), reliable updates (mixed) or 0,
+ * device seconds of the solve (coefficient set-up through finalise)}.
+ * dump_dir as for CloverLeaf. */
+#define OPS_B200_TEA_SOLVE_COLS 7
 int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summaries, int max_summaries, int *n_summaries,
                          double *solves, int max_solves, int *n_solves, double *device_seconds, const char *dump_dir);
 

@@ -65,7 +65,9 @@ class TeaDeck(ctypes.Structure):
                 ("summary_frequency", ctypes.c_int), ("max_iters", ctypes.c_int), ("eps", ctypes.c_double),
                 ("coefficient", ctypes.c_int), ("preconditioner", ctypes.c_int), ("solver", ctypes.c_int),
                 ("reflective_boundary", ctypes.c_int), ("check_result", ctypes.c_int),
-                ("number_of_states", ctypes.c_int), ("states", CloverState * 24)]
+                ("number_of_states", ctypes.c_int), ("states", CloverState * 24),
+                ("fused", ctypes.c_int), ("mixed", ctypes.c_int), ("true_residual_stop", ctypes.c_int),
+                ("reliable_delta", ctypes.c_double)]
 
 
 _lib = None

@@ -101,7 +101,8 @@ def cloverleaf(deck, warmup_steps=0, dump_dir=None, max_summaries=100000):
 # read_input.cpp:70-103 defaults (Jacobi, no preconditioner, conductivity).
 TEA_DEFAULTS = dict(x_cells=10, y_cells=10, xmin=0.0, ymin=0.0, xmax=100.0, ymax=100.0, initial_timestep=0.1,
                     end_time=10.0, end_step=640000, summary_frequency=10, max_iters=1000, eps=1e-10,
-                    coefficient=1, preconditioner=0, solver=0, reflective_boundary=0, check_result=0)
+                    coefficient=1, preconditioner=0, solver=0, reflective_boundary=0, check_result=0,
+                    fused=0, mixed=0, true_residual_stop=0, reliable_delta=0.1)
 
 
 def tea_deck(**kw):
@@ -154,11 +155,13 @@ def tea_deck_text(deck):
 
 
 def tealeaf(deck, dump_dir=None, max_rows=100000):
-    """Runs a TeaLeaf deck. Returns (summaries[n, 6], solves[m, 4], device_seconds):
+    """Runs a TeaLeaf deck. Returns (summaries[n, 6], solves[m, 7], device_seconds):
     summaries: step, time, volume, mass, internal energy, temperature;
-    solves: iterations, initial residual, error ratio, exact residual ratio."""
+    solves: iterations, initial residual, error ratio, exact residual ratio,
+    true FP64 residual ratio (fused solves, else -1), reliable updates,
+    solve device seconds."""
     out = np.zeros((max_rows, 6))
-    sv = np.zeros((max_rows, 4))
+    sv = np.zeros((max_rows, 7))
     n, ns = ctypes.c_int(0), ctypes.c_int(0)
     secs = ctypes.c_double(0.0)
     check(lib().ops_b200_app_tealeaf(ctypes.byref(deck), out.ctypes.data, max_rows, ctypes.byref(n), sv.ctypes.data,

@@ -12,6 +12,7 @@
 
 #include "../../include/ops_b200.h"
 #include "clover_common.h"
+#include "heat_pcg.h"
 #include "runtime.h"
 
 namespace opsb {
@@ -48,12 +49,21 @@ struct Tea {
   int red_vol, red_mass, red_ie, red_temp;
 
   std::vector<double> summaries;  // step, time, vol, mass, ie, temp
-  std::vector<double> solves;     // per solve: iterations, initial residual, error ratio, exact error ratio
+  std::vector<double> solves;     // per solve: OPS_B200_TEA_SOLVE_COLS values
+  int fused = 0, mixed = 0, true_stop = 0;
+  double delta = 0.1;
+  heat::Solver solver;
+  cudaEvent_t ev_solve[2] = {nullptr, nullptr};
 
   explicit Tea(Runtime &rt) : r(rt) {
     memset(states, 0, sizeof(states));
     memset(&grid, 0, sizeof(grid));
     memset(&field, 0, sizeof(field));
+    for (cudaEvent_t &e : ev_solve) OPSB_CUDA(cudaEventCreate(&e));
+  }
+  ~Tea() {
+    for (cudaEvent_t e : ev_solve)
+      if (e) cudaEventDestroy(e);
   }
 
   void loop(const char *k, const int *range, std::initializer_list<Arg> a) {
@@ -88,6 +98,13 @@ struct Tea {
     number_of_states = d.number_of_states;
     if (number_of_states < 1 || number_of_states > 24) throw Error(E_ARG, "1..24 states are supported");
     if (d.solver != 0 && d.solver != 1) throw Error(E_UNSUPPORTED, "solver must be 0 (Jacobi) or 1 (CG)");
+    fused = d.fused != 0;
+    mixed = d.mixed != 0;
+    true_stop = d.true_residual_stop != 0;
+    delta = d.reliable_delta;
+    if ((mixed || true_stop) && !fused) throw Error(E_ARG, "mixed and true_residual_stop need fused = 1");
+    if (fused && reflective_boundary) throw Error(E_UNSUPPORTED, "fused solves need reflective_boundary = 0");
+    if (mixed && !(delta > 0.0 && delta < 1.0)) throw Error(E_ARG, "reliable_delta must be in (0, 1)");
     for (int i = 0; i < number_of_states; i++) {
       const ops_b200_clover_state &s = d.states[i];
       states[i].defined = 1;
@@ -407,12 +424,53 @@ struct Tea {
     return error;
   }
 
+  double *interior(int d) {
+    Dat &x = r.dat(d);
+    return reinterpret_cast<double *>(x.origin_ptr()) + field.x_min + (long long)field.y_min * x.pitch;
+  }
+
+  // The CG solve as the device-resident iteration of heat_pcg.cu: the same
+  // coefficient set-up loops, then the solver on the dats' storage.
+  void tea_leaf_fused(double rx, double ry) {
+    r.execute();
+    heat::Field2D f;
+    f.nx = grid.x_cells;
+    f.ny = grid.y_cells;
+    f.pitch = r.dat(u).pitch;
+    for (int d : {vector_Kx, vector_Ky, u0, u, vector_r, vector_w, vector_p, vector_z, vector_Mi})
+      if (r.dat(d).pitch != f.pitch) throw Error(E_STATE, "fused heat solve: fields differ in pitch");
+    f.Kx = interior(vector_Kx);
+    f.Ky = interior(vector_Ky);
+    f.u0 = interior(u0);
+    f.u = interior(u);
+    f.r = interior(vector_r);
+    f.w = interior(vector_w);
+    f.p = interior(vector_p);
+    f.z = interior(vector_z);
+    f.Mi = interior(vector_Mi);
+    heat::SolveStats st;
+    const bool pre = prec != TL_PREC_NONE;
+    if (mixed)
+      solver.pcg_mixed(f, rx, ry, pre, eps, delta, max_iters, r.stream(), &st);
+    else
+      solver.pcg_fp64(f, rx, ry, pre, true_stop, eps, max_iters, r.stream(), &st);
+    r.count_kernels(solver.launches());
+    const double ir = st.initial_residual;
+    double srow[7] = {(double)st.iterations, ir, st.error / ir, -1.0, st.true_residual / ir, (double)st.outer, 0.0};
+    solves.insert(solves.end(), srow, srow + 7);
+  }
+
   // tea_solve.cpp:37-418 for tl_use_cg / tl_use_jacobi.
   void tea_leaf() {
     double rx, ry, rro = 0.0;
     set_fields({FIELD_ENERGY1, FIELD_DENSITY});
     update_halo(fields, 1);
     common_init(1, &rx, &ry);
+    if (use_cg && fused) {
+      tea_leaf_fused(rx, ry);
+      finalise();
+      return;
+    }
     set_fields({FIELD_U});
     update_halo(fields, 1);
     calc_residual(rx, ry);
@@ -452,9 +510,13 @@ struct Tea {
       exact = sqrt(calc_2norm(vector_r)) / initial_residual;
     }
     // the reference reports n - 1 (tea_solve.cpp:386), also when the loop ran out
-    double srow[4] = {(double)(n - 1), initial_residual, error / initial_residual, exact};
-    solves.insert(solves.end(), srow, srow + 4);
-    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};  // tea_leaf_finalise
+    double srow[7] = {(double)(n - 1), initial_residual, error / initial_residual, exact, -1.0, 0.0, 0.0};
+    solves.insert(solves.end(), srow, srow + 7);
+    finalise();
+  }
+
+  void finalise() {  // tea_leaf_finalise (tea_solve.cpp:400-418)
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
     loop("tea_leaf_recip2_kernel", rng,
          {dat(energy1, S2D_00, ACC_WRITE), dat(u, S2D_00, ACC_READ), dat(density, S2D_00, ACC_READ)});
     set_fields({FIELD_ENERGY1});
@@ -485,7 +547,15 @@ struct Tea {
   bool cycle() {  // diffuse.cpp:83-130
     step = step + 1;
     dt = dtinit;  // timestep.cpp:37-54
+    r.execute();
+    OPSB_CUDA(cudaEventRecord(ev_solve[0], r.stream()));
     tea_leaf();
+    r.execute();
+    OPSB_CUDA(cudaEventRecord(ev_solve[1], r.stream()));
+    OPSB_CUDA(cudaEventSynchronize(ev_solve[1]));
+    float ms = 0.f;
+    OPSB_CUDA(cudaEventElapsedTime(&ms, ev_solve[0], ev_solve[1]));
+    solves.back() = ms * 1e-3;
     currtime = currtime + dt;
     if (summary_frequency != 0)
       if ((step % summary_frequency) == 0) field_summary();
@@ -528,11 +598,12 @@ extern "C" int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summa
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (device_seconds) *device_seconds = ms * 1e-3;
-    int n = (int)(t.summaries.size() / 6), ns = (int)(t.solves.size() / 4);
+    int n = (int)(t.summaries.size() / 6), ns = (int)(t.solves.size() / OPS_B200_TEA_SOLVE_COLS);
     if (n_summaries) *n_summaries = n;
     if (n_solves) *n_solves = ns;
     if (summaries) memcpy(summaries, t.summaries.data(), sizeof(double) * 6 * std::min(n, max_summaries));
-    if (solves) memcpy(solves, t.solves.data(), sizeof(double) * 4 * std::min(ns, max_solves));
+    if (solves)
+      memcpy(solves, t.solves.data(), sizeof(double) * OPS_B200_TEA_SOLVE_COLS * std::min(ns, max_solves));
     if (dump_dir) {
       for (int i = mk.dats; i < r.ndats(); i++) {
         Dat &d = r.dat(i);

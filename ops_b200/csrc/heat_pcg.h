@@ -1,0 +1,65 @@
+// Device-resident Jacobi-preconditioned CG for the TeaLeaf 2D heat operator
+// (apps/c/TeaLeaf/tea_solve.cpp:139-356 with tea_leaf_cg.cpp:53-214): the
+// scalars alpha, beta and the stopping test live in device memory, so an
+// iteration is three kernel launches and no host round trip; iterations are
+// replayed from a CUDA graph in chunks and the host polls one chunk behind.
+//
+// Two precisions:
+//  - pcg_fp64: the reference's FP64 iteration, cell for cell (w = A p with
+//    pw = p.w; u += alpha p, r -= alpha w, z = Mi r with rz = r.z; p = beta p + z)
+//    and TeaLeaf's stopping rule sqrt|rz| < eps * ||r0||.
+//    With true_stop the test is ||r|| < eps * ||r0|| on the recursive residual.
+//  - pcg_mixed: the same iteration in FP32 (r, p, w, z and the correction e,
+//    with FP32 copies of Kx, Ky, Mi) under FP64 reliable updates (Sleijpen and
+//    van der Vorst 1996): whenever the recursive sqrt(r.z) has fallen by
+//    `delta` since the last update, or its estimate says converged, e is added
+//    to u in FP64, r = u0 - A u is recomputed in FP64 and replaces the FP32
+//    residual, and the search direction is kept. The solve stops when that
+//    FP64 residual ||u0 - A u|| < eps * ||r0||.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace opsb {
+namespace heat {
+
+// Interior of one TeaLeaf chunk: every pointer addresses the first interior
+// cell of an FP64 field with one halo cell on each side; all share `pitch`.
+struct Field2D {
+  int nx = 0, ny = 0;
+  long long pitch = 0;
+  const double *Kx = nullptr, *Ky = nullptr, *u0 = nullptr;
+  double *u = nullptr, *r = nullptr, *w = nullptr, *p = nullptr, *z = nullptr, *Mi = nullptr;
+};
+
+struct SolveStats {
+  int iterations = 0;         // as the reference reports it (n - 1 on convergence)
+  int outer = 0;              // reliable updates (mixed only)
+  int converged = 0;
+  double initial_residual = 0; // ||u0 - A u|| at entry
+  double error = 0;            // the stopping quantity at exit
+  double true_residual = 0;    // ||u0 - A u|| at exit, FP64
+};
+
+class Solver {
+ public:
+  Solver();
+  ~Solver();
+  Solver(const Solver &) = delete;
+  Solver &operator=(const Solver &) = delete;
+
+  void pcg_fp64(const Field2D &f, double rx, double ry, bool precond, bool true_stop, double eps, int max_iters,
+                cudaStream_t s, SolveStats *st);
+  void pcg_mixed(const Field2D &f, double rx, double ry, bool precond, double eps, double delta, int max_iters,
+                 cudaStream_t s, SolveStats *st);
+  // Kernels launched by the last solve (each launch counted once, including
+  // the no-op launches of a chunk that ran past convergence).
+  long long launches() const { return launches_; }
+
+ private:
+  struct Impl;
+  Impl *m_;
+  long long launches_ = 0;
+};
+
+}  // namespace heat
+}  // namespace opsb

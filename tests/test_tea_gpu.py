@@ -88,7 +88,75 @@ def test_cg_determinism_and_invariants(gpu_runtime):
                          states=seeded.tea_config4_states(150, 90, 11))
     a, sa, _ = apps.tealeaf(deck)
     b, sb, _ = apps.tealeaf(deck)
-    assert np.array_equal(a, b) and np.array_equal(sa, sb)
+    assert np.array_equal(a, b) and np.array_equal(sa[:, :6], sb[:, :6])   # column 6 is the solve's time
     np.testing.assert_allclose(a[:, 2], a[0, 2], rtol=1e-13)
     np.testing.assert_allclose(a[:, 3], a[0, 3], rtol=1e-13)
     assert (sa[:, 2] < 1e-10).all()
+
+
+@pytest.mark.parametrize("name", ["tea_cg_jacdiag_64", "tea_cg_plain_100x70"])
+def test_fused_solver_matches_reference_golden(gpu_runtime, name, tmp_path):
+    """The device-resident CG (alpha, beta and the stop test on the GPU) keeps
+    the reference's per-cell arithmetic and stopping rule: iteration counts
+    exact, summaries to 1e-12, fields to the CG tolerance."""
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    deck = apps.tea_deck(fused=1, **CASES[name])
+    summ, solves, _ = apps.tealeaf(deck, dump_dir=str(tmp_path))
+    assert np.array_equal(solves[:, 0].astype(np.int64), g["iters"])
+    np.testing.assert_allclose(as_reference_columns(summ)[:, 1:], g["summaries"][:, 1:], rtol=REL_SUM, atol=0)
+    for f in ("energy1", "u"):
+        ext = g["f_" + f]
+        got = np.fromfile(str(tmp_path / (f + ".bin"))).reshape(ext.shape)
+        np.testing.assert_allclose(got, ext, rtol=0, atol=REL_FIELD_CG * np.abs(ext).max(), err_msg=f)
+    assert (solves[:, 2] < 1e-10).all()        # the stopping quantity
+    assert (solves[:, 4] > 0).all() and (solves[:, 4] < 1e-8).all()   # true FP64 residual ratio
+
+
+def test_fused_matches_loop_chain(gpu_runtime, tmp_path):
+    """Fused and loop-by-loop CG on a 300x200 seeded problem: same iteration
+    counts, solutions equal to rounding."""
+    kw = dict(x_cells=300, y_cells=200, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=2, max_iters=5000,
+              eps=1e-10, solver=1, preconditioner=1, summary_frequency=1,
+              states=seeded.tea_config4_states(300, 200, 13))
+    (tmp_path / "a").mkdir()
+    (tmp_path / "b").mkdir()
+    a, sa, _ = apps.tealeaf(apps.tea_deck(**kw), dump_dir=str(tmp_path / "a"))
+    b, sb, _ = apps.tealeaf(apps.tea_deck(fused=1, **kw), dump_dir=str(tmp_path / "b"))
+    assert np.array_equal(sa[:, 0], sb[:, 0])
+    np.testing.assert_allclose(a[:, 2:], b[:, 2:], rtol=REL_SUM, atol=0)
+    ua = np.fromfile(str(tmp_path / "a" / "u.bin"))
+    ub = np.fromfile(str(tmp_path / "b" / "u.bin"))
+    np.testing.assert_allclose(ub, ua, rtol=0, atol=REL_FIELD_CG * np.abs(ua).max())
+
+
+def test_true_residual_stop(gpu_runtime):
+    """true_residual_stop: the FP64 solve runs until ||u0 - A u|| < 1e-10 ||r0||,
+    which takes at least as many iterations as TeaLeaf's sqrt|r.z| test."""
+    kw = dict(x_cells=256, y_cells=192, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=1, max_iters=20000,
+              eps=1e-10, solver=1, preconditioner=1, summary_frequency=1,
+              states=seeded.tea_config4_states(256, 192, 21))
+    _, sa, _ = apps.tealeaf(apps.tea_deck(fused=1, **kw))
+    _, sb, _ = apps.tealeaf(apps.tea_deck(fused=1, true_residual_stop=1, **kw))
+    assert sb[0, 0] >= sa[0, 0]
+    assert sb[0, 4] < 1.5e-10          # recomputed FP64 residual; the recursive one met 1e-10
+
+
+@pytest.mark.parametrize("precond", [1, 0])
+def test_mixed_precision_reaches_fp64_residual(gpu_runtime, precond, tmp_path):
+    """FP32 PCG under FP64 reliable updates: the FP64 residual ||u0 - A u|| /
+    ||r0|| ends below 1e-10 and the solution agrees with the FP64 solve to the
+    accuracy that residual implies."""
+    kw = dict(x_cells=256, y_cells=192, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=1, max_iters=20000,
+              eps=1e-10, solver=1, preconditioner=precond, summary_frequency=1,
+              states=seeded.tea_config4_states(256, 192, 21))
+    (tmp_path / "a").mkdir()
+    (tmp_path / "b").mkdir()
+    a, sa, _ = apps.tealeaf(apps.tea_deck(fused=1, **kw), dump_dir=str(tmp_path / "a"))
+    b, sb, _ = apps.tealeaf(apps.tea_deck(fused=1, mixed=1, reliable_delta=0.1, **kw), dump_dir=str(tmp_path / "b"))
+    assert sb[0, 4] < 1e-10 and sb[0, 2] < 1e-10
+    assert sb[0, 5] >= 5                       # reliable updates: one per decade at least
+    assert sb[0, 0] < 2.0 * sa[0, 0]           # the search direction survives the updates
+    ua = np.fromfile(str(tmp_path / "a" / "u.bin"))
+    ub = np.fromfile(str(tmp_path / "b" / "u.bin"))
+    assert np.linalg.norm(ub - ua) / np.linalg.norm(ua) < 1e-8
+    np.testing.assert_allclose(b[:, 2:4], a[:, 2:4], rtol=1e-12, atol=0)   # volume and mass: untouched by the solve
