@@ -286,6 +286,18 @@ int ops_b200_laplace_sweep_noalloc(int imax, int jmax, const double *A, double *
                                    double *max_delta, void *stream);
 const char *ops_b200_noalloc_last_error(void);
 
+/* ---- learned preconditioner building blocks (no reference counterpart) --
+ * 3x3 convolution, stride 1, zero padding 1, on the tcgen05 tensor cores:
+ * x NHWC BF16 [n][h][w][cin], weights BF16 [9][cout][cin] (tap = (dy+1)*3 +
+ * (dx+1)), y NHWC BF16 [n][h][w][cout], FP32 accumulation. mode 0: y =
+ * relu(conv + bias); 1: y = conv + bias; 2: y = conv * (mask > 0) with mask
+ * BF16 shaped like y; 3: y = conv. (cin, cout) in {(16,16), (16,32), (32,16),
+ * (32,32), (32,64), (64,32), (64,64)}; pointers 16-byte aligned. Synchronous
+ * on `stream` (a cudaStream_t, NULL = default); OPS_B200_ERR_TIMEOUT if a
+ * pipeline wait inside the kernel expired. */
+int ops_b200_conv3x3_bf16(const void *x, const void *w, const float *bias, const void *mask, void *y, int n, int h,
+                          int wd, int cin, int cout, int mode, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

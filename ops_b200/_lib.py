@@ -126,6 +126,7 @@ def _declare(L):
         "ops_b200_tridMultiDimBatch": ([i, i, P, i, i, i, i], i),
         "ops_b200_tridMultiDimBatch_Inc": ([i, i, P, i, i, i, i, i], i),
         "ops_b200_trid_batch": ([i, i, i, P, P], i),
+        "ops_b200_conv3x3_bf16": ([P, P, P, P, P, i, i, i, i, i, i, P], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
