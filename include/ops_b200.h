@@ -298,6 +298,78 @@ const char *ops_b200_noalloc_last_error(void);
 int ops_b200_conv3x3_bf16(const void *x, const void *w, const float *bias, const void *mask, void *y, int n, int h,
                           int wd, int cin, int cout, int mode, void *stream);
 
+/* ---- heat solves on caller-owned device fields (no reference counterpart)
+ * The TeaLeaf operator A u = (1 + rx (Kx + Kx_e) + ry (Ky + Ky_n)) u - ...
+ * (apps/c/TeaLeaf/tea_leaf_common_kernels.h) on an nx x ny interior. Every
+ * pointer addresses the first interior cell of an FP64 field with a one-cell
+ * ring (index -1 .. n), row pitch `pitch` elements; Kx and Ky are the face
+ * coefficients TeaLeaf's tea_leaf_common_init_Kx_Ky_kernel produces (zero on
+ * the domain boundary). u holds the initial guess and receives the solution.
+ * The solve stops when ||u0 - A u|| < eps ||r0|| (method 0: TeaLeaf's
+ * sqrt|r.z| test) or after max_iters iterations. */
+typedef struct ops_b200_heat_system {
+  int nx, ny;
+  long long pitch;
+  const double *Kx, *Ky, *u0;
+  double *u;
+  double rx, ry;
+} ops_b200_heat_system;
+
+typedef struct ops_b200_heat_stats {
+  int iterations;          /* CG iterations (method 0: as TeaLeaf prints them) */
+  int updates;             /* reliable updates (method 2) */
+  int converged;
+  int fallbacks;           /* learned -> Jacobi switches (method 3) */
+  double initial_residual; /* ||u0 - A u|| at entry */
+  double final_residual;   /* ||u0 - A u|| at exit, FP64 */
+  double seconds;          /* device time of the solve */
+  long long launches;      /* kernels launched by the solve */
+} ops_b200_heat_stats;
+
+#define OPS_B200_HEAT_PCG 0          /* FP64 Jacobi-PCG, TeaLeaf's stopping rule */
+#define OPS_B200_HEAT_PCG_TRUE 1     /* FP64 Jacobi-PCG, stop on ||r|| < eps ||r0|| */
+#define OPS_B200_HEAT_MIXED 2        /* FP32 Jacobi-PCG under FP64 reliable updates */
+#define OPS_B200_HEAT_FCG_LEARNED 3  /* flexible CG, learned preconditioner `net`, Jacobi fallback */
+#define OPS_B200_HEAT_FCG_JACOBI 4   /* the same flexible CG with Jacobi (no network) */
+
+/* Solves A u = u0. `net` names a learned preconditioner (method 3); window:
+ * method 3 falls back to Jacobi when ||r|| has not halved over `window`
+ * iterations (0 = only on lost positive curvature). r_out (device, may be
+ * NULL) receives u0 - A u at exit. Synchronous on `stream`. Not reentrant:
+ * one solve at a time per process (a shared workspace is kept per size). */
+int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, double eps, int max_iters, int window,
+                        double *r_out, ops_b200_heat_stats *stats, void *stream);
+
+/* ---- learned multigrid preconditioner (no reference counterpart) ---------
+ * A 4-level U-Net-shaped CNN (16/32/64/64 channels, 3x3 BF16 convolutions on
+ * the tensor cores, FP32 accumulation) mapping a residual and the face
+ * coefficients to M(r) = r / diag(A) + s * net(...), s = rms(r / diag(A));
+ * trained on residual/error pairs (loss mean_n ||M(r_n) - e_n||^2 / ||e_n||^2)
+ * by the library's own forward and backward kernels with Adam. A batch is n
+ * fields of h x w interior cells (multiples of 8) laid out like
+ * ops_b200_heat_system, image n starting `image` elements after image 0. */
+typedef struct ops_b200_heat_batch {
+  int n, h, w;
+  long long pitch, image;
+  const double *r, *Kx, *Ky;
+  double rx, ry;
+} ops_b200_heat_batch;
+
+int ops_b200_lmg_create(unsigned long long seed);   /* returns a handle */
+int ops_b200_lmg_destroy(int net);
+int ops_b200_lmg_num_params(void);
+/* FP32 parameters: per conv layer W [9][cout][cin] then b [cout] (layers
+ * C0, C1a, C1b, C2a, C2b, C3a, C3b, C2u, C1u, C0u), then wout [16], bout. */
+int ops_b200_lmg_get_params(int net, float *host);
+int ops_b200_lmg_set_params(int net, const float *host);   /* also resets Adam */
+int ops_b200_lmg_get_grads(int net, float *host);          /* of the last train step */
+/* out (device, batch layout) = M(r). Synchronous on `stream`. */
+int ops_b200_lmg_apply(int net, const ops_b200_heat_batch *b, double *out, void *stream);
+/* Forward + backward on a batch with targets e (device, batch layout); one
+ * Adam step when lr > 0; *loss receives the batch loss before the step. */
+int ops_b200_lmg_train_step(int net, const ops_b200_heat_batch *b, const double *e, double lr, double *loss,
+                            void *stream);
+
 #ifdef __cplusplus
 }
 #endif

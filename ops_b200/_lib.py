@@ -70,6 +70,24 @@ class TeaDeck(ctypes.Structure):
                 ("reliable_delta", ctypes.c_double)]
 
 
+class HeatSystem(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("pitch", ctypes.c_longlong),
+                ("Kx", ctypes.c_void_p), ("Ky", ctypes.c_void_p), ("u0", ctypes.c_void_p), ("u", ctypes.c_void_p),
+                ("rx", ctypes.c_double), ("ry", ctypes.c_double)]
+
+
+class HeatStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("updates", ctypes.c_int), ("converged", ctypes.c_int),
+                ("fallbacks", ctypes.c_int), ("initial_residual", ctypes.c_double),
+                ("final_residual", ctypes.c_double), ("seconds", ctypes.c_double), ("launches", ctypes.c_longlong)]
+
+
+class HeatBatch(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("h", ctypes.c_int), ("w", ctypes.c_int), ("pitch", ctypes.c_longlong),
+                ("image", ctypes.c_longlong), ("r", ctypes.c_void_p), ("Kx", ctypes.c_void_p),
+                ("Ky", ctypes.c_void_p), ("rx", ctypes.c_double), ("ry", ctypes.c_double)]
+
+
 _lib = None
 
 
@@ -127,6 +145,15 @@ def _declare(L):
         "ops_b200_tridMultiDimBatch_Inc": ([i, i, P, i, i, i, i, i], i),
         "ops_b200_trid_batch": ([i, i, i, P, P], i),
         "ops_b200_conv3x3_bf16": ([P, P, P, P, P, i, i, i, i, i, i, P], i),
+        "ops_b200_heat_solve": ([P, i, i, ctypes.c_double, i, i, P, P, P], i),
+        "ops_b200_lmg_create": ([ctypes.c_ulonglong], i),
+        "ops_b200_lmg_destroy": ([i], i),
+        "ops_b200_lmg_num_params": ([], i),
+        "ops_b200_lmg_get_params": ([i, P], i),
+        "ops_b200_lmg_set_params": ([i, P], i),
+        "ops_b200_lmg_get_grads": ([i, P], i),
+        "ops_b200_lmg_apply": ([i, P, P, P], i),
+        "ops_b200_lmg_train_step": ([i, P, P, ctypes.c_double, P, P], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

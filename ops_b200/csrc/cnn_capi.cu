@@ -52,3 +52,239 @@ extern "C" int ops_b200_conv3x3_bf16(const void *x, const void *w, const float *
     return 0;
   });
 }
+
+// ---------------------------------------------------------------------------
+// raw heat solves and the learned preconditioner's network handles
+// ---------------------------------------------------------------------------
+#include <memory>
+#include <vector>
+
+#include "heat_pcg.h"
+#include "lmg.h"
+
+namespace opsb {
+namespace {
+
+struct HeatWorkspace {
+  int nx = 0, ny = 0;
+  long long pitch = 0;
+  double *buf = nullptr;
+  double *r = nullptr, *w = nullptr, *p = nullptr, *z = nullptr, *Mi = nullptr;
+  heat::Solver solver;
+  ~HeatWorkspace() { cudaFree(buf); }
+  void ensure(int x, int y, long long pt, cudaStream_t s) {
+    if (x == nx && y == ny && pt == pitch && buf) return;
+    cudaFree(buf);
+    buf = nullptr;
+    const size_t one = (size_t)pt * (y + 2);
+    OPSB_CUDA(cudaMalloc(&buf, 5 * one * sizeof(double)));
+    OPSB_CUDA(cudaMemsetAsync(buf, 0, 5 * one * sizeof(double), s));
+    double **f[5] = {&r, &w, &p, &z, &Mi};
+    for (int k = 0; k < 5; k++) *f[k] = buf + k * one + pt + 1;
+    nx = x;
+    ny = y;
+    pitch = pt;
+  }
+};
+
+std::mutex g_mu;
+HeatWorkspace &workspace() {
+  static HeatWorkspace ws;
+  return ws;
+}
+std::vector<std::unique_ptr<lmg::Net>> &nets() {
+  static std::vector<std::unique_ptr<lmg::Net>> v;
+  return v;
+}
+lmg::Net &net_of(int h) {
+  if (h < 0 || h >= (int)nets().size() || !nets()[h]) throw Error(E_ARG, "unknown learned-preconditioner handle");
+  return *nets()[h];
+}
+lmg::Fields fields_of(const ops_b200_heat_batch *b) {
+  if (!b || !b->r || !b->Kx || !b->Ky) throw Error(E_ARG, "heat batch: null field");
+  if (b->n < 1 || b->h < 8 || b->w < 8 || b->h % 8 || b->w % 8)
+    throw Error(E_ARG, "heat batch: h and w must be positive multiples of 8");
+  if (b->pitch < b->w + 2 || (b->n > 1 && b->image < b->pitch * (b->h + 2)))
+    throw Error(E_ARG, "heat batch: pitch or image stride too small for a one-cell ring");
+  lmg::Fields f;
+  f.n = b->n;
+  f.h = b->h;
+  f.w = b->w;
+  f.pitch = b->pitch;
+  f.image = b->image;
+  f.r = b->r;
+  f.Kx = b->Kx;
+  f.Ky = b->Ky;
+  f.rx = b->rx;
+  f.ry = b->ry;
+  return f;
+}
+
+}  // namespace
+}  // namespace opsb
+
+extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, double eps, int max_iters,
+                                   int window, double *r_out, ops_b200_heat_stats *stats, void *stream) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!sys || !sys->Kx || !sys->Ky || !sys->u0 || !sys->u) throw Error(E_ARG, "heat system: null field");
+    if (sys->nx < 1 || sys->ny < 1 || sys->pitch < sys->nx + 2) throw Error(E_ARG, "heat system: bad shape");
+    if (method < OPS_B200_HEAT_PCG || method > OPS_B200_HEAT_FCG_JACOBI) throw Error(E_ARG, "heat system: method");
+    if (!(eps > 0.0) || max_iters < 0) throw Error(E_ARG, "heat system: eps > 0 and max_iters >= 0 required");
+    std::lock_guard<std::mutex> lk(g_mu);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    HeatWorkspace &ws = workspace();
+    ws.ensure(sys->nx, sys->ny, sys->pitch, s);
+    heat::Field2D f;
+    f.nx = sys->nx;
+    f.ny = sys->ny;
+    f.pitch = sys->pitch;
+    f.Kx = sys->Kx;
+    f.Ky = sys->Ky;
+    f.u0 = sys->u0;
+    f.u = sys->u;
+    f.r = ws.r;
+    f.w = ws.w;
+    f.p = ws.p;
+    f.z = ws.z;
+    f.Mi = ws.Mi;
+    ws.solver.diag(f, sys->rx, sys->ry, s);
+    heat::SolveStats st;
+    cudaEvent_t e0, e1;
+    OPSB_CUDA(cudaEventCreate(&e0));
+    OPSB_CUDA(cudaEventCreate(&e1));
+    OPSB_CUDA(cudaEventRecord(e0, s));
+    if (method == OPS_B200_HEAT_PCG || method == OPS_B200_HEAT_PCG_TRUE) {
+      ws.solver.pcg_fp64(f, sys->rx, sys->ry, true, method == OPS_B200_HEAT_PCG_TRUE, eps, max_iters, s, &st);
+    } else if (method == OPS_B200_HEAT_MIXED) {
+      if (sys->nx < 1) throw Error(E_ARG, "heat system: bad shape");
+      ws.solver.pcg_mixed(f, sys->rx, sys->ry, true, eps, 0.1, max_iters, s, &st);
+    } else {
+      heat::Solver::Precond M;
+      if (method == OPS_B200_HEAT_FCG_LEARNED) {
+        lmg::Net *np = &net_of(net);
+        if (sys->nx % 8 || sys->ny % 8) throw Error(E_ARG, "learned preconditioner: nx and ny must be multiples of 8");
+        lmg::Fields lf;
+        lf.n = 1;
+        lf.h = sys->ny;
+        lf.w = sys->nx;
+        lf.pitch = sys->pitch;
+        lf.image = 0;
+        lf.r = ws.r;
+        lf.Kx = sys->Kx;
+        lf.Ky = sys->Ky;
+        lf.rx = sys->rx;
+        lf.ry = sys->ry;
+        M = [np, lf](const double *, double *z, cudaStream_t ss) -> long long {
+          const long long before = np->launches();
+          np->apply(lf, z, ss);
+          return np->launches() - before;
+        };
+      }
+      ws.solver.fcg(f, sys->rx, sys->ry, eps, max_iters, M, window, s, &st);
+    }
+    OPSB_CUDA(cudaEventRecord(e1, s));
+    OPSB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    OPSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    double fin = st.true_residual;
+    if (r_out) fin = ws.solver.residual(f, sys->rx, sys->ry, r_out, s);
+    if (method == OPS_B200_HEAT_FCG_LEARNED) {
+      int err = 0;
+      OPSB_CUDA(cudaMemcpy(&err, cnn::error_word(), sizeof(int), cudaMemcpyDeviceToHost));
+      if (err) throw Error(E_TIMEOUT, "learned preconditioner: a convolution pipeline wait expired");
+    }
+    if (stats) {
+      stats->iterations = st.iterations;
+      stats->updates = st.outer;
+      stats->converged = st.converged;
+      stats->fallbacks = st.fallbacks;
+      stats->initial_residual = st.initial_residual;
+      stats->final_residual = fin;
+      stats->seconds = ms * 1e-3;
+      stats->launches = ws.solver.launches();
+    }
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_lmg_create(unsigned long long seed) {
+  using namespace opsb;
+  return capi_guard([&] {
+    std::lock_guard<std::mutex> lk(g_mu);
+    nets().emplace_back(new lmg::Net(seed));
+    return (int)nets().size() - 1;
+  });
+}
+
+extern "C" int ops_b200_lmg_destroy(int net) {
+  using namespace opsb;
+  return capi_guard([&] {
+    std::lock_guard<std::mutex> lk(g_mu);
+    net_of(net);
+    nets()[net].reset();
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_lmg_num_params(void) { return opsb::lmg::Net::num_params(); }
+
+extern "C" int ops_b200_lmg_get_params(int net, float *host) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!host) throw Error(E_ARG, "null buffer");
+    net_of(net).get_params(host);
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_lmg_set_params(int net, const float *host) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!host) throw Error(E_ARG, "null buffer");
+    net_of(net).set_params(host);
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_lmg_get_grads(int net, float *host) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!host) throw Error(E_ARG, "null buffer");
+    net_of(net).get_grads(host);
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_lmg_apply(int net, const ops_b200_heat_batch *b, double *out, void *stream) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!out) throw Error(E_ARG, "null output");
+    lmg::Fields f = fields_of(b);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    net_of(net).apply(f, out, s);
+    OPSB_CUDA(cudaStreamSynchronize(s));
+    int err = 0;
+    OPSB_CUDA(cudaMemcpy(&err, cnn::error_word(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) throw Error(E_TIMEOUT, "learned preconditioner: a convolution pipeline wait expired");
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_lmg_train_step(int net, const ops_b200_heat_batch *b, const double *e, double lr,
+                                       double *loss, void *stream) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!e) throw Error(E_ARG, "null target");
+    lmg::Fields f = fields_of(b);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    lmg::Net &nt = net_of(net);
+    const double L = nt.loss_and_grad(f, e, s);
+    if (lr > 0.0) nt.adam(lr, s);
+    OPSB_CUDA(cudaStreamSynchronize(s));
+    if (loss) *loss = L;
+    return 0;
+  });
+}

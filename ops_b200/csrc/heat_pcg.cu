@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "heat_pcg.h"
 #include "runtime.h"
@@ -332,6 +333,114 @@ __global__ void __launch_bounds__(NT) k_to_float(Geom g, Geom g32, const double 
     }
 }
 
+
+// ---- flexible CG (Notay 2000, FCG with one-step truncation) ----------------
+// k_fw: w = A p, pw = p.w, pr = p.r -> alpha = pr / pw; a non-positive pw
+// (the preconditioned direction lost positive curvature) stops with done = 4.
+__global__ void __launch_bounds__(NT) k_fw(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
+                                           const double *__restrict__ p, const double *__restrict__ r,
+                                           double *__restrict__ w, double rx, double ry, Scalars *s, double *part,
+                                           unsigned *cnt) {
+  __shared__ double sm[kWarps];
+  __shared__ int last;
+  if (s->done) return;
+  double acc[2] = {0.0, 0.0};
+  HEAT_CELLS(g) {
+    const long long i = (long long)y * g.pitch + x;
+    const double wv = smvp(Kx, Ky, p, i, g.pitch, rx, ry);
+    w[i] = wv;
+    acc[0] = acc[0] + wv * p[i];
+    acc[1] = acc[1] + p[i] * r[i];
+  }
+  if (publish<2>(acc, part, cnt, sm, &last)) {
+    const double pw = grid_total<2>(part, 0, sm);
+    const double pr = grid_total<2>(part, 1, sm);
+    if (tid_() == 0) {
+      s->pw = pw;
+      if (pw > 0.0) s->alpha = pr / pw;
+      else s->done = 4;
+      *cnt = 0u;
+    }
+  }
+}
+
+// u += alpha p, r -= alpha w, rr = r.r; stop when ||r|| < eps ||r0||.
+__global__ void __launch_bounds__(NT) k_fupd(Geom g, double *__restrict__ u, const double *__restrict__ p,
+                                             double *__restrict__ r, const double *__restrict__ w, Scalars *s,
+                                             double *part, unsigned *cnt) {
+  __shared__ double sm[kWarps];
+  __shared__ int last;
+  if (s->done) return;
+  const double alpha = s->alpha;
+  double acc[1] = {0.0};
+  HEAT_CELLS(g) {
+    const long long i = (long long)y * g.pitch + x;
+    u[i] = u[i] + alpha * p[i];
+    const double rv = r[i] - alpha * w[i];
+    r[i] = rv;
+    acc[0] = acc[0] + rv * rv;
+  }
+  if (publish<1>(acc, part, cnt, sm, &last)) {
+    const double t = grid_total<1>(part, 0, sm);
+    if (tid_() == 0) {
+      s->rr = t;
+      s->err = sqrt(t);
+      s->iters = s->iters + 1;
+      if (s->err < s->stop) s->done = 1;
+      else if (s->iters >= s->max_iters) s->done = 2;
+      *cnt = 0u;
+    }
+  }
+}
+
+// beta = -(z.w) / pw.
+__global__ void __launch_bounds__(NT) k_fzw(Geom g, const double *__restrict__ z, const double *__restrict__ w,
+                                            Scalars *s, double *part, unsigned *cnt) {
+  __shared__ double sm[kWarps];
+  __shared__ int last;
+  double acc[1] = {0.0};
+  HEAT_CELLS(g) {
+    const long long i = (long long)y * g.pitch + x;
+    acc[0] = acc[0] + z[i] * w[i];
+  }
+  if (publish<1>(acc, part, cnt, sm, &last)) {
+    const double t = grid_total<1>(part, 0, sm);
+    if (tid_() == 0) {
+      s->beta = -t / s->pw;
+      *cnt = 0u;
+    }
+  }
+}
+
+// p = z + beta p, or p = z on a restart.
+__global__ void __launch_bounds__(NT) k_fp(Geom g, double *__restrict__ p, const double *__restrict__ z,
+                                           const Scalars *s, int restart) {
+  const double beta = restart ? 0.0 : s->beta;
+  HEAT_CELLS(g) {
+    const long long i = (long long)y * g.pitch + x;
+    p[i] = restart ? z[i] : z[i] + beta * p[i];
+  }
+}
+
+// z = Mi r (Jacobi).
+__global__ void __launch_bounds__(NT) k_jacobi(Geom g, const double *__restrict__ Mi, const double *__restrict__ r,
+                                               double *__restrict__ z) {
+  HEAT_CELLS(g) {
+    const long long i = (long long)y * g.pitch + x;
+    z[i] = Mi[i] * r[i];
+  }
+}
+
+// tea_leaf_common_init_diag_init_kernel (tea_leaf_common_kernels.h:38):
+// Mi = 1 / (1 + ry (Ky(0,1) + Ky(0,0)) + rx (Kx(1,0) + Kx(0,0))) on the interior.
+__global__ void __launch_bounds__(NT) k_diag(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
+                                             double rx, double ry, double *__restrict__ Mi) {
+  HEAT_CELLS(g) {
+    const long long i = (long long)y * g.pitch + x;
+    Mi[i] = 1.0 / (1.0 + ry * (Ky[i + g.pitch] + Ky[i]) + rx * (Kx[i + 1] + Kx[i]));
+  }
+}
+
 void check_launch(const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw Error(E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -625,6 +734,111 @@ void Solver::pcg_mixed(const Field2D &f, double rx, double ry, bool precond, dou
   out->converged = done;
   out->error = h.err;
   out->true_residual = h.err;
+}
+
+
+void Solver::diag(const Field2D &f, double rx, double ry, cudaStream_t st) {
+  validate(f);
+  k_diag<<<grid_for(f.nx, f.ny), dim3(BX, BY), 0, st>>>(Geom{f.nx, f.ny, f.pitch}, f.Kx, f.Ky, rx, ry, f.Mi);
+  check_launch("heat solver diagonal");
+}
+
+double Solver::residual(const Field2D &f, double rx, double ry, double *outp, cudaStream_t st) {
+  validate(f);
+  Impl &m = *m_;
+  m.ensure_base();
+  Scalars t = fresh(0.0);
+  OPSB_CUDA(cudaMemcpyAsync(m.s32, &t, sizeof(t), cudaMemcpyHostToDevice, st));
+  k_resid<<<grid_for(f.nx, f.ny), dim3(BX, BY), 0, st>>>(Geom{f.nx, f.ny, f.pitch}, f.Kx, f.Ky, f.u, f.u0, outp, rx,
+                                                         ry, 0.0, m.s32, m.part, m.cnt);
+  check_launch("heat residual");
+  OPSB_CUDA(cudaMemcpyAsync(&t, m.s32, sizeof(t), cudaMemcpyDeviceToHost, st));
+  OPSB_CUDA(cudaStreamSynchronize(st));
+  return sqrt(fabs(t.rr));
+}
+
+void Solver::fcg(const Field2D &f, double rx, double ry, double eps, int max_iters, const Precond &M, int window,
+                 cudaStream_t st, SolveStats *out) {
+  validate(f);
+  Impl &m = *m_;
+  m.ensure_base();
+  launches_ = 0;
+  const Geom g{f.nx, f.ny, f.pitch};
+  const dim3 grid = grid_for(f.nx, f.ny), block(BX, BY);
+  Scalars h = fresh(0.0);
+  h.max_iters = max_iters;
+  OPSB_CUDA(cudaMemcpyAsync(m.s64, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  k_resid<<<grid, block, 0, st>>>(g, f.Kx, f.Ky, f.u, f.u0, f.r, rx, ry, eps, m.s64, m.part, m.cnt);
+  check_launch("fcg init");
+  launches_ += 1;
+  bool learned = static_cast<bool>(M);
+  auto precond = [&] {
+    if (learned) {
+      launches_ += M(f.r, f.z, st);
+    } else {
+      k_jacobi<<<grid, block, 0, st>>>(g, f.Mi, f.r, f.z);
+      launches_ += 1;
+    }
+  };
+  OPSB_CUDA(cudaMemcpyAsync(&h, m.s64, sizeof(h), cudaMemcpyDeviceToHost, st));
+  OPSB_CUDA(cudaStreamSynchronize(st));
+  const double r0 = sqrt(fabs(h.rr0));
+  out->initial_residual = r0;
+  out->fallbacks = 0;
+  bool done = h.done == 1 || r0 == 0.0;
+  if (!done) {
+    // the initial residual kernel leaves done = 0 and iters = 0
+    precond();
+    k_fp<<<grid, block, 0, st>>>(g, f.p, f.z, m.s64, 1);
+    launches_ += 1;
+  }
+  std::vector<double> hist;
+  while (!done) {
+    k_fw<<<grid, block, 0, st>>>(g, f.Kx, f.Ky, f.p, f.r, f.w, rx, ry, m.s64, m.part, m.cnt);
+    k_fupd<<<grid, block, 0, st>>>(g, f.u, f.p, f.r, f.w, m.s64, m.part, m.cnt);
+    check_launch("fcg iteration");
+    launches_ += 2;
+    OPSB_CUDA(cudaMemcpyAsync(&h, m.s64, sizeof(h), cudaMemcpyDeviceToHost, st));
+    OPSB_CUDA(cudaStreamSynchronize(st));
+    if (h.done == 1 || h.done == 2) break;
+    bool restart = false;
+    if (h.done == 4) {
+      restart = true;  // lost positive curvature: fall back to Jacobi and restart the recursion
+    } else {
+      hist.push_back(h.err);
+      const size_t k = hist.size();
+      if (learned && window > 0 && k > (size_t)window && hist[k - 1] > 0.5 * hist[k - 1 - window]) restart = true;
+    }
+    if (restart) {
+      if (learned) out->fallbacks++;
+      learned = false;
+      hist.clear();
+      int zero = 0;
+      OPSB_CUDA(cudaMemcpyAsync(&m.s64->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+      precond();
+      k_fp<<<grid, block, 0, st>>>(g, f.p, f.z, m.s64, 1);
+      launches_ += 1;
+      continue;
+    }
+    precond();
+    k_fzw<<<grid, block, 0, st>>>(g, f.z, f.w, m.s64, m.part, m.cnt);
+    k_fp<<<grid, block, 0, st>>>(g, f.p, f.z, m.s64, 0);
+    check_launch("fcg direction");
+    launches_ += 2;
+  }
+  out->iterations = h.iters;
+  out->converged = h.done == 1 || done;
+  out->error = h.err;
+  out->outer = 0;
+  // true FP64 residual at exit (into w)
+  Scalars t = fresh(0.0);
+  OPSB_CUDA(cudaMemcpyAsync(m.s32, &t, sizeof(t), cudaMemcpyHostToDevice, st));
+  k_resid<<<grid, block, 0, st>>>(g, f.Kx, f.Ky, f.u, f.u0, f.w, rx, ry, 0.0, m.s32, m.part, m.cnt);
+  check_launch("fcg residual");
+  launches_ += 1;
+  OPSB_CUDA(cudaMemcpyAsync(&t, m.s32, sizeof(t), cudaMemcpyDeviceToHost, st));
+  OPSB_CUDA(cudaStreamSynchronize(st));
+  out->true_residual = sqrt(fabs(t.rr));
 }
 
 }  // namespace heat

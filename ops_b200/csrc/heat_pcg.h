@@ -16,8 +16,14 @@
 //    to u in FP64, r = u0 - A u is recomputed in FP64 and replaces the FP32
 //    residual, and the search direction is kept. The solve stops when that
 //    FP64 residual ||u0 - A u|| < eps * ||r0||.
+//  - fcg: flexible CG (Notay 2000, one-step truncation) with a caller-supplied
+//    preconditioner z = M(r) (the learned one), alpha = p.r / p.w,
+//    beta = -z.w / p.w; it falls back to Jacobi and restarts the recursion
+//    when p.w <= 0 or when ||r|| has not halved over `window` iterations.
 #pragma once
 #include <cuda_runtime.h>
+
+#include <functional>
 
 namespace opsb {
 namespace heat {
@@ -35,6 +41,7 @@ struct SolveStats {
   int iterations = 0;         // as the reference reports it (n - 1 on convergence)
   int outer = 0;              // reliable updates (mixed only)
   int converged = 0;
+  int fallbacks = 0;          // learned -> Jacobi switches (fcg only)
   double initial_residual = 0; // ||u0 - A u|| at entry
   double error = 0;            // the stopping quantity at exit
   double true_residual = 0;    // ||u0 - A u|| at exit, FP64
@@ -51,6 +58,14 @@ class Solver {
                 cudaStream_t s, SolveStats *st);
   void pcg_mixed(const Field2D &f, double rx, double ry, bool precond, double eps, double delta, int max_iters,
                  cudaStream_t s, SolveStats *st);
+  // z = M(r) on the interior of the solve's fields; returns kernels launched.
+  using Precond = std::function<long long(const double *r, double *z, cudaStream_t s)>;
+  void fcg(const Field2D &f, double rx, double ry, double eps, int max_iters, const Precond &M, int window,
+           cudaStream_t s, SolveStats *st);
+  // Mi = 1 / diag(A) on the interior (tea_leaf_common_init_diag_init_kernel).
+  void diag(const Field2D &f, double rx, double ry, cudaStream_t s);
+  // out = u0 - A u on the interior; returns ||out||.
+  double residual(const Field2D &f, double rx, double ry, double *out, cudaStream_t s);
   // Kernels launched by the last solve (each launch counted once, including
   // the no-op launches of a chunk that ran past convergence).
   long long launches() const { return launches_; }

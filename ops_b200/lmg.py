@@ -1,0 +1,185 @@
+"""Learned multigrid preconditioner for the TeaLeaf heat solve (no reference
+counterpart; the reference's solvers are Jacobi, CG, Chebyshev and PPCG).
+
+Pipeline, all arithmetic on the GPU through the library's C-ABI:
+  1. seeded coefficient fields (16 density rectangles, rho log-uniform in
+     [0.1, 100] over rho = 1; TeaLeaf's CONDUCTIVITY face coefficients),
+  2. residual/error pairs from Jacobi-PCG: a converged FP64 solve gives u*,
+     truncated solves from the same start give u_k, r_k = u0 - A u_k and
+     e_k = u* - u_k,
+  3. training of the network (tcgen05 forward and input-gradient
+     convolutions, CUDA-core weight gradients, Adam),
+  4. flexible CG with the trained network as preconditioner, falling back to
+     Jacobi-PCG when the network stops helping.
+Device buffers are torch CUDA tensors (allocation only)."""
+import ctypes
+
+import numpy as np
+
+from . import seeded
+from ._lib import HeatBatch, HeatStats, HeatSystem, check, lib
+
+PCG, PCG_TRUE, MIXED, FCG_LEARNED, FCG_JACOBI = 0, 1, 2, 3, 4
+
+
+def _vp(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def density_field(n, seed, nrect=16):
+    """Cell densities and energies of the seeded heat problem on an n x n grid
+    over [0, 10]^2 (cell centres inside a rectangle take its state)."""
+    st = seeded.tea_config4_states(n, n, seed, n=nrect)
+    rho = np.full((n, n), st[0]["density"])
+    en = np.full((n, n), st[0]["energy"])
+    xc = (np.arange(n) + 0.5) * (10.0 / n)
+    for s in st[1:]:
+        mx = (xc >= s["xmin"]) & (xc < s["xmax"])
+        my = (xc >= s["ymin"]) & (xc < s["ymax"])
+        m = my[:, None] & mx[None, :]
+        rho[m] = s["density"]
+        en[m] = s["energy"]
+    return rho, en
+
+
+def padded_problem(rho, en):
+    """Kx, Ky (tea_leaf_common_init_Kx_Ky_kernel with CONDUCTIVITY: face value
+    (w- + w) / (2 w- w), zero on the domain boundary) and u0 = energy * density,
+    as (ny + 2) x (nx + 2) arrays with a one-cell ring."""
+    ny, nx = rho.shape
+    Kx = np.zeros((ny + 2, nx + 2))
+    Ky = np.zeros((ny + 2, nx + 2))
+    w = rho
+    Kx[1:-1, 2:-1] = (w[:, :-1] + w[:, 1:]) / (2.0 * w[:, :-1] * w[:, 1:])
+    Ky[2:-1, 1:-1] = (w[:-1, :] + w[1:, :]) / (2.0 * w[:-1, :] * w[1:, :])
+    u0 = np.zeros((ny + 2, nx + 2))
+    u0[1:-1, 1:-1] = en * rho
+    return Kx, Ky, u0
+
+
+def interior(t, pitch):
+    """Pointer to the first interior cell of a padded field tensor."""
+    return ctypes.c_void_p(t.data_ptr() + (pitch + 1) * t.element_size())
+
+
+def solve(Kx, Ky, u0, u, rx, ry, method=PCG_TRUE, net=-1, eps=1e-10, max_iters=100000, window=40, r_out=None,
+          stream=None):
+    """Heat solve on padded (ny + 2, nx + 2) FP64 CUDA tensors; u is updated.
+    Returns the solve statistics as a dict."""
+    ny, nx = Kx.shape[0] - 2, Kx.shape[1] - 2
+    pitch = nx + 2
+    sysd = HeatSystem(nx, ny, pitch, interior(Kx, pitch), interior(Ky, pitch), interior(u0, pitch),
+                      interior(u, pitch), rx, ry)
+    st = HeatStats()
+    check(lib().ops_b200_heat_solve(ctypes.byref(sysd), method, net, eps, max_iters, window,
+                                    None if r_out is None else interior(r_out, pitch), ctypes.byref(st),
+                                    None if stream is None else ctypes.c_void_p(stream)))
+    return {k: getattr(st, k) for k, _ in HeatStats._fields_}
+
+
+class Net:
+    """Handle on a learned-preconditioner network held by the library."""
+
+    def __init__(self, seed=5):
+        self.h = lib().ops_b200_lmg_create(seed)
+        check(self.h)
+
+    def close(self):
+        if self.h >= 0:
+            lib().ops_b200_lmg_destroy(self.h)
+            self.h = -1
+
+    @staticmethod
+    def num_params():
+        return lib().ops_b200_lmg_num_params()
+
+    def params(self):
+        out = np.zeros(self.num_params(), dtype=np.float32)
+        check(lib().ops_b200_lmg_get_params(self.h, out.ctypes.data))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.num_params()
+        check(lib().ops_b200_lmg_set_params(self.h, p.ctypes.data))
+
+    def grads(self):
+        out = np.zeros(self.num_params(), dtype=np.float32)
+        check(lib().ops_b200_lmg_get_grads(self.h, out.ctypes.data))
+        return out
+
+    @staticmethod
+    def _batch(r, Kx, Ky, rx, ry):
+        n, hp, wp = r.shape
+        return HeatBatch(n, hp - 2, wp - 2, wp, hp * wp, interior(r[0], wp), interior(Kx[0], wp),
+                         interior(Ky[0], wp), rx, ry)
+
+    def apply(self, r, Kx, Ky, rx, ry, out):
+        """out = M(r) for a batch of padded (n, h + 2, w + 2) FP64 CUDA tensors."""
+        b = self._batch(r, Kx, Ky, rx, ry)
+        check(lib().ops_b200_lmg_apply(self.h, ctypes.byref(b), interior(out[0], r.shape[2]), None))
+
+    def train_step(self, r, Kx, Ky, e, rx, ry, lr):
+        """One forward/backward (and Adam step when lr > 0); returns the loss."""
+        b = self._batch(r, Kx, Ky, rx, ry)
+        loss = ctypes.c_double(0.0)
+        check(lib().ops_b200_lmg_train_step(self.h, ctypes.byref(b), interior(e[0], r.shape[2]), lr,
+                                            ctypes.byref(loss), None))
+        return loss.value
+
+
+def generate_pairs(nfields, n, seed0=1000, snaps=(2, 8, 32), rx_range=(100.0, 1000.0), device="cuda"):
+    """Residual/error pairs from Jacobi-PCG on `nfields` seeded n x n problems.
+    Field i uses seed seed0 + i and rx = ry log-uniform in rx_range (folded
+    into the coefficients, so the pairs are for rx = ry = 1). Returns padded
+    CUDA tensors r, e, Kx, Ky of shape (nfields * len(snaps), n + 2, n + 2)."""
+    import torch
+    m = nfields * len(snaps)
+    R = torch.zeros((m, n + 2, n + 2), dtype=torch.float64, device=device)
+    E = torch.zeros_like(R)
+    KX = torch.zeros_like(R)
+    KY = torch.zeros_like(R)
+    kx = torch.zeros((n + 2, n + 2), dtype=torch.float64, device=device)
+    ky, b, u, ustar, r = (torch.zeros_like(kx) for _ in range(5))
+    j = 0
+    for i in range(nfields):
+        rho, en = density_field(n, seed0 + i)
+        Kx, Ky, u0 = padded_problem(rho, en)
+        rx = float(rx_range[0] * (rx_range[1] / rx_range[0]) ** seeded.u01(seed0 + i, np.array([7], np.uint64))[0])
+        kx.copy_(torch.from_numpy(Kx * rx))
+        ky.copy_(torch.from_numpy(Ky * rx))
+        b.copy_(torch.from_numpy(u0))
+        ustar.copy_(b)
+        solve(kx, ky, b, ustar, 1.0, 1.0, method=PCG_TRUE, eps=1e-12, max_iters=100000)
+        for k in snaps:
+            u.copy_(b)
+            solve(kx, ky, b, u, 1.0, 1.0, method=PCG, eps=1e-30, max_iters=k, r_out=r)
+            R[j].copy_(r)
+            E[j].copy_(ustar - u)
+            KX[j].copy_(kx)
+            KY[j].copy_(ky)
+            j += 1
+    # the ring of r and e is not part of the pairs
+    for t in (R, E):
+        t[:, 0, :] = 0
+        t[:, -1, :] = 0
+        t[:, :, 0] = 0
+        t[:, :, -1] = 0
+    return R, E, KX, KY
+
+
+def train(net, data, steps=1000, batch=16, lr=1e-3, seed=0, log=None):
+    """Adam on random batches of the pairs; returns the loss history."""
+    import torch
+    R, E, KX, KY = data
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    hist = []
+    for it in range(steps):
+        idx = torch.randint(0, R.shape[0], (batch,), generator=g).to(R.device)
+        lr_t = lr * (0.1 if it > 0.8 * steps else 1.0)
+        L = net.train_step(R[idx].contiguous(), KX[idx].contiguous(), KY[idx].contiguous(), E[idx].contiguous(),
+                           1.0, 1.0, lr_t)
+        hist.append(L)
+        if log and (it % 100 == 0 or it == steps - 1):
+            log(f"step {it} loss {L:.4f}")
+    return hist

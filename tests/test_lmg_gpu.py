@@ -1,0 +1,124 @@
+"""Learned multigrid preconditioner on the B200 (no reference counterpart).
+
+1. The network's forward output and its parameter gradients (tcgen05 forward
+   and input-gradient convolutions, CUDA-core weight gradients) against the
+   numpy oracle (oracle/cnn.py), which rounds weights and stored activations
+   to BF16 where the kernels do. The kernels also store gradients in BF16 and
+   sum in another order, so the check is relative L2 per layer: within 5e-2
+   for gradients (a wrong backward is off by O(1)) and 2e-2 for the network
+   part of M(r).
+2. Training on residual/error pairs from Jacobi-PCG lowers the loss.
+3. Flexible CG with the trained network reaches the FP64 residual 1e-10 on
+   held-out fields in fewer iterations than Jacobi-PCG: the gain the network
+   brings over the same method without it."""
+import numpy as np
+import pytest
+
+from oracle import cnn as ref
+
+pytestmark = pytest.mark.gpu
+
+
+def small_problem(n=2, h=32, w=32, seed=3):
+    rng = np.random.default_rng(seed)
+    r = np.zeros((n, h + 2, w + 2))
+    e = np.zeros_like(r)
+    r[:, 1:-1, 1:-1] = rng.standard_normal((n, h, w))
+    e[:, 1:-1, 1:-1] = rng.standard_normal((n, h, w))
+    Kx = np.zeros_like(r)
+    Ky = np.zeros_like(r)
+    Kx[:, 1:-1, 2:-1] = rng.uniform(0.01, 5.0, (n, h, w - 1))
+    Ky[:, 2:-1, 1:-1] = rng.uniform(0.01, 5.0, (n, h - 1, w))
+    return r, Kx, Ky, e
+
+
+def cuda(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_forward_and_gradients_match_oracle(gpu_runtime):
+    import torch
+    from ops_b200 import lmg
+    r, Kx, Ky, e = small_problem()
+    p = ref.init_params(seed=1, out_scale=0.5)
+    net = lmg.Net(seed=1)
+    try:
+        net.set_params(p)
+        out = torch.zeros_like(cuda(r))
+        net.apply(cuda(r), cuda(Kx), cuda(Ky), 30.0, 30.0, out)
+        M_ref, A = ref.net_forward(p, r, Kx, Ky, 30.0, 30.0)
+        got = out.cpu().numpy()[:, 1:-1, 1:-1]
+        assert rel(got - A["z"], M_ref - A["z"]) < 2e-2
+        loss = net.train_step(cuda(r), cuda(Kx), cuda(Ky), cuda(e), 30.0, 30.0, 0.0)
+        L_ref, g_ref = ref.net_loss_grad(p, r, Kx, Ky, e, 30.0, 30.0)
+        assert abs(loss - L_ref) < 1e-3 * L_ref
+        g = net.grads().astype(np.float64)
+        o = 0
+        for l, (ci, co) in enumerate(ref.LAYERS):
+            k = 9 * ci * co + co
+            assert rel(g[o:o + k], g_ref[o:o + k]) < 5e-2, (l, rel(g[o:o + k], g_ref[o:o + k]))
+            o += k
+        assert rel(g[o:], g_ref[o:]) < 1e-2
+        assert np.array_equal(net.params(), p)   # lr = 0: no step
+    finally:
+        net.close()
+
+
+def test_untrained_network_is_jacobi(gpu_runtime):
+    import torch
+    from ops_b200 import lmg
+    r, Kx, Ky, _ = small_problem(seed=4)
+    net = lmg.Net(seed=2)
+    try:
+        out = torch.zeros_like(cuda(r))
+        net.apply(cuda(r), cuda(Kx), cuda(Ky), 30.0, 30.0, out)
+        _, A = ref.net_forward(net.params(), r, Kx, Ky, 30.0, 30.0)
+        np.testing.assert_allclose(out.cpu().numpy()[:, 1:-1, 1:-1], A["z"], rtol=1e-15, atol=0)
+    finally:
+        net.close()
+
+
+@pytest.fixture(scope="module")
+def trained(gpu_runtime):
+    from ops_b200 import lmg
+    data = lmg.generate_pairs(120, 64, seed0=1000, snaps=(2, 8, 32))
+    net = lmg.Net(seed=5)
+    hist = lmg.train(net, data, steps=400, batch=16, lr=2e-3)
+    yield net, hist
+    net.close()
+
+
+def test_training_lowers_loss(trained):
+    _, hist = trained
+    assert np.mean(hist[-40:]) < 0.7 * np.mean(hist[:10])
+
+
+def test_learned_fcg_beats_jacobi_pcg(trained):
+    import torch
+    from ops_b200 import lmg
+    net, _ = trained
+    n, rx = 64, 400.0
+    its_pcg, its_fcg = [], []
+    for seed in (90001, 90002, 90003):
+        rho, en = lmg.density_field(n, seed)
+        Kx, Ky, u0 = lmg.padded_problem(rho, en)
+        kx, ky, b = cuda(Kx), cuda(Ky), cuda(u0)
+        u = b.clone()
+        sp = lmg.solve(kx, ky, b, u, rx, rx, method=lmg.PCG_TRUE, eps=1e-10)
+        u2 = b.clone()
+        sj = lmg.solve(kx, ky, b, u2, rx, rx, method=lmg.FCG_JACOBI, eps=1e-10)
+        u3 = b.clone()
+        sl = lmg.solve(kx, ky, b, u3, rx, rx, method=lmg.FCG_LEARNED, net=net.h, eps=1e-10, window=40)
+        for s in (sp, sj, sl):
+            assert s["converged"] and s["final_residual"] < 1.5e-10 * s["initial_residual"]
+        assert abs(sj["iterations"] - sp["iterations"]) <= 0.1 * sp["iterations"] + 2
+        ua, uc = u.cpu().numpy(), u3.cpu().numpy()
+        assert rel(uc, ua) < 1e-8
+        its_pcg.append(sp["iterations"])
+        its_fcg.append(sl["iterations"])
+    assert sum(its_fcg) < 0.8 * sum(its_pcg), (its_fcg, its_pcg)
