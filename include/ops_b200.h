@@ -343,7 +343,7 @@ int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, do
 /* ---- learned multigrid preconditioner (no reference counterpart) ---------
  * A 4-level U-Net-shaped CNN (16/32/64/64 channels, 3x3 BF16 convolutions on
  * the tensor cores, FP32 accumulation) mapping a residual and the face
- * coefficients to M(r) = r / diag(A) + s * net(...), s = rms(r / diag(A));
+ * coefficients to M(r) = r / diag(A) + s * net(r / s, ...), s = rms(r);
  * trained on residual/error pairs (loss mean_n ||M(r_n) - e_n||^2 / ||e_n||^2)
  * by the library's own forward and backward kernels with Adam. A batch is n
  * fields of h x w interior cells (multiples of 8) laid out like
@@ -366,9 +366,11 @@ int ops_b200_lmg_get_grads(int net, float *host);          /* of the last train 
 /* out (device, batch layout) = M(r). Synchronous on `stream`. */
 int ops_b200_lmg_apply(int net, const ops_b200_heat_batch *b, double *out, void *stream);
 /* Forward + backward on a batch with targets e (device, batch layout); one
- * Adam step when lr > 0; *loss receives the batch loss before the step. */
-int ops_b200_lmg_train_step(int net, const ops_b200_heat_batch *b, const double *e, double lr, double *loss,
-                            void *stream);
+ * Adam step when lr > 0; *loss receives the batch loss before the step.
+ * loss_kind 0: mean_n ||M(r) - e||^2 / ||e||^2; 1: the same ratio in the
+ * A-norm, d.Ad / e.Ae with d = M(r) - e (what CG convergence depends on). */
+int ops_b200_lmg_train_step(int net, const ops_b200_heat_batch *b, const double *e, int loss_kind, double lr,
+                            double *loss, void *stream);
 
 #ifdef __cplusplus
 }

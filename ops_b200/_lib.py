@@ -153,7 +153,7 @@ def _declare(L):
         "ops_b200_lmg_set_params": ([i, P], i),
         "ops_b200_lmg_get_grads": ([i, P], i),
         "ops_b200_lmg_apply": ([i, P, P, P], i),
-        "ops_b200_lmg_train_step": ([i, P, P, ctypes.c_double, P, P], i),
+        "ops_b200_lmg_train_step": ([i, P, P, i, ctypes.c_double, P, P], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

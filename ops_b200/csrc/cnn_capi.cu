@@ -88,6 +88,14 @@ struct HeatWorkspace {
 };
 
 std::mutex g_mu;
+cudaStream_t own_stream() {
+  static cudaStream_t st[64] = {nullptr};
+  int dev = 0;
+  OPSB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error(E_CUDA, "device index out of range");
+  if (!st[dev]) OPSB_CUDA(cudaStreamCreate(&st[dev]));
+  return st[dev];
+}
 HeatWorkspace &workspace() {
   static HeatWorkspace ws;
   return ws;
@@ -132,7 +140,11 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
     if (method < OPS_B200_HEAT_PCG || method > OPS_B200_HEAT_FCG_JACOBI) throw Error(E_ARG, "heat system: method");
     if (!(eps > 0.0) || max_iters < 0) throw Error(E_ARG, "heat system: eps > 0 and max_iters >= 0 required");
     std::lock_guard<std::mutex> lk(g_mu);
+    // the iteration chunks are replayed from CUDA graphs, which cannot be
+    // captured on the legacy NULL stream: a NULL stream means the library's own
+    // blocking stream (ordered with the NULL stream both ways)
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!s) s = own_stream();
     HeatWorkspace &ws = workspace();
     ws.ensure(sys->nx, sys->ny, sys->pitch, s);
     heat::Field2D f;
@@ -273,15 +285,16 @@ extern "C" int ops_b200_lmg_apply(int net, const ops_b200_heat_batch *b, double 
   });
 }
 
-extern "C" int ops_b200_lmg_train_step(int net, const ops_b200_heat_batch *b, const double *e, double lr,
-                                       double *loss, void *stream) {
+extern "C" int ops_b200_lmg_train_step(int net, const ops_b200_heat_batch *b, const double *e, int loss_kind,
+                                       double lr, double *loss, void *stream) {
   using namespace opsb;
   return capi_guard([&] {
     if (!e) throw Error(E_ARG, "null target");
     lmg::Fields f = fields_of(b);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     lmg::Net &nt = net_of(net);
-    const double L = nt.loss_and_grad(f, e, s);
+    if (loss_kind != lmg::LOSS_L2 && loss_kind != lmg::LOSS_ANORM) throw Error(E_ARG, "loss_kind must be 0 or 1");
+    const double L = nt.loss_and_grad(f, e, loss_kind, s);
     if (lr > 0.0) nt.adam(lr, s);
     OPSB_CUDA(cudaStreamSynchronize(s));
     if (loss) *loss = L;

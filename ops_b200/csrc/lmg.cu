@@ -107,7 +107,7 @@ __device__ __forceinline__ Coef coef(const Fields &f, int n, int y, int x) {
   return k;
 }
 
-// Per image, per block: partial sums of z^2, z = r / D.
+// Per image, per block: partial sums of r^2.
 __global__ void k_zsq(Fields f, double *part) {
   __shared__ double sm[kT / 32];
   const int n = blockIdx.y;
@@ -115,15 +115,14 @@ __global__ void k_zsq(Fields f, double *part) {
   double acc = 0.0;
   for (int p = blockIdx.x * kT + threadIdx.x; p < hw; p += gridDim.x * kT) {
     const int y = p / f.w, x = p - y * f.w;
-    const Coef k = coef(f, n, y, x);
-    const double z = f.r[n * f.image + (long long)y * f.pitch + x] / k.D;
-    acc += z * z;
+    const double r = f.r[n * f.image + (long long)y * f.pitch + x];
+    acc += r * r;
   }
   acc = block_sum_d(acc, sm);
   if (threadIdx.x == 0) part[n * gridDim.x + blockIdx.x] = acc;
 }
 
-// s[n] = rms(z) (1 when the residual is zero), partials added in block order.
+// s[n] = rms(r) (1 when the residual is zero), partials added in block order.
 __global__ void k_scale(const double *part, int nblk, int hw, double *s, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -140,9 +139,8 @@ __global__ void k_features(Fields f, const double *s, bf16 *x0) {
     const int rem = (int)(p - (long long)n * f.h * f.w);
     const int y = rem / f.w, x = rem - y * f.w;
     const Coef k = coef(f, n, y, x);
-    const double z = f.r[n * f.image + (long long)y * f.pitch + x] / k.D;
     float v[16] = {0};
-    v[0] = (float)(z / s[n]);
+    v[0] = (float)(f.r[n * f.image + (long long)y * f.pitch + x] / s[n]);
     v[1] = (float)(k.a / k.D);
     v[2] = (float)(k.b / k.D);
     v[3] = (float)(k.c / k.D);
@@ -274,15 +272,17 @@ __global__ void k_out(Fields f, const double *s, const bf16 *h0, const float *pa
   }
 }
 
-// Loss partials per image: sum (pred - e)^2 and sum e^2.
-__global__ void k_loss_part(Fields f, const float *pred, const double *e, double *part) {
+// d = pred - e in place (FP32, dense n x h x w); per-image partials of d.d
+// and e.e (the L2 loss).
+__global__ void k_diff(Fields f, float *pd, const double *e, double *part) {
   __shared__ double sm[kT / 32];
   const int n = blockIdx.y, hw = f.h * f.w;
   double a = 0.0, b = 0.0;
   for (int p = blockIdx.x * kT + threadIdx.x; p < hw; p += gridDim.x * kT) {
     const int y = p / f.w, x = p - y * f.w;
     const double ev = e[n * f.image + (long long)y * f.pitch + x];
-    const double d = (double)pred[(long long)n * hw + p] - ev;
+    const double d = (double)pd[(long long)n * hw + p] - ev;
+    pd[(long long)n * hw + p] = (float)d;
     a += d * d;
     b += ev * ev;
   }
@@ -294,7 +294,35 @@ __global__ void k_loss_part(Fields f, const float *pred, const double *e, double
   }
 }
 
-// Per image: E[n] = ||e||^2; loss = mean_n ||pred - e||^2 / E[n] (one thread).
+// A-norm loss: G = A d (the heat operator on the interior, d zero outside)
+// and per-image partials of d.(A d) and e.(A e).
+__global__ void k_anorm(Fields f, const float *d, const double *e, float *G, double *part) {
+  __shared__ double sm[kT / 32];
+  const int n = blockIdx.y, hw = f.h * f.w;
+  const float *dn = d + (long long)n * hw;
+  double a = 0.0, b = 0.0;
+  for (int p = blockIdx.x * kT + threadIdx.x; p < hw; p += gridDim.x * kT) {
+    const int y = p / f.w, x = p - y * f.w;
+    const Coef k = coef(f, n, y, x);
+    const double dc = dn[p];
+    const double dw = x > 0 ? dn[p - 1] : 0.0, de = x + 1 < f.w ? dn[p + 1] : 0.0;
+    const double ds = y > 0 ? dn[p - f.w] : 0.0, dnn = y + 1 < f.h ? dn[p + f.w] : 0.0;
+    const double Ad = k.D * dc - k.a * dw - k.b * de - k.c * ds - k.d * dnn;
+    const long long i = n * f.image + (long long)y * f.pitch + x;
+    const double Ae = k.D * e[i] - k.a * e[i - 1] - k.b * e[i + 1] - k.c * e[i - f.pitch] - k.d * e[i + f.pitch];
+    G[(long long)n * hw + p] = (float)Ad;
+    a += dc * Ad;
+    b += e[i] * Ae;
+  }
+  a = block_sum_d(a, sm);
+  b = block_sum_d(b, sm);
+  if (threadIdx.x == 0) {
+    part[(n * gridDim.x + blockIdx.x) * 2] = a;
+    part[(n * gridDim.x + blockIdx.x) * 2 + 1] = b;
+  }
+}
+
+// Per image: E[n] = ||e||^2 (or e.Ae); loss = mean_n d.d / E[n] (or d.Ad / E[n]) (one thread).
 __global__ void k_loss_finish(const double *part, int nblk, int n, double *E, double *loss) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double L = 0.0;
@@ -311,10 +339,11 @@ __global__ void k_loss_finish(const double *part, int nblk, int n, double *E, do
   *loss = L / (double)n;
 }
 
-// dL/dy = (2 / n) s (pred - e) / E, then through the output layer:
-// g0u = dy * wout * (h0 > 0); per-block partials of dwout = sum dy h0, dbout = sum dy.
-__global__ void k_out_bwd(Fields f, const double *s, const double *E, const float *pred, const double *e,
-                          const bf16 *h0, const float *params, int wout_off, bf16 *g0u, float *part) {
+// dL/dy = (2 / n) s G / E with G = pred - e (L2) or A (pred - e) (A-norm),
+// then through the output layer: g0u = dy * wout * (h0 > 0); per-block
+// partials of dwout = sum dy h0, dbout = sum dy.
+__global__ void k_out_bwd(Fields f, const double *s, const double *E, const float *G, const bf16 *h0,
+                          const float *params, int wout_off, bf16 *g0u, float *part) {
   __shared__ float wsm[16];
   __shared__ double sm[kT / 32];
   if (threadIdx.x < 16) wsm[threadIdx.x] = params[wout_off + threadIdx.x];
@@ -327,8 +356,9 @@ __global__ void k_out_bwd(Fields f, const double *s, const double *E, const floa
     const int n = (int)(p / ((long long)f.h * f.w));
     const int rem = (int)(p - (long long)n * f.h * f.w);
     const int y = rem / f.w, x = rem - y * f.w;
-    const double ev = e[n * f.image + (long long)y * f.pitch + x];
-    const double dm = 2.0 / (double)f.n * ((double)pred[p] - ev) / E[n];
+    (void)y;
+    (void)x;
+    const double dm = 2.0 / (double)f.n * (double)G[p] / E[n];
     const float dy = (float)(dm * s[n]);
     float v[16], g[16];
     ld8(h0 + p * 16, v);
@@ -485,7 +515,7 @@ struct Net::Impl {
   char *act = nullptr;
   bf16 *x0, *e0, *u0, *h0, *p1, *a1, *e1, *u1, *h1, *p2, *a2, *e2, *u2, *h2, *p3, *a3, *h3;
   bf16 *g0u, *du0, *ge0, *g1u, *du1, *ge1, *ga1, *dp1, *g2u, *du2, *ge2, *ga2, *dp2, *g3b, *ga3, *dp3;
-  float *pred = nullptr, *wpart = nullptr, *opart = nullptr;
+  float *pred = nullptr, *gbuf = nullptr, *wpart = nullptr, *opart = nullptr;
   double *dscal = nullptr;  // s[n], E[n], loss, partials
   int zblk = 0;
 
@@ -521,13 +551,15 @@ struct Net::Impl {
     const size_t wpart_b = ((size_t)kWgX * maxlen * 4 + 255) / 256 * 256;
     const size_t opart_b = ((size_t)148 * 16 * 17 * 4 + 255) / 256 * 256;
     const size_t dscal_b = ((size_t)(2 * n + 1 + 2 * n * zblk) * 8 + 255) / 256 * 256;
-    check(cudaMalloc(&act, bytes + pred_b + wpart_b + opart_b + dscal_b), "learned preconditioner buffers");
+    check(cudaMalloc(&act, bytes + 2 * pred_b + wpart_b + opart_b + dscal_b), "learned preconditioner buffers");
     char *c = act;
     for (auto &b : list) {
       *b.p = reinterpret_cast<bf16 *>(c);
       c += ((size_t)b.elems * 2 + 255) / 256 * 256;
     }
     pred = reinterpret_cast<float *>(c);
+    c += pred_b;
+    gbuf = reinterpret_cast<float *>(c);
     c += pred_b;
     wpart = reinterpret_cast<float *>(c);
     c += wpart_b;
@@ -652,7 +684,7 @@ void wgrad(const bf16 *x, const bf16 *g, int n, int h, int w, float *wpart, floa
 }
 }  // namespace
 
-double Net::loss_and_grad(const Fields &f, const double *e, cudaStream_t s) {
+double Net::loss_and_grad(const Fields &f, const double *e, int kind, cudaStream_t s) {
   Impl &m = *m_;
   m.ensure(f.n, f.h, f.w);
   check(cudaMemsetAsync(cnn::error_word(), 0, sizeof(int), s), "conv error word");
@@ -661,10 +693,16 @@ double Net::loss_and_grad(const Fields &f, const double *e, cudaStream_t s) {
   const int n = f.n, h = f.h, w = f.w;
   k_out<<<blocks_for((long long)n * h * w), kT, 0, s>>>(f, m.dscal, m.h0, m.params, o.wout, nullptr, 0, 0, m.pred);
   double *E = m.dscal + n, *loss = m.dscal + 2 * n, *lpart = m.dscal + 2 * n + 1;
-  k_loss_part<<<dim3(m.zblk, n), kT, 0, s>>>(f, m.pred, e, lpart);
+  k_diff<<<dim3(m.zblk, n), kT, 0, s>>>(f, m.pred, e, lpart);
+  const float *G = m.pred;
+  if (kind == LOSS_ANORM) {
+    k_anorm<<<dim3(m.zblk, n), kT, 0, s>>>(f, m.pred, e, m.gbuf, lpart);
+    G = m.gbuf;
+    launches_ += 1;
+  }
   k_loss_finish<<<1, 32, 0, s>>>(lpart, m.zblk, n, E, loss);
   const int ob = blocks_for((long long)n * h * w);
-  k_out_bwd<<<ob, kT, 0, s>>>(f, m.dscal, E, m.pred, e, m.h0, m.params, o.wout, m.g0u, m.opart);
+  k_out_bwd<<<ob, kT, 0, s>>>(f, m.dscal, E, G, m.h0, m.params, o.wout, m.g0u, m.opart);
   k_sum_parts<<<1, kT, 0, s>>>(m.opart, ob, 17, m.grads + o.wout);
   launches_ += 6;
   const int h1 = h / 2, w1 = w / 2, h2 = h / 4, w2 = w / 4, h3 = h / 8, w3 = w / 8;
@@ -686,17 +724,17 @@ double Net::loss_and_grad(const Fields &f, const double *e, cudaStream_t s) {
   k_add_poolT_mask<<<blocks_for((long long)n * h * w * 2), kT, 0, s>>>(m.du0, m.dp1, m.e0, m.ge0, n, h, w, 16);
   launches_ += 16;
   // weight gradients (CUDA cores, fixed-order partial sums)
-  float *G = m.grads;
-  wgrad<16, 16>(m.u0, m.g0u, n, h, w, m.wpart, G + o.w[C0U], s);
-  wgrad<32, 16>(m.u1, m.g1u, n, h1, w1, m.wpart, G + o.w[C1U], s);
-  wgrad<64, 32>(m.u2, m.g2u, n, h2, w2, m.wpart, G + o.w[C2U], s);
-  wgrad<64, 64>(m.a3, m.g3b, n, h3, w3, m.wpart, G + o.w[C3B], s);
-  wgrad<64, 64>(m.p3, m.ga3, n, h3, w3, m.wpart, G + o.w[C3A], s);
-  wgrad<64, 64>(m.a2, m.ge2, n, h2, w2, m.wpart, G + o.w[C2B], s);
-  wgrad<32, 64>(m.p2, m.ga2, n, h2, w2, m.wpart, G + o.w[C2A], s);
-  wgrad<32, 32>(m.a1, m.ge1, n, h1, w1, m.wpart, G + o.w[C1B], s);
-  wgrad<16, 32>(m.p1, m.ga1, n, h1, w1, m.wpart, G + o.w[C1A], s);
-  wgrad<16, 16>(m.x0, m.ge0, n, h, w, m.wpart, G + o.w[C0], s);
+  float *WG = m.grads;
+  wgrad<16, 16>(m.u0, m.g0u, n, h, w, m.wpart, WG + o.w[C0U], s);
+  wgrad<32, 16>(m.u1, m.g1u, n, h1, w1, m.wpart, WG + o.w[C1U], s);
+  wgrad<64, 32>(m.u2, m.g2u, n, h2, w2, m.wpart, WG + o.w[C2U], s);
+  wgrad<64, 64>(m.a3, m.g3b, n, h3, w3, m.wpart, WG + o.w[C3B], s);
+  wgrad<64, 64>(m.p3, m.ga3, n, h3, w3, m.wpart, WG + o.w[C3A], s);
+  wgrad<64, 64>(m.a2, m.ge2, n, h2, w2, m.wpart, WG + o.w[C2B], s);
+  wgrad<32, 64>(m.p2, m.ga2, n, h2, w2, m.wpart, WG + o.w[C2A], s);
+  wgrad<32, 32>(m.a1, m.ge1, n, h1, w1, m.wpart, WG + o.w[C1B], s);
+  wgrad<16, 32>(m.p1, m.ga1, n, h1, w1, m.wpart, WG + o.w[C1A], s);
+  wgrad<16, 16>(m.x0, m.ge0, n, h, w, m.wpart, WG + o.w[C0], s);
   check(cudaGetLastError(), "learned preconditioner backward");
   launches_ += 20;
   double L = 0.0;

@@ -14,8 +14,8 @@
 //   h1  = relu(C1u (up h2 + e1))                    16 ch, H/2
 //   h0  = relu(C0u (up h1 + e0))                    16 ch, H
 //   y   = wout . h0 + bout                          1 ch, FP32
-//   M(r) = z + s y,  z = r / diag(A),  s = rms(z) per image
-// Features: z / s and the four normalised face weights a/D, b/D, c/D, d/D
+//   M(r) = z + s y,  z = r / diag(A),  s = rms(r) per image
+// Features: r / s and the four normalised face weights a/D, b/D, c/D, d/D
 // (a = rx Kx(i), b = rx Kx(i+1), c = ry Ky(j), d = ry Ky(j+1),
 // D = 1 + a + b + c + d = diag(A)). The output layer starts at zero, so an
 // untrained network is the Jacobi preconditioner.
@@ -39,6 +39,7 @@ struct Fields {
 };
 
 constexpr int kLayers = 10;
+enum { LOSS_L2 = 0, LOSS_ANORM = 1 };
 
 class Net {
  public:
@@ -58,9 +59,10 @@ class Net {
   // buffers for (n, h, w) on first use.
   void apply(const Fields &f, double *out, cudaStream_t s);
   // Forward + backward for a batch with targets e (same layout as f);
-  // gradients of loss = mean_n ||M(r_n) - e_n||^2 / ||e_n||^2 land in the
-  // gradient buffer. Returns the loss.
-  double loss_and_grad(const Fields &f, const double *e, cudaStream_t s);
+  // gradients of loss = mean_n ||M(r_n) - e_n||^2 / ||e_n||^2 (LOSS_L2) or of
+  // the same ratio in the A-norm, (d.Ad) / (e.Ae) with d = M(r_n) - e_n
+  // (LOSS_ANORM), land in the gradient buffer. Returns the loss.
+  double loss_and_grad(const Fields &f, const double *e, int kind, cudaStream_t s);
   // One Adam step on the stored gradients.
   void adam(double lr, cudaStream_t s);
   long long launches() const { return launches_; }

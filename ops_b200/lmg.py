@@ -8,7 +8,10 @@ Pipeline, all arithmetic on the GPU through the library's C-ABI:
      truncated solves from the same start give u_k, r_k = u0 - A u_k and
      e_k = u* - u_k,
   3. training of the network (tcgen05 forward and input-gradient
-     convolutions, CUDA-core weight gradients, Adam),
+     convolutions, CUDA-core weight gradients, Adam) on the A-norm error
+     ||M(r) - e||_A / ||e||_A, then rounds of on-policy pairs taken along the
+     learned FCG's own iterates and retraining (a network trained only on
+     PCG residuals stalls FCG once the residuals leave that distribution),
   4. flexible CG with the trained network as preconditioner, falling back to
      Jacobi-PCG when the network stops helping.
 Device buffers are torch CUDA tensors (allocation only)."""
@@ -119,13 +122,14 @@ class Net:
         b = self._batch(r, Kx, Ky, rx, ry)
         check(lib().ops_b200_lmg_apply(self.h, ctypes.byref(b), interior(out[0], r.shape[2]), None))
 
-    def train_step(self, r, Kx, Ky, e, rx, ry, lr):
-        """One forward/backward (and Adam step when lr > 0); returns the loss."""
+    def train_step(self, r, Kx, Ky, e, rx, ry, lr, loss="anorm"):
+        """One forward/backward (and Adam step when lr > 0); returns the loss
+        ("l2": ||M(r) - e||^2 / ||e||^2, "anorm": the same in the A-norm)."""
         b = self._batch(r, Kx, Ky, rx, ry)
-        loss = ctypes.c_double(0.0)
-        check(lib().ops_b200_lmg_train_step(self.h, ctypes.byref(b), interior(e[0], r.shape[2]), lr,
-                                            ctypes.byref(loss), None))
-        return loss.value
+        out = ctypes.c_double(0.0)
+        check(lib().ops_b200_lmg_train_step(self.h, ctypes.byref(b), interior(e[0], r.shape[2]),
+                                            {"l2": 0, "anorm": 1}[loss], lr, ctypes.byref(out), None))
+        return out.value
 
 
 def generate_pairs(nfields, n, seed0=1000, snaps=(2, 8, 32), rx_range=(100.0, 1000.0), device="cuda"):
@@ -168,7 +172,61 @@ def generate_pairs(nfields, n, seed0=1000, snaps=(2, 8, 32), rx_range=(100.0, 10
     return R, E, KX, KY
 
 
-def train(net, data, steps=1000, batch=16, lr=1e-3, seed=0, log=None):
+def generate_on_policy(net, nfields, n, seed0, snaps=(2, 4, 8, 16, 32, 64), rx_range=(100.0, 1000.0),
+                       device="cuda"):
+    """Residual/error pairs along the learned FCG's own trajectory: like
+    generate_pairs, but u_k comes from k iterations of flexible CG with the
+    current network, so the pairs are the residuals the network meets when
+    it is used as a preconditioner."""
+    import torch
+    m = nfields * len(snaps)
+    R = torch.zeros((m, n + 2, n + 2), dtype=torch.float64, device=device)
+    E, KX, KY = (torch.zeros_like(R) for _ in range(3))
+    kx = torch.zeros((n + 2, n + 2), dtype=torch.float64, device=device)
+    ky, b, u, ustar, r = (torch.zeros_like(kx) for _ in range(5))
+    j = 0
+    for i in range(nfields):
+        rho, en = density_field(n, seed0 + i)
+        Kx, Ky, u0 = padded_problem(rho, en)
+        rx = float(rx_range[0] * (rx_range[1] / rx_range[0]) ** seeded.u01(seed0 + i, np.array([7], np.uint64))[0])
+        kx.copy_(torch.from_numpy(Kx * rx))
+        ky.copy_(torch.from_numpy(Ky * rx))
+        b.copy_(torch.from_numpy(u0))
+        ustar.copy_(b)
+        solve(kx, ky, b, ustar, 1.0, 1.0, method=PCG_TRUE, eps=1e-12, max_iters=100000)
+        for k in snaps:
+            u.copy_(b)
+            solve(kx, ky, b, u, 1.0, 1.0, method=FCG_LEARNED, net=net.h, eps=1e-30, window=0, max_iters=k, r_out=r)
+            R[j].copy_(r)
+            E[j].copy_(ustar - u)
+            KX[j].copy_(kx)
+            KY[j].copy_(ky)
+            j += 1
+    for t in (R, E):
+        t[:, 0, :] = 0
+        t[:, -1, :] = 0
+        t[:, :, 0] = 0
+        t[:, :, -1] = 0
+    return R, E, KX, KY
+
+
+def fit(net, n=128, nfields=300, steps=1500, rounds=3, lr=2e-3, batch=16, seed0=1000, log=None):
+    """The training recipe: PCG pairs, then `rounds` rounds of on-policy pairs
+    (half as many fields each, new seeds) added to the set, training after
+    each. Returns the loss history of every round."""
+    import torch
+    data = generate_pairs(nfields, n, seed0=seed0)
+    hists = [train(net, data, steps=steps, batch=batch, lr=lr, seed=0)]
+    for rd in range(rounds):
+        extra = generate_on_policy(net, max(1, nfields // 2), n, seed0 + 100000 * (rd + 1))
+        data = tuple(torch.cat([a, b]) for a, b in zip(data, extra))
+        hists.append(train(net, data, steps=steps, batch=batch, lr=0.5 * lr, seed=rd + 1))
+        if log:
+            log(f"round {rd + 1}: {data[0].shape[0]} pairs, loss {np.mean(hists[-1][-50:]):.4f}")
+    return hists
+
+
+def train(net, data, steps=1000, batch=16, lr=1e-3, seed=0, log=None, loss="anorm"):
     """Adam on random batches of the pairs; returns the loss history."""
     import torch
     R, E, KX, KY = data
@@ -178,7 +236,7 @@ def train(net, data, steps=1000, batch=16, lr=1e-3, seed=0, log=None):
         idx = torch.randint(0, R.shape[0], (batch,), generator=g).to(R.device)
         lr_t = lr * (0.1 if it > 0.8 * steps else 1.0)
         L = net.train_step(R[idx].contiguous(), KX[idx].contiguous(), KY[idx].contiguous(), E[idx].contiguous(),
-                           1.0, 1.0, lr_t)
+                           1.0, 1.0, lr_t, loss)
         hist.append(L)
         if log and (it % 100 == 0 or it == steps - 1):
             log(f"step {it} loss {L:.4f}")

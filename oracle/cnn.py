@@ -67,12 +67,13 @@ def features(r, Kx, Ky, rx, ry):
     c = ry * Ky[:, 1:-1, 1:-1]
     d = ry * Ky[:, 2:, 1:-1]
     D = 1.0 + a + b + c + d
-    z = r[:, 1:-1, 1:-1] / D
-    s = np.sqrt(np.mean(z ** 2, axis=(1, 2)))
+    ri = r[:, 1:-1, 1:-1]
+    z = ri / D
+    s = np.sqrt(np.mean(ri ** 2, axis=(1, 2)))
     s = np.where(s > 0, s, 1.0)
     n, h, w = z.shape
     x0 = np.zeros((n, h, w, 16), dtype=np.float64)
-    x0[..., 0] = z / s[:, None, None]
+    x0[..., 0] = ri / s[:, None, None]
     x0[..., 1] = a / D
     x0[..., 2] = b / D
     x0[..., 3] = c / D
@@ -150,18 +151,37 @@ def conv_bwd(x, W, g):
     return dxp[:, 1:-1, 1:-1, :], dW, g2.sum(axis=0)
 
 
-def net_loss_grad(p, r, Kx, Ky, e, rx, ry, bf16=True):
-    """loss = mean_n ||M(r_n) - e_n||^2 / ||e_n||^2 and its gradient (float64)
-    with respect to the flat parameters, back-propagated through the stored
-    (rounded) activations."""
+def apply_A(u, Kx, Ky, rx, ry):
+    """The heat operator on interior arrays u (n, h, w), zero outside."""
+    a = rx * Kx[:, 1:-1, 1:-1]
+    b = rx * Kx[:, 1:-1, 2:]
+    c = ry * Ky[:, 1:-1, 1:-1]
+    d = ry * Ky[:, 2:, 1:-1]
+    up_ = np.pad(u, ((0, 0), (1, 1), (1, 1)))
+    return ((1 + a + b + c + d) * u - a * up_[:, 1:-1, :-2] - b * up_[:, 1:-1, 2:] - c * up_[:, :-2, 1:-1]
+            - d * up_[:, 2:, 1:-1])
+
+
+def net_loss_grad(p, r, Kx, Ky, e, rx, ry, bf16=True, anorm=False):
+    """loss = mean_n ||M(r_n) - e_n||^2 / ||e_n||^2 (or, with anorm, the same
+    ratio in the A-norm: d.Ad / e.Ae with d = M(r_n) - e_n) and its gradient
+    (float64) with respect to the flat parameters, back-propagated through the
+    stored (rounded) activations."""
     L, wout, bout = unpack(p)
     M, A = net_forward(p, r, Kx, Ky, rx, ry, bf16)
     Wb = A["W"]
     ei = e[:, 1:-1, 1:-1]
     n = r.shape[0]
-    E = np.sum(ei ** 2, axis=(1, 2))
-    loss = float(np.mean(np.sum((M - ei) ** 2, axis=(1, 2)) / E))
-    dM = 2.0 / n * (M - ei) / E[:, None, None]
+    d = M - ei
+    if anorm:
+        Ad = apply_A(d, Kx, Ky, rx, ry)
+        E = np.sum(ei * apply_A(ei, Kx, Ky, rx, ry), axis=(1, 2))
+        loss = float(np.mean(np.sum(d * Ad, axis=(1, 2)) / E))
+        dM = 2.0 / n * Ad / E[:, None, None]
+    else:
+        E = np.sum(ei ** 2, axis=(1, 2))
+        loss = float(np.mean(np.sum(d ** 2, axis=(1, 2)) / E))
+        dM = 2.0 / n * d / E[:, None, None]
     dy = dM * A["s"][:, None, None]
     grads = [None] * 10
     dwout = np.einsum("nhw,nhwc->c", dy, A["h0"])

@@ -2,6 +2,7 @@
 differences on the CPU: the exact (FP64, unrounded) network's analytic
 gradient must match central differences of its loss."""
 import numpy as np
+import pytest
 
 from oracle import cnn as ref
 
@@ -19,10 +20,11 @@ def small_problem(n=2, h=16, w=16, seed=3):
     return r, Kx, Ky, e
 
 
-def test_oracle_gradient_matches_finite_differences():
+@pytest.mark.parametrize("anorm", [False, True])
+def test_oracle_gradient_matches_finite_differences(anorm):
     r, Kx, Ky, e = small_problem()
     p = ref.init_params(seed=1, out_scale=0.5).astype(np.float64)
-    loss, g = ref.net_loss_grad(p, r, Kx, Ky, e, 30.0, 30.0, bf16=False)
+    loss, g = ref.net_loss_grad(p, r, Kx, Ky, e, 30.0, 30.0, bf16=False, anorm=anorm)
     rng = np.random.default_rng(0)
     idx = np.concatenate([rng.choice(p.size - 17, 24, replace=False), np.arange(p.size - 17, p.size)])
     for i in idx:
@@ -30,8 +32,8 @@ def test_oracle_gradient_matches_finite_differences():
         pp, pm = p.copy(), p.copy()
         pp[i] += h
         pm[i] -= h
-        lp, _ = ref.net_loss_grad(pp, r, Kx, Ky, e, 30.0, 30.0, bf16=False)
-        lm, _ = ref.net_loss_grad(pm, r, Kx, Ky, e, 30.0, 30.0, bf16=False)
+        lp, _ = ref.net_loss_grad(pp, r, Kx, Ky, e, 30.0, 30.0, bf16=False, anorm=anorm)
+        lm, _ = ref.net_loss_grad(pm, r, Kx, Ky, e, 30.0, 30.0, bf16=False, anorm=anorm)
         fd = (lp - lm) / (2 * h)
         assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(fd)), (i, fd, g[i])
     assert loss > 0

@@ -54,16 +54,17 @@ def test_forward_and_gradients_match_oracle(gpu_runtime):
         M_ref, A = ref.net_forward(p, r, Kx, Ky, 30.0, 30.0)
         got = out.cpu().numpy()[:, 1:-1, 1:-1]
         assert rel(got - A["z"], M_ref - A["z"]) < 2e-2
-        loss = net.train_step(cuda(r), cuda(Kx), cuda(Ky), cuda(e), 30.0, 30.0, 0.0)
-        L_ref, g_ref = ref.net_loss_grad(p, r, Kx, Ky, e, 30.0, 30.0)
-        assert abs(loss - L_ref) < 1e-3 * L_ref
-        g = net.grads().astype(np.float64)
-        o = 0
-        for l, (ci, co) in enumerate(ref.LAYERS):
-            k = 9 * ci * co + co
-            assert rel(g[o:o + k], g_ref[o:o + k]) < 5e-2, (l, rel(g[o:o + k], g_ref[o:o + k]))
-            o += k
-        assert rel(g[o:], g_ref[o:]) < 1e-2
+        for kind in ("l2", "anorm"):
+            loss = net.train_step(cuda(r), cuda(Kx), cuda(Ky), cuda(e), 30.0, 30.0, 0.0, loss=kind)
+            L_ref, g_ref = ref.net_loss_grad(p, r, Kx, Ky, e, 30.0, 30.0, anorm=kind == "anorm")
+            assert abs(loss - L_ref) < 1e-3 * L_ref, kind
+            g = net.grads().astype(np.float64)
+            o = 0
+            for l, (ci, co) in enumerate(ref.LAYERS):
+                k = 9 * ci * co + co
+                assert rel(g[o:o + k], g_ref[o:o + k]) < 5e-2, (kind, l, rel(g[o:o + k], g_ref[o:o + k]))
+                o += k
+            assert rel(g[o:], g_ref[o:]) < 1e-2, kind
         assert np.array_equal(net.params(), p)   # lr = 0: no step
     finally:
         net.close()
