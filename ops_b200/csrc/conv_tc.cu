@@ -129,12 +129,13 @@ struct Cfg {
   static constexpr int A_BYTES = kTileM * S;
   static constexpr int W_TAP = COUT * S;
   static constexpr int W_BYTES = 9 * W_TAP;
-  static constexpr int STAGES = CIN == 16 ? 12 : 8;
-  static constexpr int TMEM_COLS = 2 * COUT;           // two accumulator buffers (32, 64 or 128 columns)
+  static constexpr int STAGES = CIN == 16 ? 16 : 8;
+  static constexpr int NACC = 4;                       // accumulator buffers in tensor memory
+  static constexpr int TMEM_COLS = NACC * COUT;        // 64, 128 or 256 columns
   static constexpr int OFF_W = 0;
   static constexpr int OFF_A = (W_BYTES + 1023) / 1024 * 1024;
   static constexpr int OFF_BAR = OFF_A + STAGES * A_BYTES;
-  static constexpr int NBAR = 2 * STAGES + 5;
+  static constexpr int NBAR = 2 * STAGES + 2 * NACC + 1;
   static constexpr int SMEM = OFF_BAR + NBAR * 8 + 16 + 1024;  // + alignment slack
   static_assert(COUT % 16 == 0 && COUT >= 16 && COUT <= 64, "Cout");
   static_assert(CIN == 16 || CIN == 32 || CIN == 64, "Cin");
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t *sA = smem + C::OFF_A;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + C::OFF_BAR);
   uint64_t *full = bars, *empty = bars + C::STAGES, *acc_full = bars + 2 * C::STAGES,
-           *acc_empty = acc_full + 2, *wbar = acc_full + 4;
+           *acc_empty = acc_full + C::NACC, *wbar = acc_empty + C::NACC;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + C::NBAR);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < C::NACC; b++) {
       mbar_init(&acc_full[b], 1);
       mbar_init(&acc_empty[b], 4);
     }
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (!ok) break;
         umma_commit(&acc_full[b]);
-        if (++b == 2) {
+        if (++b == C::NACC) {
           b = 0;
           aph ^= 1u;
         }
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[b]);
-      if (++b == 2) {
+      if (++b == C::NACC) {
         b = 0;
         aph ^= 1u;
       }
@@ -396,8 +397,11 @@ cudaError_t launch(const __nv_bfloat16 *x, const __nv_bfloat16 *w, const ConvArg
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_tc_kernel<CIN, COUT>, kThreads, C::SMEM);
+  // resident CTAs per SM: shared memory (228 KB, 1 KB reserved per CTA) and
+  // tensor memory (512 columns) both bound it
+  int per_sm = 233472 / (C::SMEM + 1024);
+  if (per_sm > 512 / C::TMEM_COLS) per_sm = 512 / C::TMEM_COLS;
+  if (per_sm > 4) per_sm = 4;
   if (per_sm < 1) per_sm = 1;
   int sms = 148;
   int dev = 0;

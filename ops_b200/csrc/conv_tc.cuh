@@ -17,8 +17,9 @@
 // Warp roles (192 threads): warp 0 issues the TMA loads (and owns the tensor
 // memory allocation), warp 1 issues the MMAs from one thread, warps 2-5 drain
 // the accumulators (each warp reads its 32-lane quarter of tensor memory),
-// add the bias, apply ReLU or a gradient mask and store BF16. Two accumulator
-// buffers let the epilogue of one tile overlap the MMAs of the next. Every
+// add the bias, apply ReLU or a gradient mask and store BF16. Four accumulator
+// buffers let the epilogues of earlier tiles overlap the MMAs of later ones,
+// and several CTAs share an SM where shared and tensor memory allow. Every
 // mbarrier wait is bounded: on expiry the kernel records an error code,
 // stops issuing work, waits (bounded) for its own copies in flight, frees its
 // tensor memory and returns.

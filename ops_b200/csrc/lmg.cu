@@ -544,7 +544,8 @@ struct Net::Impl {
         {&g3b, P3 * 64}, {&ga3, P3 * 64}, {&dp3, P3 * 64}};
     size_t bytes = 0;
     for (auto &b : list) bytes += ((size_t)b.elems * 2 + 255) / 256 * 256;
-    zblk = (int)std::min<long long>(64, (h * (long long)w + kT - 1) / kT);
+    zblk = (int)std::max<long long>(1, std::min<long long>(std::min<long long>(1024, 148 * 8 / n),
+                                                            (h * (long long)w + kT - 1) / kT));
     const size_t pred_b = ((size_t)P0 * 4 + 255) / 256 * 256;
     int maxlen = 0;
     for (int l = 0; l < kLayers; l++) maxlen = std::max(maxlen, 9 * kDefs[l].cin * kDefs[l].cout + kDefs[l].cout);

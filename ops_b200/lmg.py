@@ -210,7 +210,7 @@ def generate_on_policy(net, nfields, n, seed0, snaps=(2, 4, 8, 16, 32, 64), rx_r
     return R, E, KX, KY
 
 
-def fit(net, n=128, nfields=300, steps=1500, rounds=3, lr=2e-3, batch=16, seed0=1000, log=None):
+def fit(net, n=64, nfields=300, steps=1500, rounds=3, lr=2e-3, batch=16, seed0=1000, log=None):
     """The training recipe: PCG pairs, then `rounds` rounds of on-policy pairs
     (half as many fields each, new seeds) added to the set, training after
     each. Returns the loss history of every round."""

@@ -86,17 +86,19 @@ def test_untrained_network_is_jacobi(gpu_runtime):
 
 @pytest.fixture(scope="module")
 def trained(gpu_runtime):
+    """The training recipe (PCG pairs, then three rounds of on-policy pairs from
+    the learned FCG's own iterates) on 64 x 64 seeded fields."""
     from ops_b200 import lmg
-    data = lmg.generate_pairs(120, 64, seed0=1000, snaps=(2, 8, 32))
     net = lmg.Net(seed=5)
-    hist = lmg.train(net, data, steps=400, batch=16, lr=2e-3)
-    yield net, hist
+    hists = lmg.fit(net, n=64, nfields=300, steps=1500, rounds=3)
+    yield net, hists
     net.close()
 
 
 def test_training_lowers_loss(trained):
-    _, hist = trained
-    assert np.mean(hist[-40:]) < 0.7 * np.mean(hist[:10])
+    _, hists = trained
+    first = hists[0]
+    assert np.mean(first[-40:]) < 0.7 * np.mean(first[:10])
 
 
 def test_learned_fcg_beats_jacobi_pcg(trained):
