@@ -13,6 +13,8 @@ configurations with synthetic seeded inputs:
   adi      batched tridiagonal x/y/z sweeps (ops_tridMultiDimBatch), one
            256^3 block or 64 uneven blocks, FP64 or FP32; a step is the three
            sweeps.
+  learned  the same heat solve with the learned multigrid preconditioner in
+           flexible CG (trained on the GPU first), next to plain Jacobi-PCG.
   tea      implicit heat conduction (TeaLeaf CG, Jacobi preconditioner) on
            4096x4096 with 16 seeded density rectangles; a step is one implicit
            timestep solved to residual 1e-10, FP64 PCG beside FP32-inner /
@@ -686,8 +688,140 @@ def reference_tea(args, world, rank):
     }
 
 
+# ---------------------------------------------------------------------------
+# Learned multigrid preconditioner in flexible CG vs plain Jacobi-PCG
+# ---------------------------------------------------------------------------
+def bench_learned(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    from ops_b200 import cnn, lmg
+    from ops_b200 import ops as O
+
+    peaks, peak_kind = load_peaks()
+    O.ops_init(local, 0)
+    N = args.grid or TEA_N
+    rx = 0.004 / (10.0 / N) ** 2          # the implicit timestep of the 4096^2 heat problem (dt = 0.004)
+    K, W = args.steps, args.warmup
+
+    # training on the GPU: PCG pairs + three on-policy rounds on 64^2 fields
+    t0 = time.perf_counter()
+    net = lmg.Net(seed=5)
+    hists = lmg.fit(net, n=64, nfields=300, steps=1500, rounds=3)
+    torch.cuda.synchronize(local)
+    train_s = time.perf_counter() - t0
+
+    rho, en = lmg.density_field(N, 4)
+    Kx, Ky, u0 = lmg.padded_problem(rho, en)
+    kx, ky, b = (torch.from_numpy(a).cuda(local) for a in (Kx, Ky, u0))
+    u = torch.empty_like(b)
+
+    def run(method, window=40):
+        u.copy_(b)
+        return lmg.solve(kx, ky, b, u, rx, rx, method=method, net=net.h, eps=1e-10, window=window, max_iters=20000)
+
+    for _ in range(W):
+        run(lmg.PCG_TRUE)
+        run(lmg.FCG_LEARNED)
+    barrier(pg, local)
+    with ClockSampler(local) as cs:
+        plain = [run(lmg.PCG_TRUE) for _ in range(K)]
+        learned = [run(lmg.FCG_LEARNED) for _ in range(K)]
+    clocks = cs.summary()
+    u_learned = u.clone()
+    run(lmg.PCG_TRUE)
+    err = float(torch.linalg.norm(u_learned - u) / torch.linalg.norm(u))
+    t_plain = max_over_ranks(pg, float(np.median([s["seconds"] for s in plain])), local)
+    t_learned = max_over_ranks(pg, float(np.median([s["seconds"] for s in learned])), local)
+
+    # the dominant kernel: the full-resolution 16 -> 16 channel tcgen05 convolution
+    x = torch.zeros((1, N, N, 16), dtype=torch.bfloat16, device=f"cuda:{local}")
+    y = torch.empty_like(x)
+    wt = torch.zeros((9, 16, 16), dtype=torch.bfloat16, device=f"cuda:{local}")
+    bias = torch.zeros(16, dtype=torch.float32, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream(local)
+    for _ in range(3):
+        cnn.conv3x3(x, wt, y, bias=bias, mode=cnn.CONV_BIAS_RELU, stream=stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(10):
+        cnn.conv3x3(x, wt, y, bias=bias, mode=cnn.CONV_BIAS_RELU, stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    conv_ms = e0.elapsed_time(e1) / 10
+    conv_bytes = 2.0 * N * N * 16 * 2          # read x, write y (BF16, 16 channels)
+    conv_gbs = conv_bytes / (conv_ms * 1e-3) / 1e9
+    conv_tflops = 2.0 * 9 * 16 * 16 * N * N / (conv_ms * 1e-3) / 1e12
+
+    # the gain on the training scale: held-out 64^2 fields, rx = 400
+    small = []
+    for seed in (90001, 90002, 90003):
+        r_, e_ = lmg.density_field(64, seed)
+        a, c, d = lmg.padded_problem(r_, e_)
+        skx, sky, sb = (torch.from_numpy(v).cuda(local) for v in (a, c, d))
+        row = {}
+        for name, m in (("pcg", lmg.PCG_TRUE), ("learned_fcg", lmg.FCG_LEARNED)):
+            su = sb.clone()
+            st = lmg.solve(skx, sky, sb, su, 400.0, 400.0, method=m, net=net.h, eps=1e-10, window=40)
+            row[name] = {"iterations": st["iterations"], "seconds": st["seconds"], "fallbacks": st["fallbacks"]}
+        small.append(row)
+
+    # e2e: host arrays in (pinned), one learned solve through the C-ABI, solution out
+    hk = [torch.from_numpy(a).pin_memory() for a in (Kx, Ky, u0)]
+    barrier(pg, local)
+    te = time.perf_counter()
+    dk = [t.cuda(local, non_blocking=True) for t in hk]
+    du = dk[2].clone()
+    st_e2e = lmg.solve(dk[0], dk[1], dk[2], du, rx, rx, method=lmg.FCG_LEARNED, net=net.h, eps=1e-10, window=40)
+    host_u = du.cpu()
+    e2e_s = max_over_ranks(pg, time.perf_counter() - te, local)
+    net.close()
+
+    line = {
+        "metric": "time to 1e-10 residual (learned FCG)", "value": t_learned, "unit": "s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": t_learned * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 solve / bf16 network",
+        "data": "synthetic (rho=1 background + 16 SplitMix64-seeded rectangles, rho log-uniform [0.1,100], seed 4);"
+                " network trained on 300 + 3 x 150 seeded 64^2 fields",
+        "config": {"workload": f"tealeaf2d_learned_fcg_{N}x{N}", "grid": [N, N], "rx": rx, "eps": 1e-10,
+                   "network": "4-level U-Net 16/32/64/64 ch, 3x3 tcgen05 BF16 convs, FP32 accumulation",
+                   "training": "A-norm loss, PCG pairs + 3 on-policy rounds, 64^2 fields, 1500 Adam steps each",
+                   "fallback": "Jacobi-PCG when ||r|| has not halved in 40 iterations",
+                   "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+        "plain_pcg": {"seconds": t_plain, "iterations": plain[0]["iterations"],
+                      "final_residual_ratio": plain[0]["final_residual"] / plain[0]["initial_residual"]},
+        "learned_fcg": {"seconds": t_learned, "iterations": learned[0]["iterations"],
+                        "fallbacks": learned[0]["fallbacks"],
+                        "final_residual_ratio": learned[0]["final_residual"] / learned[0]["initial_residual"],
+                        "rel_l2_vs_fp64_pcg_solution": err, "time_ratio_vs_plain": t_learned / t_plain},
+        "training": {"seconds": train_s, "final_loss_per_round": [float(np.mean(h[-50:])) for h in hists]},
+        "small_scale_gain_64x64_rx400": small,
+        "roofline": {"bound": "hbm", "achieved": conv_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": conv_gbs / peaks["hbm_gbs"], "traffic": None,
+                     "kernel": "conv3x3_tc_kernel<16,16> (full-resolution layer)", "avg_launch_ms": conv_ms,
+                     "alg_bytes_per_launch": conv_bytes, "tensor_tflops": conv_tflops,
+                     "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 3 * (N + 2) ** 2 * 8,
+                "d2h_bytes_per_step": (N + 2) ** 2 * 8, "solve_seconds": st_e2e["seconds"],
+                "note": "Kx, Ky, u0 from pinned host memory, one learned-FCG solve through ops_b200_heat_solve,"
+                        " solution back to the host"},
+        "gpu_launches": int(learned[0]["launches"]), "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        base = cpu_reference_tea(args.cpu_tea_iters, threads, N)
+        if base:
+            line["cpu_baseline"] = {
+                "value": base[0] * plain[0]["iterations"], "unit": "s", "cores": threads, "kind": "reference",
+                "sample": f"reference TeaLeaf OpenMP build, same {N}^2 deck, seconds per CG iteration from runs"
+                          f" capped at 2 and {2 + args.cpu_tea_iters} iterations, times the FP64 PCG count"}
+    del host_u
+    return line
+
+
 WORKLOADS = {"laplace": (bench_laplace, reference_laplace), "clover": (bench_clover, reference_clover),
-             "adi": (bench_adi, reference_adi), "tea": (bench_tea, reference_tea)}
+             "adi": (bench_adi, reference_adi), "tea": (bench_tea, reference_tea),
+             "learned": (bench_learned, reference_tea)}
 
 
 def main():
@@ -709,7 +843,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"laplace": 200, "clover": 200, "adi": 50, "tea": 3}.get(args.workload, 20)
+        args.steps = {"laplace": 200, "clover": 200, "adi": 50, "tea": 3, "learned": 2}.get(args.workload, 20)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_setup(args)
