@@ -76,6 +76,24 @@ int ops_b200_decl_strided_stencil(int dims, int points, const int *stencil, cons
 /* ops_decl_reduction_handle (ops/c/src/core/ops_lib_core.cpp:1119). */
 int ops_b200_decl_reduction_handle(int size, const char *type, const char *name);
 
+/* ops_decl_halo (ops/c/include/ops_lib_core.h:888, ops_lib_core.cpp:998):
+ * a box of iter_size (block dims entries) copied from dat `from` to dat
+ * `to`; dat dimension i walks box dimension |dir[i]| - 1, backwards when
+ * dir[i] < 0, from logical index *_base[i]. The dats may live on different
+ * blocks and differ in type only as float <-> double. Both boxes must lie in
+ * the dats' allocations (OPS_B200_ERR_ARG otherwise). Returns a halo handle. */
+int ops_b200_decl_halo(int from, int to, const int *iter_size, const int *from_base, const int *to_base,
+                       const int *from_dir, const int *to_dir);
+/* ops_decl_halo_group (ops_lib_core.h:902). Returns a group handle. */
+int ops_b200_decl_halo_group(int nhalos, const int *halos);
+/* ops_halo_transfer (ops_lib_core.h:911, ops_device_singlenode_common.cpp:262):
+ * flushes queued loops, then copies every halo of the group (one kernel for
+ * independent halos, else one per halo in declaration order). */
+int ops_b200_halo_transfer(int group);
+/* ops_timers (ops/c/src/core/ops_dummy_singlenode.cpp:901): process CPU
+ * seconds and monotonic wall-clock seconds. */
+int ops_b200_timers(double *cpu, double *et);
+
 /* ops_decl_const / ops_update_const (ops/c/include/ops_lib_core.h:947,971):
  * flushes queued loops, then updates every kernel constant of that name. */
 int ops_b200_decl_const(const char *name, int dim, const char *type, const void *data);

@@ -120,6 +120,10 @@ def _declare(L):
         "ops_b200_decl_stencil": ([i, i, P, cp], i),
         "ops_b200_decl_strided_stencil": ([i, i, P, P, cp], i),
         "ops_b200_decl_reduction_handle": ([i, cp, cp], i),
+        "ops_b200_decl_halo": ([i, i, P, P, P, P, P], i),
+        "ops_b200_decl_halo_group": ([i, P], i),
+        "ops_b200_halo_transfer": ([i], i),
+        "ops_b200_timers": ([P, P], i),
         "ops_b200_decl_const": ([cp, i, cp, P], i),
         "ops_b200_update_const": ([cp, i, cp, P], i),
         "ops_b200_par_loop": ([cp, cp, i, i, P, i, P], i),

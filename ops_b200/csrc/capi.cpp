@@ -1,4 +1,5 @@
 // extern "C" entry points of include/ops_b200.h over the C++ runtime.
+#include <time.h>
 #include "../../include/ops_b200.h"
 
 #include <cstring>
@@ -103,6 +104,33 @@ int ops_b200_decl_strided_stencil(int dims, int points, const int *stencil, cons
 
 int ops_b200_decl_reduction_handle(int size, const char *type, const char *name) {
   return guarded([&] { return rt().decl_reduction(size, type, name); });
+}
+
+int ops_b200_decl_halo(int from, int to, const int *iter_size, const int *from_base, const int *to_base,
+                       const int *from_dir, const int *to_dir) {
+  return guarded([&] { return rt().decl_halo(from, to, iter_size, from_base, to_base, from_dir, to_dir); });
+}
+
+int ops_b200_decl_halo_group(int nhalos, const int *halos) {
+  return guarded([&] { return rt().decl_halo_group(nhalos, halos); });
+}
+
+int ops_b200_halo_transfer(int group) {
+  return guarded([&] {
+    rt().halo_transfer(group);
+    return 0;
+  });
+}
+
+int ops_b200_timers(double *cpu, double *et) {
+  return guarded([&] {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    if (et) *et = (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+    clock_gettime(CLOCK_PROCESS_CPUTIME_ID, &ts);
+    if (cpu) *cpu = (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+    return 0;
+  });
 }
 
 int ops_b200_decl_const(const char *name, int dim, const char *type, const void *data) {

@@ -137,6 +137,12 @@ class Runtime {
                const void *data, int type_size, const char *type, const char *name);
   int decl_stencil(int dims, int points, const int *offs, const int *stride, const char *name);
   int decl_reduction(int size, const char *type, const char *name);
+  // ops_decl_halo / ops_decl_halo_group / ops_halo_transfer
+  // (ops/c/src/core/ops_lib_core.cpp:998-1040, ops_device_singlenode_common.cpp:262-346)
+  int decl_halo(int from, int to, const int *iter, const int *from_base, const int *to_base, const int *from_dir,
+                const int *to_dir);
+  int decl_halo_group(int n, const int *halos);
+  void halo_transfer(int group);
   void decl_const(const char *name, int dim, const char *type, const void *data);
 
   void par_loop(const LoopInfo *loop, const char *name, int block, int dim, const int *range,
@@ -217,6 +223,14 @@ class Runtime {
   cudaStream_t stream_ = nullptr;
   std::vector<Block> blocks_;
   std::vector<std::unique_ptr<Dat>> dats_;
+  struct Halo {
+    int from = -1, to = -1;
+    int iter[3], fbase[3], tbase[3], fdir[3], tdir[3];
+  };
+  std::vector<Halo> halos_;
+  std::vector<std::vector<int>> halo_groups_;
+  void *halo_desc_d_ = nullptr;
+  size_t halo_desc_cap_ = 0;
   std::vector<Stencil> stencils_;
   std::vector<Reduction> reductions_;
   std::vector<Desc> queue_;

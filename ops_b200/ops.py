@@ -108,6 +108,37 @@ def ops_decl_reduction_handle(size, type_, name):
                          type_, name)
 
 
+def _ivec(v):
+    a = np.ascontiguousarray(v, dtype=np.int32)
+    return a, a.ctypes.data
+
+
+def ops_decl_halo(from_dat, to_dat, iter_size, from_base, to_base, from_dir, to_dir):
+    """ops_decl_halo (ops/c/include/ops_lib_core.h:888); returns a halo handle."""
+    arrs = [_ivec(v) for v in (iter_size, from_base, to_base, from_dir, to_dir)]
+    f = from_dat.index if hasattr(from_dat, "index") else int(from_dat)
+    t = to_dat.index if hasattr(to_dat, "index") else int(to_dat)
+    return check(lib().ops_b200_decl_halo(f, t, *[p for _, p in arrs]))
+
+
+def ops_decl_halo_group(halos):
+    """ops_decl_halo_group (ops_lib_core.h:902); returns a group handle."""
+    a, p = _ivec(list(halos))
+    return check(lib().ops_b200_decl_halo_group(len(a), p))
+
+
+def ops_halo_transfer(group):
+    """ops_halo_transfer (ops_lib_core.h:911)."""
+    check(lib().ops_b200_halo_transfer(group))
+
+
+def ops_timers():
+    """ops_timers: (cpu seconds, wall-clock seconds)."""
+    c, e = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    check(lib().ops_b200_timers(ctypes.byref(c), ctypes.byref(e)))
+    return c.value, e.value
+
+
 def ops_decl_const(name, dim, type_, data):
     arr = np.ascontiguousarray(np.atleast_1d(data), dtype=_TYPES[type_][0]) if type_ in _TYPES else data
     check(lib().ops_b200_decl_const(name.encode(), dim, type_.encode(),

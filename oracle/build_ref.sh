@@ -77,6 +77,13 @@ build_app cloverleaf "$CL" \
   "clover_leaf.cpp initialise_chunk.cpp generate.cpp ideal_gas.cpp update_halo.cpp field_summary.cpp viscosity.cpp calc_dt.cpp PdV.cpp revert.cpp accelerate.cpp flux_calc.cpp advec_cell.cpp advec_mom.cpp reset_field.cpp" \
   "start.cpp time_step.cpp build_field.cpp read_input.cpp initialise.cpp advection.cpp" "" &
 
+# halo transfer cases: a driver of our own on the reference's public API,
+# compiled against libops_seq.a with the reference's template loop path
+# (ops_seq_v2.h, no translation)
+(mkdir -p "$OUT/halo_cases" && cd "$OUT/halo_cases" && \
+  $CXX $CXXFLAGS $INC "$HERE/ref_drivers/halo_cases.cpp" -L"$OUT/lib" -lops_seq -o "$OUT/bin/halo_cases" && \
+  echo "built $OUT/bin/halo_cases") &
+
 TL=$REF/apps/c/TeaLeaf
 build_app tealeaf "$TL" \
   "tea_leaf.cpp field_summary.cpp generate.cpp initialise_chunk.cpp start.cpp set_field.cpp tea_leaf_cg.cpp tea_leaf_cheby.cpp tea_leaf_common.cpp tea_leaf_jacobi.cpp tea_leaf_ppcg.cpp update_halo.cpp" \

@@ -186,3 +186,27 @@ def tea():
 
 if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "tea":
     tea()
+
+
+# ---------------------------------------------------------------------------
+# halo transfer cases from the reference library (oracle/ref_drivers/halo_cases.cpp)
+# ---------------------------------------------------------------------------
+def halo():
+    exe = oracle.reference_binary("halo_cases")
+    if exe is None:
+        raise SystemExit("oracle/_ref/bin/halo_cases missing: run oracle/build_ref.sh")
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        subprocess.run([exe, td], check=True, capture_output=True, timeout=300)
+        for c in range(6):
+            for name, dt in (("a", np.float64), ("b", np.float64), ("bf", np.float32)):
+                raw = open(os.path.join(td, f"case{c}_{name}.bin"), "rb").read()
+                nx, ny = np.frombuffer(raw[:8], dtype=np.int32)
+                out[f"case{c}_{name}"] = np.frombuffer(raw[8:], dtype=dt).reshape(ny, nx).copy()
+    path = os.path.join(HERE, "halo_cases.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, len(out))
+
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "halo":
+    halo()
