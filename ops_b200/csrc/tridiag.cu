@@ -8,17 +8,22 @@
 //
 // B200 design: one persistent launch walks a work list of line groups over
 // any number of systems (blocks of different shapes solve in one launch).
-// Every line is split into chunks, one chunk per thread; a thread runs the
-// modified Thomas elimination on its chunk in registers, expressing each row
-// through the chunk's first and last unknowns (the partition method of
+// Every line is split into chunks of about 8 rows, one chunk per thread; a
+// thread runs the modified Thomas elimination on its chunk, expressing each
+// row through the chunk's first and last unknowns (the partition method of
 // Wang 1981, as used for GPUs by Laszlo, Giles and Appleyard, ACM TOMS 42(4)
-// 2016). The chunks' end rows form a small tridiagonal system in shared
-// memory, solved by Thomas; a last pass substitutes back. Coefficients and
-// right-hand sides are read once and the solution written once: 40 bytes per
-// FP64 unknown (48 for _Inc), nothing else touches HBM.
-//   * lines along y or z (strided): a warp holds 32 neighbouring lines
-//     (coalesced along x), the 8 warps of a CTA hold the 8 chunks;
-//   * lines along x (contiguous): a warp holds one line, lane = chunk.
+// 2016):
+//   forward, rows 0 and 1 normalised, then for i >= 2
+//     r = 1 / (b_i - a_i c'_{i-1}),  d'_i = r (d_i - a_i d'_{i-1}),
+//     a'_i = -r a_i a'_{i-1},        c'_i = r c_i;
+//   backward for i = m-3 .. 1
+//     d'_i -= c'_i d'_{i+1},  a'_i -= c'_i a'_{i+1},  c'_i = -c'_i c'_{i+1};
+//   row 0 folds in row 1.
+// The chunks' end rows form a small tridiagonal system in shared memory,
+// solved by parallel cyclic reduction; a last pass substitutes back. The lines of a work item
+// are staged through shared memory, so coefficients and right-hand sides are
+// read from HBM once and the solution written once: 40 bytes per FP64
+// unknown (48 for _Inc).
 #include <algorithm>
 #include <cstdio>
 #include <vector>
@@ -68,193 +73,243 @@ __device__ __forceinline__ double recip(double x) {
   return r * __longlong_as_double((2046LL - ex) << 52);
 }
 
-// Modified Thomas on rows [r0, r0+m) of one line (m >= 2): afterwards row i
-// reads  aa_i x_first + x_i + cc_i x_last = dd_i  for 0 < i < m-1, and the
-// end rows keep their outside couplings:
-//   aa_0 x_prev_last + x_first + cc_0 x_last   = dd_0
-//   aa_{m-1} x_first + x_last + cc_{m-1} x_next_first = dd_{m-1}
-// The last row's coefficients are returned in la, lc, ld as they are
-// produced (row m-1 is final after the forward sweep); reading them back
-// from the arrays with a run-time index would move the arrays to local memory.
-template <class T, int M>
-__device__ __forceinline__ void chunk_eliminate(const T *a, const T *b, const T *c, const T *d, long long ss, int m,
-                                                T (&aa)[M], T (&cc)[M], T (&dd)[M], T &la, T &lc, T &ld) {
-  // All of the chunk's loads are issued before any arithmetic, so each
-  // thread keeps 4*m independent requests in flight.
-  T bb[M];
-#pragma unroll
-  for (int i = 0; i < M; i++) {
-    if (i < m) {
-      aa[i] = __ldg(a + i * ss);
-      bb[i] = __ldg(b + i * ss);
-      cc[i] = __ldg(c + i * ss);
-      dd[i] = __ldg(d + i * ss);
-    }
-  }
-  // Forward sweep in place: (a_i, c_i, d_i) become (aa_i, cc_i, dd_i).
-#pragma unroll
-  for (int i = 0; i < M; i++) {
-    if (i < m) {
-      if (i < 2) {
-        const T r = recip(bb[i]);
-        aa[i] = aa[i] * r;
-        cc[i] = cc[i] * r;
-        dd[i] = dd[i] * r;
-      } else {
-        const T ai = aa[i];
-        const T r = recip(bb[i] - ai * cc[i - 1]);
-        dd[i] = r * (dd[i] - ai * dd[i - 1]);
-        aa[i] = -r * ai * aa[i - 1];
-        cc[i] = r * cc[i];
-      }
-      if (i == m - 1) {
-        la = aa[i];
-        lc = cc[i];
-        ld = dd[i];
-      }
-    }
-  }
-#pragma unroll
-  for (int i = M - 3; i >= 1; i--) {
-    if (i <= m - 3) {
-      dd[i] = dd[i] - cc[i] * dd[i + 1];
-      aa[i] = aa[i] - cc[i] * aa[i + 1];
-      cc[i] = -cc[i] * cc[i + 1];
-    }
-  }
-  if (m > 2) {
-    const T r = recip(T(1) - cc[0] * aa[1]);
-    dd[0] = r * (dd[0] - cc[0] * dd[1]);
-    aa[0] = r * aa[0];
-    cc[0] = -r * cc[0] * cc[1];
-  }
-}
+// One work item = L neighbouring lines x n rows of one system, staged in
+// shared memory: the four coefficient tiles are loaded with cp.async (rows
+// of the tile along whichever dimension is contiguous in HBM, so the loads
+// coalesce), each thread eliminates its chunk of about 8 rows in place in
+// shared memory, the chunks' end rows form the reduced system (solved per
+// line by Thomas), and the substituted solution is stored with the same
+// coalesced mapping. Registers stay few, so two CTAs share an SM and one
+// CTA's loads overlap the other's elimination. Tile rows are padded to
+// L + 1 elements to spread the chunks over the shared-memory banks.
+constexpr int kTileThreads = 256;
 
-// Thomas on the reduced system held in shared memory: row k has
-// A[k] x_{k-1} + x_k + C[k] x_{k+1} = D[k]; the solution overwrites D.
+constexpr size_t kTileSmem = 110 * 1024;  // per CTA, so that two CTAs share an SM
+
 template <class T>
-__device__ __forceinline__ void reduced_solve(T *A, T *C, T *D, int n, int stride) {
-  // forward
-  T cp = C[0];
-  T dp = D[0];
-  C[0] = cp;
-  for (int k = 1; k < n; k++) {
-    const T ak = A[k * stride];
-    const T r = recip(T(1) - ak * cp);
-    cp = C[k * stride] * r;
-    dp = (D[k * stride] - ak * dp) * r;
-    C[k * stride] = cp;
-    D[k * stride] = dp;
-  }
-  for (int k = n - 2; k >= 0; k--) D[k * stride] = D[k * stride] - C[k * stride] * D[(k + 1) * stride];
+size_t tile_smem(int L, int n) {
+  return (size_t)(4 * (L + 1) * n + 8 * (kTileThreads / L) * L) * sizeof(T);
 }
 
-template <class T, int M>
-__device__ __forceinline__ void chunk_store(T *d, T *u, long long ss, int m, const T (&aa)[M], const T (&cc)[M],
-                                            const T (&dd)[M], T xf, T xl) {
-#pragma unroll
-  for (int i = 0; i < M; i++) {
-    if (i < m) {
-      T x = (i == 0) ? xf : (i == m - 1) ? xl : dd[i] - aa[i] * xf - cc[i] * xl;
-      if (u) u[i * ss] += x;
-      else d[i * ss] = x;
-    }
-  }
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+template <class T>
+__device__ __forceinline__ void cp_async(T *dst, const T *src) {
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
-constexpr int kLinesContig = 8;      // warps per CTA = lines per CTA (lane = chunk)
-
-// Lines along y or z: threadIdx.x = line (neighbouring x), threadIdx.y =
-// chunk. L lines x K chunks = 256 threads: FP64 uses 16 x 16 so that a chunk
-// of a 256-point line (16 rows, three coefficient arrays) stays in registers.
-template <class T, int M, int L, int K>
-__global__ void __launch_bounds__(256) trid_strided_kernel(const Sys *__restrict__ sys, const Work *__restrict__ work,
-                                                           int nwork) {
-  __shared__ T A[2 * K][L], C[2 * K][L], Dv[2 * K][L];
-  const int lane = threadIdx.x, chunk = threadIdx.y;
+template <class T>
+__global__ void __launch_bounds__(kTileThreads, 2) trid_tile_kernel(const Sys *__restrict__ sys,
+                                                                    const Work *__restrict__ work, int nwork, int L,
+                                                                    int nmax) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int P = L + 1;  // padded tile row
+  const int tile = P * nmax;
+  T *ta = reinterpret_cast<T *>(smraw);
+  T *tb = ta + tile, *tc = tb + tile, *td = tc + tile;
+  const int K = kTileThreads / L;
+  T *RA = td + tile, *RB = RA + 2 * K * L, *RC = RB + 2 * K * L, *RD = RC + 2 * K * L;
+  const int tid = threadIdx.x;
+  const int l = tid % L, chunk = tid / L;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const Work wk = work[w];
     const Sys s = sys[wk.sys];
-    const int line = wk.l0 + lane;
-    const bool active = line < s.nl0;
     const int n = s.n;
+    const int nl = min(L, s.nl0 - wk.l0);
+    const long long base = (long long)wk.l0 * s.s0 + (long long)wk.l1 * s.s1;
+    const T *ga = reinterpret_cast<const T *>(s.a) + base;
+    const T *gb = reinterpret_cast<const T *>(s.b) + base;
+    const T *gc = reinterpret_cast<const T *>(s.c) + base;
+    T *gd = reinterpret_cast<T *>(s.d) + base;
+    T *gu = s.u ? reinterpret_cast<T *>(s.u) + base : nullptr;
+    const bool rows_contig = s.ss == 1;
+    const int warp = tid >> 5, lane = tid & 31;
+    // 1. stage the four tiles: along x one warp per line (lanes walk the
+    // contiguous rows), otherwise thread t takes line t mod L and every
+    // (256 / L)-th row from t / L, so each warp-wide copy covers L
+    // neighbouring lines of 256 / L rows; no division per element
+    if (rows_contig) {
+      for (int ll = warp; ll < nl; ll += kTileThreads / 32) {
+        const long long g0 = (long long)ll * s.s0;
+        for (int i = lane; i < n; i += 32) {
+          const int si = i * P + ll;
+          cp_async(ta + si, ga + g0 + i);
+          cp_async(tb + si, gb + g0 + i);
+          cp_async(tc + si, gc + g0 + i);
+          cp_async(td + si, gd + g0 + i);
+        }
+      }
+    } else if (l < nl) {
+      const long long g0 = (long long)l * s.s0;
+      for (int i = chunk; i < n; i += K) {
+        const long long g = g0 + (long long)i * s.ss;
+        const int si = i * P + l;
+        cp_async(ta + si, ga + g);
+        cp_async(tb + si, gb + g);
+        cp_async(tc + si, gc + g);
+        cp_async(td + si, gd + g);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    // 2. eliminate this thread's chunk in place (same recurrences as chunk_eliminate)
     const int kact = n >= 2 * K ? K : (n / 2 > 0 ? n / 2 : 1);
     const int r0 = chunk * n / kact, r1 = (chunk + 1) * n / kact, m = r1 - r0;
-    const long long off = (long long)line * s.s0 + (long long)wk.l1 * s.s1 + (long long)r0 * s.ss;
-    const T *a = reinterpret_cast<const T *>(s.a) + off;
-    const T *b = reinterpret_cast<const T *>(s.b) + off;
-    const T *c = reinterpret_cast<const T *>(s.c) + off;
-    T *d = reinterpret_cast<T *>(s.d) + off;
-    T *u = s.u ? reinterpret_cast<T *>(s.u) + off : nullptr;
-    T aa[M], cc[M], dd[M];
-    const bool mine = active && chunk < kact;
-    if (mine && n == 1) {
-      const T x = __ldg(d) * recip(__ldg(b));
-      if (u) *u += x;
-      else *d = x;
-    }
-    const bool work_here = mine && n > 1;
-    if (work_here) {
-      T la = T(0), lc = T(0), ld = T(0);
-      chunk_eliminate<T, M>(a, b, c, d, s.ss, m, aa, cc, dd, la, lc, ld);
-      A[2 * chunk][lane] = chunk == 0 ? T(0) : aa[0];
-      C[2 * chunk][lane] = cc[0];
-      Dv[2 * chunk][lane] = dd[0];
-      A[2 * chunk + 1][lane] = la;
-      C[2 * chunk + 1][lane] = chunk == kact - 1 ? T(0) : lc;
-      Dv[2 * chunk + 1][lane] = ld;
+    const bool mine = l < nl && chunk < kact && n > 1;
+    if (n == 1 && chunk == 0 && l < nl) td[l] = td[l] * recip(tb[l]);
+    if (mine) {
+      T pa = T(0), pc = T(0), pd = T(0);
+      for (int i = 0; i < m; i++) {
+        const int q = (r0 + i) * P + l;
+        const T ai = ta[q], bi = tb[q], ci = tc[q], di = td[q];
+        T na, nc, nd;
+        if (i < 2) {
+          const T r = recip(bi);
+          na = ai * r;
+          nc = ci * r;
+          nd = di * r;
+        } else {
+          const T r = recip(bi - ai * pc);
+          nd = r * (di - ai * pd);
+          na = -r * ai * pa;
+          nc = r * ci;
+        }
+        ta[q] = na;
+        tc[q] = nc;
+        td[q] = nd;
+        pa = na;
+        pc = nc;
+        pd = nd;
+      }
+      const T la = pa, lc = pc, ld = pd;
+      if (m > 3) {
+        const int q1 = (r0 + m - 2) * P + l;
+        T na = ta[q1], nc = tc[q1], nd = td[q1];
+        for (int i = m - 3; i >= 1; i--) {
+          const int q = (r0 + i) * P + l;
+          const T ci = tc[q];
+          nd = td[q] - ci * nd;
+          na = ta[q] - ci * na;
+          nc = -ci * nc;
+          ta[q] = na;
+          tc[q] = nc;
+          td[q] = nd;
+        }
+      }
+      const int q0 = r0 * P + l, q1 = (r0 + 1) * P + l;
+      T a0 = ta[q0], c0 = tc[q0], d0 = td[q0];
+      if (m > 2) {
+        const T r = recip(T(1) - c0 * ta[q1]);
+        d0 = r * (d0 - c0 * td[q1]);
+        a0 = r * a0;
+        c0 = -r * c0 * tc[q1];
+        ta[q0] = a0;
+        tc[q0] = c0;
+        td[q0] = d0;
+      }
+      RA[(2 * chunk) * L + l] = chunk == 0 ? T(0) : a0;
+      RB[(2 * chunk) * L + l] = T(1);
+      RC[(2 * chunk) * L + l] = c0;
+      RD[(2 * chunk) * L + l] = d0;
+      RA[(2 * chunk + 1) * L + l] = la;
+      RB[(2 * chunk + 1) * L + l] = T(1);
+      RC[(2 * chunk + 1) * L + l] = chunk == kact - 1 ? T(0) : lc;
+      RD[(2 * chunk + 1) * L + l] = ld;
     }
     __syncthreads();
-    if (chunk == 0 && active && n > 1) reduced_solve<T>(&A[0][lane], &C[0][lane], &Dv[0][lane], 2 * kact, L);
-    __syncthreads();
-    if (work_here) chunk_store<T, M>(d, u, s.ss, m, aa, cc, dd, Dv[2 * chunk][lane], Dv[2 * chunk + 1][lane]);
-    __syncthreads();
-  }
-}
-
-// Lines along x: threadIdx.y = line, threadIdx.x = chunk.
-template <class T, int M>
-__global__ void __launch_bounds__(256) trid_contig_kernel(const Sys *__restrict__ sys, const Work *__restrict__ work,
-                                                          int nwork) {
-  __shared__ T A[kLinesContig][64], C[kLinesContig][64], Dv[kLinesContig][64];
-  const int chunk = threadIdx.x, wl = threadIdx.y;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const Work wk = work[w];
-    const Sys s = sys[wk.sys];
-    const int line = wk.l0 + wl;
-    const bool active = line < s.nl0;
-    const int n = s.n;
-    const int kact = n >= 64 ? 32 : (n / 2 > 0 ? n / 2 : 1);
-    const int r0 = chunk * n / kact, r1 = (chunk + 1) * n / kact, m = r1 - r0;
-    const long long off = (long long)line * s.s0 + (long long)wk.l1 * s.s1 + (long long)r0 * s.ss;
-    const T *a = reinterpret_cast<const T *>(s.a) + off;
-    const T *b = reinterpret_cast<const T *>(s.b) + off;
-    const T *c = reinterpret_cast<const T *>(s.c) + off;
-    T *d = reinterpret_cast<T *>(s.d) + off;
-    T *u = s.u ? reinterpret_cast<T *>(s.u) + off : nullptr;
-    T aa[M], cc[M], dd[M];
-    const bool mine = active && chunk < kact;
-    if (mine && n == 1) {
-      const T x = __ldg(d) * recip(__ldg(b));
-      if (u) *u += x;
-      else *d = x;
+    // 3. the reduced system (2 kact rows per line) by parallel cyclic
+    // reduction (Hockney 1965): at stride h every row eliminates its
+    // neighbours h above and below, log2(2 kact) steps with every chunk
+    // thread taking its two rows; afterwards x_k = d_k / b_k.
+    if (n > 1) {
+      const int N = 2 * kact;
+      const bool act = l < nl && chunk < kact;
+      for (int h = 1; h < N; h *= 2) {
+        T na[2], nb[2], nc[2], nd[2];
+        if (act) {
+#pragma unroll
+          for (int j = 0; j < 2; j++) {
+            const int k = 2 * chunk + j;
+            const int q = k * L + l;
+            T ak = RA[q], bk = RB[q], ck = RC[q], dk = RD[q];
+            if (k - h >= 0) {
+              const int qm = (k - h) * L + l;
+              const T al = -ak * recip(RB[qm]);
+              ak = al * RA[qm];
+              bk = bk + al * RC[qm];
+              dk = dk + al * RD[qm];
+            } else {
+              ak = T(0);
+            }
+            if (k + h < N) {
+              const int qp = (k + h) * L + l;
+              const T ga = -ck * recip(RB[qp]);
+              ck = ga * RC[qp];
+              bk = bk + ga * RA[qp];
+              dk = dk + ga * RD[qp];
+            } else {
+              ck = T(0);
+            }
+            na[j] = ak;
+            nb[j] = bk;
+            nc[j] = ck;
+            nd[j] = dk;
+          }
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+          for (int j = 0; j < 2; j++) {
+            const int q = (2 * chunk + j) * L + l;
+            RA[q] = na[j];
+            RB[q] = nb[j];
+            RC[q] = nc[j];
+            RD[q] = nd[j];
+          }
+        }
+        __syncthreads();
+      }
+      if (act) {
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          const int q = (2 * chunk + j) * L + l;
+          RD[q] = RD[q] * recip(RB[q]);
+        }
+      }
     }
-    const bool work_here = mine && n > 1;
-    if (work_here) {
-      T la = T(0), lc = T(0), ld = T(0);
-      chunk_eliminate<T, M>(a, b, c, d, s.ss, m, aa, cc, dd, la, lc, ld);
-      A[wl][2 * chunk] = chunk == 0 ? T(0) : aa[0];
-      C[wl][2 * chunk] = cc[0];
-      Dv[wl][2 * chunk] = dd[0];
-      A[wl][2 * chunk + 1] = la;
-      C[wl][2 * chunk + 1] = chunk == kact - 1 ? T(0) : lc;
-      Dv[wl][2 * chunk + 1] = ld;
+    __syncthreads();
+    // 4. substitute back into the d tile
+    if (mine) {
+      const T xf = RD[(2 * chunk) * L + l], xl = RD[(2 * chunk + 1) * L + l];
+      for (int i = 0; i < m; i++) {
+        const int q = (r0 + i) * P + l;
+        td[q] = (i == 0) ? xf : (i == m - 1) ? xl : td[q] - ta[q] * xf - tc[q] * xl;
+      }
     }
-    __syncwarp();
-    if (chunk == 0 && active && n > 1) reduced_solve<T>(&A[wl][0], &C[wl][0], &Dv[wl][0], 2 * kact, 1);
-    __syncwarp();
-    if (work_here) chunk_store<T, M>(d, u, s.ss, m, aa, cc, dd, Dv[wl][2 * chunk], Dv[wl][2 * chunk + 1]);
-    __syncwarp();
+    __syncthreads();
+    // 5. store (d = x, or u += x), with the loads' mapping
+    if (rows_contig) {
+      for (int ll = warp; ll < nl; ll += kTileThreads / 32) {
+        const long long g0 = (long long)ll * s.s0;
+        for (int i = lane; i < n; i += 32) {
+          const T x = td[i * P + ll];
+          if (gu) gu[g0 + i] += x;
+          else gd[g0 + i] = x;
+        }
+      }
+    } else if (l < nl) {
+      const long long g0 = (long long)l * s.s0;
+      for (int i = chunk; i < n; i += K) {
+        const long long g = g0 + (long long)i * s.ss;
+        const T x = td[i * P + l];
+        if (gu) gu[g] += x;
+        else gd[g] = x;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -271,17 +326,20 @@ Buffers &buffers() {
 
 template <class T>
 void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, long long *kernels) {
+  (void)solvedim;
   int maxn = 0;
   for (const Sys &s : systems) maxn = std::max(maxn, s.n);
   if (maxn == 0) return;
-  const bool contig = solvedim == 0;
+  // lines per work item: the largest power of two (<= 64) whose tiles fit
+  int L = 64;
+  while (L > 1 && tile_smem<T>(L, maxn) > kTileSmem) L /= 2;
+  if (tile_smem<T>(L, maxn) > kTileSmem) throw Error(E_UNSUPPORTED, "tridiagonal lines longer than the tile budget");
   std::vector<Work> work;
   for (int i = 0; i < (int)systems.size(); i++) {
     const Sys &s = systems[i];
     if (s.n == 0) continue;
-    const int g = contig ? kLinesContig : 16;
     for (int l1 = 0; l1 < s.nl1; l1++)
-      for (int l0 = 0; l0 < s.nl0; l0 += g) work.push_back({i, l0, l1});
+      for (int l0 = 0; l0 < s.nl0; l0 += L) work.push_back({i, l0, l1});
   }
   if (work.empty()) return;
   Buffers &B = buffers();
@@ -298,27 +356,15 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
   OPSB_CUDA(cudaMemcpyAsync(B.sys, systems.data(), systems.size() * sizeof(Sys), cudaMemcpyHostToDevice, stream));
   OPSB_CUDA(cudaMemcpyAsync(B.work, work.data(), work.size() * sizeof(Work), cudaMemcpyHostToDevice, stream));
   const int nwork = (int)work.size();
-  const int grid = std::min(nwork, 148 * 4);
-  if (contig) {
-    // 32 chunks per line for n >= 64 (ceil(n/32) rows each), else n/2 chunks of at most 3 rows.
-    const int need = std::max(3, (maxn + 31) / 32);
-    dim3 blk(32, kLinesContig);
-    // (no 4-row variant: with arrays that small the compiler turns the
-    // unrolled selects back into indexed accesses and spills them to local memory)
-    if (need <= 8) trid_contig_kernel<T, 8><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
-    else if (need <= 16) trid_contig_kernel<T, 16><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
-    else throw Error(E_UNSUPPORTED, "tridiagonal lines along x longer than 512 are not supported");
-  } else {
-    // 16 lines x 16 chunks: a chunk of a 256-point line holds 16 rows, whose
-    // four coefficient arrays stay in registers. A chunk holds ceil(n/K) rows
-    // for n >= 2K, else at most 3.
-    constexpr int L = 16, K = 16;
-    const int need = std::max(3, (maxn + K - 1) / K);
-    dim3 blk(L, K);
-    if (need <= 8) trid_strided_kernel<T, 8, L, K><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
-    else if (need <= 16) trid_strided_kernel<T, 16, L, K><<<grid, blk, 0, stream>>>(B.sys, B.work, nwork);
-    else throw Error(E_UNSUPPORTED, "tridiagonal lines along y/z longer than 256 are not supported");
+  const size_t smem = tile_smem<T>(L, maxn);
+  static size_t attr_set = 0;
+  if (smem > attr_set) {
+    OPSB_CUDA(cudaFuncSetAttribute(trid_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = smem;
   }
+  const int per_sm = std::max(1, std::min(2, (int)(233472 / (smem + 1024))));
+  const int grid = std::min(nwork, 148 * per_sm);
+  trid_tile_kernel<T><<<grid, kTileThreads, smem, stream>>>(B.sys, B.work, nwork, L, maxn);
   OPSB_CUDA(cudaGetLastError());
   if (kernels) (*kernels)++;
 }
