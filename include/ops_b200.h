@@ -148,6 +148,10 @@ int ops_b200_set_option(const char *name, int value);
 /* Counters since the last reset: kernels launched by this library, CUDA
  * graphs launched, loops queued. */
 int ops_b200_counters(long long *kernels, long long *graphs, long long *loops);
+/* Loops dropped since ops_b200_init because an identical loop with unchanged
+ * inputs and outputs was already queued in the same flush (no reference
+ * counterpart; disabled with the "fusion" option). */
+int ops_b200_loops_skipped(long long *skipped);
 int ops_b200_reset_counters(void);
 
 /* Per-kernel device timing: while enabled, every launch is bracketed by CUDA

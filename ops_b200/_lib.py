@@ -124,6 +124,7 @@ def _declare(L):
         "ops_b200_decl_halo_group": ([i, P], i),
         "ops_b200_halo_transfer": ([i], i),
         "ops_b200_timers": ([P, P], i),
+        "ops_b200_loops_skipped": ([P], i),
         "ops_b200_decl_const": ([cp, i, cp, P], i),
         "ops_b200_update_const": ([cp, i, cp, P], i),
         "ops_b200_par_loop": ([cp, cp, i, i, P, i, P], i),

@@ -122,6 +122,13 @@ int ops_b200_halo_transfer(int group) {
   });
 }
 
+int ops_b200_loops_skipped(long long *skipped) {
+  return guarded([&] {
+    if (skipped) *skipped = rt().loops_skipped();
+    return 0;
+  });
+}
+
 int ops_b200_timers(double *cpu, double *et) {
   return guarded([&] {
     struct timespec ts;

@@ -287,10 +287,18 @@ struct Exec<K, void (C::*)(P...) const> {
   }
 };
 
+// Resident 256-thread CTAs per SM the register allocation must allow: 4
+// (at most 64 registers a thread) unless a kernel states `min_blocks`. These
+// loops are latency-bound streams, so occupancy is worth a few spills.
+template <class K, class = void> struct LoopMinBlocks { static constexpr int value = 4; };
+template <class K> struct LoopMinBlocks<K, std::void_t<decltype(K::min_blocks)>> {
+  static constexpr int value = K::min_blocks;
+};
+
 // The generic loop kernel. blockDim = (BX, BY); blocks tile x exactly and
 // stride over the remaining (y, z) rows.
 template <class K>
-__global__ void __launch_bounds__(256) exec_loop(const __grid_constant__ LoopParams lp) {
+__global__ void __launch_bounds__(256, LoopMinBlocks<K>::value) exec_loop(const __grid_constant__ LoopParams lp) {
   using E = Exec<K, decltype(&K::operator())>;
   typename E::Tup t;
   E::init_all(t, lp, typename E::Seq{});

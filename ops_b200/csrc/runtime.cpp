@@ -318,9 +318,63 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         throw Error(E_ARG, "unknown arg kind");
     }
   }
+  LoopRecord rec;
+  if (redundant(d, rec)) {
+    loops_skipped_++;
+    return;
+  }
   queue_.push_back(std::move(d));
+  qrec_.push_back(std::move(rec));
   loops_enqueued_++;
   if (queue_.size() >= 4096) execute();
+}
+
+// A loop that only reads some dats and writes others is redundant when an
+// identical loop (kernel, block, range, args, global values) is already
+// queued in this flush and none of its inputs or outputs has been written
+// since: running it again would store the same values. (The reference's
+// CloverLeaf momentum advection, for one, recomputes its volume and mass
+// fluxes for the second velocity component.) Fills `rec` for the new loop.
+bool Runtime::redundant(const Desc &d, LoopRecord &rec) {
+  const size_t na = d.args.size();
+  rec.ver.assign(na, 0);
+  rec.pure = fusion_on_ && !d.loop->internal;
+  for (size_t i = 0; i < na; i++) {
+    const Arg &a = d.args[i];
+    if (a.kind == ARG_DAT) {
+      if (a.acc != ACC_READ && a.acc != ACC_WRITE) rec.pure = false;
+      auto it = dat_ver_.find(a.dat);
+      rec.ver[i] = it == dat_ver_.end() ? 0 : it->second;
+    } else if (a.kind == ARG_REDUCE || (a.kind == ARG_GBL && a.acc != ACC_READ)) {
+      rec.pure = false;
+    }
+  }
+  if (rec.pure) {
+    for (size_t q = queue_.size(); q-- > 0;) {
+      const LoopRecord &r = qrec_[q];
+      const Desc &e = queue_[q];
+      if (!r.pure || e.loop != d.loop || e.block != d.block || e.args.size() != na ||
+          memcmp(e.range, d.range, sizeof(d.range)) != 0)
+        continue;
+      bool same = true;
+      for (size_t i = 0; i < na && same; i++) {
+        const Arg &x = e.args[i], &y = d.args[i];
+        same = x.kind == y.kind && x.dat == y.dat && x.stencil == y.stencil && x.acc == y.acc && x.opt == y.opt &&
+               x.dim == y.dim && x.gbl == y.gbl && r.ver[i] == rec.ver[i];
+      }
+      if (same) return true;
+    }
+  }
+  // not redundant: the dats it writes get new versions
+  for (size_t i = 0; i < na; i++) {
+    const Arg &a = d.args[i];
+    if (a.kind == ARG_DAT && a.acc != ACC_READ) {
+      const unsigned long long v = ++ver_counter_;
+      dat_ver_[a.dat] = v;
+      rec.ver[i] = v;
+    }
+  }
+  return false;
 }
 
 void Runtime::launch_shape(const int *range, int dim, bool reduces, dim3 &grid, dim3 &block) {
@@ -579,6 +633,8 @@ void Runtime::execute() {
   if (!inited_ || queue_.empty()) return;
   std::vector<Desc> q;
   q.swap(queue_);
+  qrec_.clear();
+  dat_ver_.clear();
   run_queue(q);
 }
 

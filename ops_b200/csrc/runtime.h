@@ -195,6 +195,7 @@ class Runtime {
   double alg_bytes(const Desc &d) const;
   void timed_launch_end();
   void set_fusion(int on) { fusion_on_ = on; }
+  long long loops_skipped() const { return loops_skipped_; }
   int fusion_enabled() const { return fusion_on_; }
   int diags() const { return diags_; }
   void reset_counters() { kernels_launched_ = graphs_launched_ = loops_enqueued_ = 0; }
@@ -260,6 +261,19 @@ class Runtime {
   double cur_bytes_ = 0.0;
   cudaEvent_t cur_ev_ = nullptr;
   int fusion_on_ = 1;
+  // Redundant-loop elimination within one flush: per queued loop, the
+  // version of each dat arg (read: as observed, written: as produced);
+  // dat versions count the writes of the queued loops and restart at every
+  // flush (every other way of changing a dat flushes first).
+  struct LoopRecord {
+    bool pure = false;                 // only READ/WRITE dats, READ globals, indices
+    std::vector<unsigned long long> ver;
+  };
+  std::vector<LoopRecord> qrec_;
+  std::unordered_map<int, unsigned long long> dat_ver_;
+  unsigned long long ver_counter_ = 0;
+  long long loops_skipped_ = 0;
+  bool redundant(const Desc &d, LoopRecord &rec);
   long long kernels_launched_ = 0, graphs_launched_ = 0, loops_enqueued_ = 0;
 };
 

@@ -132,6 +132,13 @@ def ops_halo_transfer(group):
     check(lib().ops_b200_halo_transfer(group))
 
 
+def loops_skipped():
+    """Loops dropped as redundant since ops_init (see ops_b200_loops_skipped)."""
+    v = ctypes.c_longlong(0)
+    check(lib().ops_b200_loops_skipped(ctypes.byref(v)))
+    return v.value
+
+
 def ops_timers():
     """ops_timers: (cpu seconds, wall-clock seconds)."""
     c, e = ctypes.c_double(0.0), ctypes.c_double(0.0)
