@@ -575,6 +575,20 @@ void Runtime::launch_items(std::vector<Desc> &q) {
 
 void Runtime::run_queue(std::vector<Desc> &q) {
   elide_copies(q);
+  // OPSB_TRACE_QUEUE=1: every flushed loop to stderr (kernel, range, per dat
+  // arg: name, access, stencil points), for analysing loop chains
+  static const bool trace = getenv("OPSB_TRACE_QUEUE") != nullptr;
+  if (trace) {
+    fprintf(stderr, "flush %zu loops\n", q.size());
+    for (const Desc &d : q) {
+      fprintf(stderr, "  %s [%d,%d)x[%d,%d)", d.loop->kernel.c_str(), d.range[0], d.range[1], d.range[2], d.range[3]);
+      for (const Arg &a : d.args)
+        if (a.kind == ARG_DAT)
+          fprintf(stderr, " %s:%c%d", dat(a.dat).name.c_str(), "WRIMXX"[a.acc == ACC_READ ? 2 : a.acc == ACC_WRITE ? 0 : a.acc == ACC_RW ? 1 : 3],
+                  stencils_[a.stencil].points);
+      fprintf(stderr, "\n");
+    }
+  }
   // Stage the READ globals of the whole flush into the device arena.
   gbl_used_ = 0;
   for (Desc &d : q) {
