@@ -216,9 +216,16 @@ int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int warmup_steps, 
 /* TeaLeaf 2D implicit heat conduction (apps/c/TeaLeaf/diffuse.cpp:78-148,
  * tea_solve.cpp:37-418). The deck holds the tea.in values the reference
  * reads (apps/c/TeaLeaf/read_input.cpp:70-378); states use the CloverLeaf
- * state record (velocities ignored). solver: 0 Jacobi, 1 CG;
+ * state record (velocities ignored). solver: 0 Jacobi, 1 CG, 2 Chebyshev
+ * (tl_use_chebyshev), 3 polynomially preconditioned CG (tl_use_ppcg);
  * preconditioner: 0 none, 1 Jacobi diagonal (jac_diag); coefficient:
- * 1 conductivity = density, 2 reciprocal density.
+ * 1 conductivity = density, 2 reciprocal density. Solvers 2 and 3 start
+ * with CG and switch once the error is <= ch_cg_epslim after at least
+ * ch_cg_presteps iterations (tea_solve.cpp:146-160; the reference defaults
+ * are 25 and 1.0); ppcg_inner_steps is the polynomial degree, -1 for the
+ * reference's guess 4 * (int)sqrt(sqrt(x_cells * y_cells))
+ * (read_input.cpp:351-354). These three are read as given: a deck zeroed
+ * by the caller switches at once and never by error.
  * Beyond tea.in (no reference counterpart): fused = 1 runs each CG solve as
  * the device-resident three-kernel iteration (alpha, beta and the stop test
  * stay on the GPU; same per-cell arithmetic and stopping rule as the loop
@@ -240,6 +247,9 @@ typedef struct ops_b200_tea_deck {
   ops_b200_clover_state states[24];
   int fused, mixed, true_residual_stop;
   double reliable_delta;
+  int ch_cg_presteps;                     /* tl_ch_cg_presteps */
+  double ch_cg_epslim;                    /* tl_ch_cg_epslim */
+  int ppcg_inner_steps;                   /* tl_ppcg_inner_steps */
 } ops_b200_tea_deck;
 
 /* Runs the deck. summaries: 6 doubles per field summary {step, time, volume,
@@ -248,9 +258,12 @@ typedef struct ops_b200_tea_deck {
  * initial residual, final stopping quantity / initial residual, exact residual
  * ratio (tl_check_result) or -1, true FP64 residual ratio ||u0 - A u|| / ||r0||
  * at exit or -1 (fused solves compute it), reliable updates (mixed) or 0,
- * device seconds of the solve (coefficient set-up through finalise)}.
- * dump_dir as for CloverLeaf. */
-#define OPS_B200_TEA_SOLVE_COLS 7
+ * device seconds of the solve (coefficient set-up through finalise),
+ * PPCG inner iterations (tea_solve.cpp:389-392) or 0, the iteration n at
+ * which Chebyshev or PPCG took over or -1, the eigenvalue bounds in use
+ * (estimate scaled by 0.95 and 1.05) or 0, Chebyshev's estimated iteration
+ * count est_itc or -1}. dump_dir as for CloverLeaf. */
+#define OPS_B200_TEA_SOLVE_COLS 12
 int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summaries, int max_summaries, int *n_summaries,
                          double *solves, int max_solves, int *n_solves, double *device_seconds, const char *dump_dir);
 

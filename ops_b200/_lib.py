@@ -67,7 +67,8 @@ class TeaDeck(ctypes.Structure):
                 ("reflective_boundary", ctypes.c_int), ("check_result", ctypes.c_int),
                 ("number_of_states", ctypes.c_int), ("states", CloverState * 24),
                 ("fused", ctypes.c_int), ("mixed", ctypes.c_int), ("true_residual_stop", ctypes.c_int),
-                ("reliable_delta", ctypes.c_double)]
+                ("reliable_delta", ctypes.c_double), ("ch_cg_presteps", ctypes.c_int),
+                ("ch_cg_epslim", ctypes.c_double), ("ppcg_inner_steps", ctypes.c_int)]
 
 
 class HeatSystem(ctypes.Structure):

@@ -102,7 +102,12 @@ def cloverleaf(deck, warmup_steps=0, dump_dir=None, max_summaries=100000):
 TEA_DEFAULTS = dict(x_cells=10, y_cells=10, xmin=0.0, ymin=0.0, xmax=100.0, ymax=100.0, initial_timestep=0.1,
                     end_time=10.0, end_step=640000, summary_frequency=10, max_iters=1000, eps=1e-10,
                     coefficient=1, preconditioner=0, solver=0, reflective_boundary=0, check_result=0,
-                    fused=0, mixed=0, true_residual_stop=0, reliable_delta=0.1)
+                    fused=0, mixed=0, true_residual_stop=0, reliable_delta=0.1,
+                    ch_cg_presteps=25, ch_cg_epslim=1.0, ppcg_inner_steps=-1)
+TEA_SOLVERS = {0: "tl_use_jacobi", 1: "tl_use_cg", 2: "tl_use_chebyshev", 3: "tl_use_ppcg"}
+# columns of a solve record (OPS_B200_TEA_SOLVE_COLS)
+TEA_SOLVE_COLS = ("iterations", "initial_residual", "error_ratio", "exact_ratio", "true_ratio", "reliable_updates",
+                  "seconds", "ppcg_inner_iterations", "switch_iteration", "eigmin", "eigmax", "est_itc")
 
 
 def tea_deck(**kw):
@@ -142,7 +147,10 @@ def tea_deck_text(deck):
               f" end_time={g(deck.end_time)}", f" end_step={deck.end_step}",
               f" summary_frequency={deck.summary_frequency}", f" tl_max_iters={deck.max_iters}",
               f" tl_eps={deck.eps!r}"]
-    lines.append(" tl_use_cg" if deck.solver == 1 else " tl_use_jacobi")
+    lines.append(" " + TEA_SOLVERS[deck.solver])
+    if deck.solver in (2, 3):
+        lines += [f" tl_ch_cg_presteps={deck.ch_cg_presteps}", f" tl_ch_cg_epslim={g(deck.ch_cg_epslim)}",
+                  f" tl_ppcg_inner_steps={deck.ppcg_inner_steps}"]
     if deck.preconditioner == 1:
         lines.append(" tl_preconditioner_type=jac_diag")
     lines.append(" tl_coefficient_inverse_density" if deck.coefficient == 2 else " tl_coefficient_density")
@@ -155,13 +163,15 @@ def tea_deck_text(deck):
 
 
 def tealeaf(deck, dump_dir=None, max_rows=100000):
-    """Runs a TeaLeaf deck. Returns (summaries[n, 6], solves[m, 7], device_seconds):
+    """Runs a TeaLeaf deck. Returns (summaries[n, 6], solves[m, 12], device_seconds):
     summaries: step, time, volume, mass, internal energy, temperature;
-    solves: iterations, initial residual, error ratio, exact residual ratio,
-    true FP64 residual ratio (fused solves, else -1), reliable updates,
-    solve device seconds."""
+    solves: the TEA_SOLVE_COLS columns (iterations, initial residual, error
+    ratio, exact residual ratio, true FP64 residual ratio (fused solves, else
+    -1), reliable updates, solve device seconds, PPCG inner iterations, the
+    iteration Chebyshev/PPCG took over (-1 if not), eigenvalue bounds,
+    Chebyshev's estimated iteration count (-1 if none))."""
     out = np.zeros((max_rows, 6))
-    sv = np.zeros((max_rows, 7))
+    sv = np.zeros((max_rows, len(TEA_SOLVE_COLS)))
     n, ns = ctypes.c_int(0), ctypes.c_int(0)
     secs = ctypes.c_double(0.0)
     check(lib().ops_b200_app_tealeaf(ctypes.byref(deck), out.ctypes.data, max_rows, ctypes.byref(n), sv.ctypes.data,

@@ -1,8 +1,9 @@
 // TeaLeaf 2D driver on the OPS-B200 runtime: the loop sequence of the
 // reference app (apps/c/TeaLeaf/diffuse.cpp:78-148, start.cpp:46-110,
 // tea_solve.cpp:37-418 and the files they call, cited per function) for the
-// Jacobi and Jacobi-preconditioned CG solvers, with the deck passed as a
-// struct instead of tea.in.
+// Jacobi, CG, Chebyshev and PPCG solvers (no preconditioner or the Jacobi
+// diagonal one), with the deck passed as a struct instead of tea.in.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -30,6 +31,11 @@ struct Tea {
   double dt = 0, dtinit = 0.1, currtime = 0, end_time = 10.0, eps = 1e-10;
   int end_step = 640000, summary_frequency = 10, max_iters = 1000, coefficient = CONDUCTIVITY;
   int prec = TL_PREC_NONE, use_cg = 0, reflective_boundary = 0, check_result = 0;
+  // Chebyshev / PPCG (read_input.cpp:93-101, tea_solve.cpp:37-38): the
+  // eigenvalue estimate is made once per run (`first`) and reused by every
+  // later solve; theta persists with it.
+  int use_cheby = 0, use_ppcg = 0, ch_cg_presteps = 25, ppcg_inner_steps = -1, ppcg_active = 0, first = 1;
+  double ch_cg_epslim = 1.0, eigmin = 0.0, eigmax = 0.0, theta = 0.0, cn = 0.0;
   int step = 0, complete = 0;
   int g_rect = clover::G_RECT, g_circ = clover::G_CIRC, g_point = clover::G_POINT;
   int number_of_states = 0;
@@ -93,11 +99,20 @@ struct Tea {
     coefficient = d.coefficient == 2 ? RECIP_CONDUCTIVITY : CONDUCTIVITY;
     prec = d.preconditioner == 1 ? TL_PREC_JAC_DIAG : TL_PREC_NONE;
     use_cg = d.solver == 1;
+    use_cheby = d.solver == 2;
+    use_ppcg = d.solver == 3;
+    ch_cg_presteps = d.ch_cg_presteps;
+    ch_cg_epslim = d.ch_cg_epslim;
+    ppcg_inner_steps = d.ppcg_inner_steps;
+    if (ppcg_inner_steps == -1)  // read_input.cpp:351-354
+      ppcg_inner_steps = 4 * (int)(sqrt(sqrt((double)(d.x_cells * d.y_cells))));
     reflective_boundary = d.reflective_boundary;
     check_result = d.check_result;
     number_of_states = d.number_of_states;
     if (number_of_states < 1 || number_of_states > 24) throw Error(E_ARG, "1..24 states are supported");
-    if (d.solver != 0 && d.solver != 1) throw Error(E_UNSUPPORTED, "solver must be 0 (Jacobi) or 1 (CG)");
+    if (d.solver < 0 || d.solver > 3)
+      throw Error(E_UNSUPPORTED, "solver must be 0 (Jacobi), 1 (CG), 2 (Chebyshev) or 3 (PPCG)");
+    if (d.fused && d.solver != 1) throw Error(E_ARG, "fused solves need solver = 1 (CG)");
     fused = d.fused != 0;
     mixed = d.mixed != 0;
     true_stop = d.true_residual_stop != 0;
@@ -406,7 +421,7 @@ struct Tea {
   void cg_calc_p(double beta) {  // tea_leaf_cg.cpp:188-214
     int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
     double one = 1.0;
-    int src = prec != TL_PREC_NONE ? vector_z : vector_r;
+    int src = (prec != TL_PREC_NONE || ppcg_active) ? vector_z : vector_r;
     loop("tea_leaf_axpby_kernel", rng,
          {dat(vector_p, S2D_00, ACC_RW), dat(src, S2D_00, ACC_READ), arg_gbl(&beta, 1, 8, ACC_READ),
           arg_gbl(&one, 1, 8, ACC_READ)});
@@ -423,6 +438,225 @@ struct Tea {
     r.reduction_result(red_temp, &error);
     return error;
   }
+
+  // ---- Chebyshev (tea_leaf_cheby.cpp) ------------------------------------
+  // w = A u, r = u0 - w; p = (Mi r or r) / theta; u += p   (:43-96)
+  void cheby_init(double rx, double ry) {
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    cheby_residual(rx, ry);
+    int src = vector_r;
+    if (prec != TL_PREC_NONE) {
+      diag_solve();
+      src = vector_z;
+    }
+    loop("tea_leaf_recip3_kernel", rng,
+         {dat(vector_p, S2D_00, ACC_WRITE), dat(src, S2D_00, ACC_READ), arg_gbl(&theta, 1, 8, ACC_READ)});
+    loop("tea_leaf_xpy_kernel", rng, {dat(u, S2D_00, ACC_INC), dat(vector_p, S2D_00, ACC_READ)});
+  }
+  void cheby_residual(double rx, double ry) {
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    loop("tea_leaf_cheby_init_kernel", rng,
+         {dat(vector_w, S2D_00, ACC_WRITE), dat(vector_r, S2D_00, ACC_WRITE), dat(vector_Kx, S2D_00_P10, ACC_READ),
+          dat(vector_Ky, S2D_00_0P1, ACC_READ), dat(u, S2D_00_0M1_M10_P10_0P1, ACC_READ), dat(u0, S2D_00, ACC_READ),
+          arg_gbl(&rx, 1, 8, ACC_READ), arg_gbl(&ry, 1, 8, ACC_READ)});
+  }
+  // r = u0 - A u; p = alpha_k p + beta_k (Mi r or r); u += p   (:98-151)
+  void cheby_iterate(double rx, double ry, int k) {
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    cheby_residual(rx, ry);
+    int src = vector_r;
+    if (prec != TL_PREC_NONE) {
+      diag_solve();
+      src = vector_z;
+    }
+    loop("tea_leaf_axpby_kernel", rng,
+         {dat(vector_p, S2D_00, ACC_RW), dat(src, S2D_00, ACC_READ), arg_gbl(&ch_alphas[k], 1, 8, ACC_READ),
+          arg_gbl(&ch_betas[k], 1, 8, ACC_READ)});
+    loop("tea_leaf_xpy_kernel", rng, {dat(u, S2D_00, ACC_INC), dat(vector_p, S2D_00, ACC_READ)});
+  }
+
+  // Eigenvalues of the symmetric tridiagonal matrix d[1..n] (diagonal),
+  // e[2..n] (sub-diagonal) by the implicit QL method with Wilkinson shifts
+  // (Numerical Recipes' tqli, the routine tea_leaf_cheby.cpp:153-211 calls),
+  // overwriting d. The floating-point steps are those of the reference, so
+  // the estimate rounds identically. Returns false when an eigenvalue needs
+  // more than 30 sweeps.
+  static bool ql_implicit(double *d, double *e, int n) {
+    for (int i = 1; i < n; i++) e[i] = e[i + 1];
+    e[n] = 0.0;
+    for (int l = 1; l <= n; l++) {
+      for (int sweep = 0;; sweep++) {
+        int m = l;
+        for (; m <= n - 1; m++) {  // first negligible off-diagonal at or after l
+          double dd = fabs(d[m]) + fabs(d[m + 1]);
+          if (fabs(e[m]) + dd == dd) break;
+        }
+        if (m == l) break;
+        if (sweep == 30) return false;
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = sqrt(g * g + 1.0);
+        g = d[m] - d[l] + e[l] / (g + (g < 0.0 ? -r : r));
+        double s = 1.0, c = 1.0, p = 0.0;
+        bool deflated = false;
+        for (int i = m - 1; i >= l; i--) {  // chase the bulge with Givens rotations
+          double f = s * e[i], b = c * e[i];
+          r = sqrt(f * f + g * g);
+          e[i + 1] = r;
+          if (r == 0.0) {  // underflow: the matrix split, restart this eigenvalue
+            d[i + 1] = d[i + 1] - p;
+            e[m] = 0.0;
+            deflated = true;
+            break;
+          }
+          s = f / r;
+          c = g / r;
+          g = d[i + 1] - p;
+          r = (d[i] - g) * s + 2.0 * c * b;
+          p = s * r;
+          d[i + 1] = g + p;
+          g = c * r - b;
+        }
+        if (deflated) continue;
+        d[l] = d[l] - p;
+        e[l] = g;
+        e[m] = 0.0;
+      }
+    }
+    return true;
+  }
+
+  // Extreme eigenvalues of the Lanczos matrix that k CG steps define
+  // (tea_leaf_cheby.cpp:213-254): T_jj = 1/alpha_j + beta_{j-1}/alpha_{j-1},
+  // T_{j,j+1} = sqrt(beta_j)/alpha_j. The reference bubble-sorts the
+  // eigenvalues (and would not terminate on two equal ones); a sort gives
+  // the same extremes.
+  void calc_eigenvalues(int k) {
+    std::vector<double> d(max_iters + 2, 0.0), e(max_iters + 2, 0.0);
+    for (int n = 1; n <= k; n++) {
+      d[n] = 1.0 / cg_alphas[n];
+      if (n > 1) d[n] = d[n] + cg_betas[n - 1] / cg_alphas[n - 1];
+      if (n < k) e[n + 1] = sqrt(cg_betas[n]) / cg_alphas[n];
+    }
+    bool ok = ql_implicit(d.data(), e.data(), k);
+    if (ok && k > 1) std::sort(d.begin() + 1, d.begin() + k + 1);
+    eigmin = d[1];
+    eigmax = d[k];
+    if (!ok || eigmin < 0.0 || eigmax < 0.0) throw Error(E_STATE, "Error in calculating eigenvalues");
+  }
+
+  // Chebyshev recurrence coefficients for [eigmin, eigmax]   (:256-280)
+  void calc_ch_coefs(int count) {
+    theta = (eigmax + eigmin) / 2.0;
+    double delta = (eigmax - eigmin) / 2.0;
+    double sigma = theta / delta;
+    double rho_old = 1.0 / sigma;
+    for (int n = 1; n <= count; n++) {
+      double rho_new = 1.0 / (2.0 * sigma - rho_old);
+      ch_alphas[n] = rho_new * rho_old;
+      ch_betas[n] = 2.0 * rho_new / delta;
+      rho_old = rho_new;
+    }
+  }
+
+  // First Chebyshev step and the iteration estimate   (:282-316)
+  int cheby_first_step(double rx, double ry, double *error) {
+    double bb = calc_2norm(u0);
+    cheby_init(rx, ry);
+    update_halo(fields, 1);
+    cheby_iterate(rx, ry, 1);
+    *error = calc_2norm(vector_r);
+    double it_alpha = eps / 2.0 * sqrt(bb / (*error));
+    double gamm = (sqrt(cn) - 1.0) / (sqrt(cn) + 1.0);
+    return (int)round(log(it_alpha) / (log(gamm)));
+  }
+
+  // ---- PPCG (tea_leaf_ppcg.cpp) --------------------------------------------
+  // Steps 2 and 3 of the re-initialisation when the polynomial takes over
+  // (:85-152): step 2 refreshes z = Mi r, step 3 restarts p from z.
+  double ppcg_init(int step) {
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    double rro = 0.0;
+    if (step == 1)
+      loop("tea_leaf_init_zero2_kernel", rng, {dat(vector_p, S2D_00, ACC_WRITE), dat(vector_z, S2D_00, ACC_WRITE)});
+    else if (step == 3)
+      loop("tea_leaf_init_zero_kernel", rng, {dat(vector_p, S2D_00, ACC_WRITE)});
+    if (prec != TL_PREC_NONE || (ppcg_active && step == 3)) {
+      if (step == 1 || step == 2) diag_solve();
+      if (step == 1 || step == 3)
+        loop("tea_leaf_yeqx_kernel", rng, {dat(vector_p, S2D_00, ACC_WRITE), dat(vector_z, S2D_00, ACC_READ)});
+    } else if (step == 1) {
+      loop("tea_leaf_yeqx_kernel", rng, {dat(vector_p, S2D_00, ACC_WRITE), dat(vector_r, S2D_00, ACC_READ)});
+    }
+    if (step == 1 || step == 3) {
+      loop("tea_leaf_dot_kernel", rng,
+           {dat(vector_p, S2D_00, ACC_READ), dat(vector_r, S2D_00, ACC_READ), arg_reduce(red_temp, 1, ACC_INC)});
+      r.reduction_result(red_temp, &rro);
+    }
+    return rro;
+  }
+
+  // z <- the Chebyshev polynomial of degree ppcg_inner_steps applied to r
+  // (:300-364, init_sd :51-83, inner :154-215). As in the reference, the
+  // preconditioned variant refreshes z from r, not from rtemp, every step.
+  void run_ppcg_inner_steps(double rx, double ry) {
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    int f[NUM_FIELDS] = {0};
+    f[FIELD_U] = 1;
+    update_halo(f, 1);
+    double theta_r = 1.0 / theta;
+    if (prec != TL_PREC_NONE)
+      loop("tea_leaf_ppcg_init1_kernel", rng,
+           {dat(vector_sd, S2D_00, ACC_WRITE), dat(vector_rtemp, S2D_00, ACC_WRITE),
+            dat(vector_utemp, S2D_00, ACC_WRITE), dat(vector_z, S2D_00, ACC_READ), dat(vector_r, S2D_00, ACC_READ),
+            arg_gbl(&theta_r, 1, 8, ACC_READ)});
+    else
+      loop("tea_leaf_ppcg_init2_kernel", rng,
+           {dat(vector_sd, S2D_00, ACC_WRITE), dat(vector_rtemp, S2D_00, ACC_WRITE),
+            dat(vector_utemp, S2D_00, ACC_WRITE), dat(vector_r, S2D_00, ACC_READ), arg_gbl(&theta_r, 1, 8, ACC_READ)});
+    for (int k = 1; k <= ppcg_inner_steps; k++) {
+      int g[NUM_FIELDS] = {0};
+      g[FIELD_SD] = 1;
+      g[FIELD_R] = 1;
+      update_halo(g, 1);
+      loop("tea_leaf_ppcg_inner1_kernel", rng,
+           {dat(vector_rtemp, S2D_00, ACC_INC), dat(vector_Kx, S2D_00_P10, ACC_READ),
+            dat(vector_Ky, S2D_00_0P1, ACC_READ), dat(vector_sd, S2D_00_0M1_M10_P10_0P1, ACC_READ),
+            arg_gbl(&rx, 1, 8, ACC_READ), arg_gbl(&ry, 1, 8, ACC_READ)});
+      int src = vector_rtemp;
+      if (prec != TL_PREC_NONE) {
+        diag_solve();
+        src = vector_z;
+      }
+      loop("tea_leaf_ppcg_inner2_kernel", rng,
+           {dat(vector_sd, S2D_00, ACC_RW), dat(vector_utemp, S2D_00, ACC_INC), dat(src, S2D_00, ACC_READ),
+            arg_gbl(&ch_alphas[k], 1, 8, ACC_READ), arg_gbl(&ch_betas[k], 1, 8, ACC_READ)});
+    }
+    loop("tea_leaf_yeqx_kernel", rng, {dat(vector_z, S2D_00, ACC_WRITE), dat(vector_utemp, S2D_00, ACC_READ)});
+  }
+
+  double ppcg_calc_zrnorm() {  // :217-243
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    if (prec != TL_PREC_NONE || ppcg_active)
+      loop("tea_leaf_dot_kernel", rng,
+           {dat(vector_z, S2D_00, ACC_READ), dat(vector_r, S2D_00, ACC_READ), arg_reduce(red_temp, 1, ACC_INC)});
+    else
+      loop("tea_leaf_norm2_kernel", rng, {dat(vector_r, S2D_00, ACC_READ), arg_reduce(red_temp, 1, ACC_INC)});
+    double norm = 0.0;
+    r.reduction_result(red_temp, &norm);
+    return norm;
+  }
+
+  double ppcg_calc_rrn() {  // (r - rstore) . z, :275-298
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    loop("tea_leaf_ppcg_reduce_kernel", rng,
+         {dat(vector_rstore, S2D_00, ACC_READ), dat(vector_r, S2D_00, ACC_READ), dat(vector_z, S2D_00, ACC_READ),
+          arg_reduce(red_temp, 1, ACC_INC)});
+    double rrn = 0.0;
+    r.reduction_result(red_temp, &rrn);
+    return rrn;
+  }
+
+  std::vector<double> cg_alphas, cg_betas, ch_alphas, ch_betas;
 
   double *interior(int d) {
     Dat &x = r.dat(d);
@@ -456,13 +690,18 @@ struct Tea {
       solver.pcg_fp64(f, rx, ry, pre, true_stop, eps, max_iters, r.stream(), &st);
     r.count_kernels(solver.launches());
     const double ir = st.initial_residual;
-    double srow[7] = {(double)st.iterations, ir, st.error / ir, -1.0, st.true_residual / ir, (double)st.outer, 0.0};
-    solves.insert(solves.end(), srow, srow + 7);
+    double srow[OPS_B200_TEA_SOLVE_COLS] = {(double)st.iterations, ir, st.error / ir, -1.0, st.true_residual / ir,
+                                            (double)st.outer, 0.0, 0.0, -1.0, 0.0, 0.0, -1.0};
+    solves.insert(solves.end(), srow, srow + OPS_B200_TEA_SOLVE_COLS);
   }
 
-  // tea_solve.cpp:37-418 for tl_use_cg / tl_use_jacobi.
+  // tea_solve.cpp:40-398: Jacobi, CG, and Chebyshev / PPCG after CG
+  // presteps; the solve record gets the reference's printed quantities.
   void tea_leaf() {
     double rx, ry, rro = 0.0;
+    ppcg_active = 0;
+    int cheby_calc_steps = 0, ch_switch_check = 0, ppcg_inner_iters = 0, est_itc = -1, max_cheby_iters = 0;
+    int switched_at = -1;
     set_fields({FIELD_ENERGY1, FIELD_DENSITY});
     update_halo(fields, 1);
     common_init(1, &rx, &ry);
@@ -475,8 +714,10 @@ struct Tea {
     update_halo(fields, 1);
     calc_residual(rx, ry);
     double initial_residual = calc_2norm(vector_r);
+    double old_error = initial_residual;  // the squared norm, as tea_solve.cpp:106-108 has it
     initial_residual = sqrt(fabs(initial_residual));
-    if (use_cg) {
+    const bool krylov = use_cg || use_cheby || use_ppcg;
+    if (krylov) {
       rro = cg_init();
       set_fields({FIELD_U, FIELD_P});
       update_halo(fields, 1);
@@ -484,14 +725,83 @@ struct Tea {
     } else {
       set_fields({FIELD_U});
     }
+    cg_alphas.assign(max_iters + 1, 0.0);
+    cg_betas.assign(max_iters + 1, 0.0);
     double error = 0.0;
     int n;
     for (n = 1; n <= max_iters; n++) {
-      if (use_cg) {
+      if (ch_switch_check == 0) {  // :146-160
+        if (cheby_calc_steps > 0)
+          ch_switch_check = 1;
+        else if (first == 0 && use_ppcg && n > 1)
+          ch_switch_check = 1;
+        else if (fabs(old_error) <= ch_cg_epslim && n >= ch_cg_presteps)
+          ch_switch_check = 1;
+      }
+      if ((use_cheby || use_ppcg) && ch_switch_check) {
+        if (cheby_calc_steps == 0) {  // :165-238
+          max_cheby_iters = max_iters - n + 2;
+          if (first) {
+            calc_eigenvalues(n - 1);
+            first = 0;
+            eigmin = eigmin * 0.95;
+            eigmax = eigmax * 1.05;
+          }
+          // room for max_cheby_iters = max_iters + 1 (a switch at n = 1) and
+          // for the inner steps that also run on the Chebyshev path
+          size_t len = (size_t)std::max(max_iters + 2, ppcg_inner_steps + 1);
+          ch_alphas.assign(len, 0.0);
+          ch_betas.assign(len, 0.0);
+          if (use_cheby) {
+            calc_ch_coefs(max_cheby_iters);
+            set_fields({FIELD_U});
+          } else {
+            calc_ch_coefs(ppcg_inner_steps);
+            ppcg_active = 1;
+          }
+          cn = eigmax / eigmin;
+          switched_at = n;
+          rro = ppcg_init(2);
+          run_ppcg_inner_steps(rx, ry);
+          ppcg_inner_iters = ppcg_inner_iters + ppcg_inner_steps;
+          rro = ppcg_init(3);
+          set_fields({FIELD_U, FIELD_P});
+          update_halo(fields, 1);
+          set_fields({FIELD_P});
+        }
+        if (use_cheby) {  // :240-256
+          if (cheby_calc_steps == 0) {
+            est_itc = cheby_first_step(rx, ry, &old_error);
+            cheby_calc_steps = 1;
+          } else {
+            cheby_iterate(rx, ry, cheby_calc_steps);
+            // the residual is only measured every 10th step past est_itc;
+            // in between `error` keeps its last value (and is re-rooted below)
+            if (n >= est_itc && n % 10 == 0) error = calc_2norm(vector_r);
+          }
+        } else {  // PPCG as flexible CG (:261-300)
+          double pw = cg_calc_w(rx, ry);
+          loop_yeqx(vector_rstore, vector_r);
+          rro = ppcg_calc_zrnorm();
+          double alpha = rro / pw;
+          cg_calc_ur(alpha);
+          run_ppcg_inner_steps(rx, ry);
+          ppcg_inner_iters = ppcg_inner_iters + ppcg_inner_steps;
+          double rrn = ppcg_calc_rrn();
+          double beta = rrn / rro;
+          cg_calc_p(beta);
+          error = rrn;
+          rro = rrn;
+        }
+        cheby_calc_steps = cheby_calc_steps + 1;
+      } else if (krylov) {  // :305-330
+        fields[FIELD_P] = 1;
         double pw = cg_calc_w(rx, ry);
         double alpha = rro / pw;
+        cg_alphas[n] = alpha;
         double rrn = cg_calc_ur(alpha);
         double beta = rrn / rro;
+        cg_betas[n] = beta;
         cg_calc_p(beta);
         error = rrn;
         rro = rrn;
@@ -501,6 +811,7 @@ struct Tea {
       update_halo(fields, 1);
       error = sqrt(fabs(error));
       if (fabs(error) < eps * initial_residual) break;
+      old_error = error;
     }
     double exact = -1.0;
     if (check_result) {
@@ -510,9 +821,17 @@ struct Tea {
       exact = sqrt(calc_2norm(vector_r)) / initial_residual;
     }
     // the reference reports n - 1 (tea_solve.cpp:386), also when the loop ran out
-    double srow[7] = {(double)(n - 1), initial_residual, error / initial_residual, exact, -1.0, 0.0, 0.0};
-    solves.insert(solves.end(), srow, srow + 7);
+    const bool poly = switched_at > 0;
+    double srow[OPS_B200_TEA_SOLVE_COLS] = {(double)(n - 1), initial_residual, error / initial_residual, exact, -1.0,
+                                            0.0, 0.0, (double)ppcg_inner_iters, (double)switched_at,
+                                            poly ? eigmin : 0.0, poly ? eigmax : 0.0, (double)est_itc};
+    solves.insert(solves.end(), srow, srow + OPS_B200_TEA_SOLVE_COLS);
     finalise();
+  }
+
+  void loop_yeqx(int y, int x) {  // tea_leaf_ppcg_store_r, tea_leaf_ppcg.cpp:258-273
+    int rng[] = {field.x_min, field.x_max, field.y_min, field.y_max};
+    loop("tea_leaf_yeqx_kernel", rng, {dat(y, S2D_00, ACC_WRITE), dat(x, S2D_00, ACC_READ)});
   }
 
   void finalise() {  // tea_leaf_finalise (tea_solve.cpp:400-418)
@@ -555,7 +874,7 @@ struct Tea {
     OPSB_CUDA(cudaEventSynchronize(ev_solve[1]));
     float ms = 0.f;
     OPSB_CUDA(cudaEventElapsedTime(&ms, ev_solve[0], ev_solve[1]));
-    solves.back() = ms * 1e-3;
+    solves[solves.size() - OPS_B200_TEA_SOLVE_COLS + 6] = ms * 1e-3;
     currtime = currtime + dt;
     if (summary_frequency != 0)
       if ((step % summary_frequency) == 0) field_summary();

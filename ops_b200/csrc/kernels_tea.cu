@@ -272,6 +272,66 @@ struct tea_leaf_cg_calc_ur_r_reduce_kernel {  // :17
   }
 };
 
+// ---- tea_leaf_kernels.h:30, :50 (Chebyshev and PPCG helpers) --------------------
+struct tea_leaf_xpy_kernel {  // :30
+  TL_LOOP(tea_leaf_xpy_kernel);
+  __device__ void operator()(D &u, const D &p) const { u(0, 0) = u(0, 0) + p(0, 0); }
+};
+struct tea_leaf_recip3_kernel {  // :50
+  TL_LOOP(tea_leaf_recip3_kernel);
+  __device__ void operator()(D &z, const D &x, const double *theta) const { z(0, 0) = x(0, 0) / (*theta); }
+};
+
+// ---- tea_leaf_cheby_kernels.h:7 ------------------------------------------------------
+struct tea_leaf_cheby_init_kernel {
+  TL_LOOP(tea_leaf_cheby_init_kernel);
+  __device__ void operator()(D &w, D &r, const D &Kx, const D &Ky, const D &u, const D &u0, const double *rx,
+                             const double *ry) const {
+    w(0, 0) = tea_smvp(Kx, Ky, u, *rx, *ry);
+    r(0, 0) = u0(0, 0) - w(0, 0);
+  }
+};
+
+// ---- tea_leaf_ppcg_kernels.h ----------------------------------------------------------
+struct tea_leaf_ppcg_init1_kernel {  // :7
+  TL_LOOP(tea_leaf_ppcg_init1_kernel);
+  __device__ void operator()(D &sd, D &rtemp, D &utemp, const D &z, const D &r, const double *theta_r) const {
+    sd(0, 0) = z(0, 0) * (*theta_r);
+    rtemp(0, 0) = r(0, 0);
+    utemp(0, 0) = sd(0, 0);
+  }
+};
+struct tea_leaf_ppcg_init2_kernel {  // :13
+  TL_LOOP(tea_leaf_ppcg_init2_kernel);
+  __device__ void operator()(D &sd, D &rtemp, D &utemp, const D &r, const double *theta_r) const {
+    sd(0, 0) = r(0, 0) * (*theta_r);
+    rtemp(0, 0) = r(0, 0);
+    utemp(0, 0) = sd(0, 0);
+  }
+};
+struct tea_leaf_ppcg_inner1_kernel {  // :19
+  TL_LOOP(tea_leaf_ppcg_inner1_kernel);
+  __device__ void operator()(D &rtemp, const D &Kx, const D &Ky, const D &sd, const double *rx,
+                             const double *ry) const {
+    double smvp = 0.0;
+    smvp = tea_smvp(Kx, Ky, sd, *rx, *ry);
+    rtemp(0, 0) = rtemp(0, 0) - smvp;
+  }
+};
+struct tea_leaf_ppcg_inner2_kernel {  // :30
+  TL_LOOP(tea_leaf_ppcg_inner2_kernel);
+  __device__ void operator()(D &sd, D &utemp, const D &z, const double *alpha, const double *beta) const {
+    sd(0, 0) = (*alpha) * sd(0, 0) + (*beta) * z(0, 0);
+    utemp(0, 0) = utemp(0, 0) + sd(0, 0);
+  }
+};
+struct tea_leaf_ppcg_reduce_kernel {  // :35
+  TL_LOOP(tea_leaf_ppcg_reduce_kernel);
+  __device__ void operator()(const D &rstore, const D &r, const D &z, RED<double> &rnn) const {
+    *rnn = *rnn + (r(0, 0) - rstore(0, 0)) * z(0, 0);
+  }
+};
+
 // ---- tea_leaf_jacobi_kernels.h:8 ---------------------------------------------------
 struct tea_leaf_jacobi_kernel {
   TL_LOOP(tea_leaf_jacobi_kernel);
@@ -310,7 +370,9 @@ REG(tea_leaf_common_residual_kernel) REG(tea_leaf_common_init_diag_init_kernel) 
 REG(tea_leaf_init_zero_kernel) REG(tea_leaf_yeqx_kernel) REG(tea_leaf_dot_kernel) REG(tea_leaf_axpy_kernel)
 REG(tea_leaf_axpby_kernel) REG(tea_leaf_zeqxty_kernel) REG(tea_leaf_recip_kernel) REG(tea_leaf_recip2_kernel)
 REG(tea_leaf_norm2_kernel) REG(tea_leaf_cg_calc_w_reduce_kernel) REG(tea_leaf_cg_calc_ur_r_reduce_kernel)
-REG(tea_leaf_jacobi_kernel) REG(field_summary_kernel)
+REG(tea_leaf_jacobi_kernel) REG(field_summary_kernel) REG(tea_leaf_xpy_kernel) REG(tea_leaf_recip3_kernel)
+REG(tea_leaf_cheby_init_kernel) REG(tea_leaf_ppcg_init1_kernel) REG(tea_leaf_ppcg_init2_kernel)
+REG(tea_leaf_ppcg_inner1_kernel) REG(tea_leaf_ppcg_inner2_kernel) REG(tea_leaf_ppcg_reduce_kernel)
 
 struct ConstReg {
   ConstReg() {

@@ -122,6 +122,23 @@ TEA_CASES = [
     ("tea_cg_plain_100x70", dict(x_cells=100, y_cells=70, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=1,
                                  max_iters=5000, eps=1e-10, solver=1, preconditioner=0, summary_frequency=1,
                                  states=("seeded", 100, 70, 7))),
+    # Chebyshev and PPCG after CG presteps (tea_solve.cpp:146-300); dt = 0.04
+    # gives condition numbers near 100, so the polynomial phases run for
+    # tens to hundreds of iterations, and later timesteps reuse the first
+    # solve's eigenvalue estimate
+    ("tea_cheby_plain_96", dict(x_cells=96, y_cells=96, xmax=10.0, ymax=10.0, initial_timestep=0.04, end_step=3,
+                                max_iters=5000, eps=1e-10, solver=2, preconditioner=0, summary_frequency=1,
+                                states=("seeded", 96, 96, 4))),
+    ("tea_cheby_jacdiag_80x64", dict(x_cells=80, y_cells=64, xmax=10.0, ymax=10.0, initial_timestep=0.04,
+                                     end_step=2, max_iters=5000, eps=1e-10, solver=2, preconditioner=1,
+                                     summary_frequency=1, states=("seeded", 80, 64, 11))),
+    ("tea_ppcg_plain_96", dict(x_cells=96, y_cells=96, xmax=10.0, ymax=10.0, initial_timestep=0.04, end_step=3,
+                               max_iters=5000, eps=1e-10, solver=3, preconditioner=0, summary_frequency=1,
+                               states=("seeded", 96, 96, 4))),
+    ("tea_ppcg_jacdiag_64", dict(x_cells=64, y_cells=64, xmax=10.0, ymax=10.0, initial_timestep=0.04, end_step=2,
+                                 max_iters=5000, eps=1e-10, solver=3, preconditioner=1, summary_frequency=1,
+                                 ch_cg_presteps=10, ch_cg_epslim=0.5, ppcg_inner_steps=12,
+                                 states=("seeded", 64, 64, 5))),
 ]
 TEA_DUMP = ["u", "energy1", "density"]
 
@@ -155,6 +172,13 @@ def run_reference_tea(deck_text, dump=False, threads=1, timeout=900):
         summ = [[float(x) for x in l.split()[1:7]] for l in out.splitlines() if l.strip().startswith("step:")]
         iters = [int(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Iteration count")]
         errs = [float(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Conduction error")]
+        # Chebyshev / PPCG lines (tea_solve.cpp:228-231, tea_leaf_cheby.cpp:312-313, tea_solve.cpp:389-392)
+        lines = r.stdout.splitlines()
+        poly = dict(
+            switch=[int(l.split()[2]) for l in lines if l.startswith("Switching after")],
+            eig=[[float(l.split()[2]), float(l.split()[5])] for l in lines if l.startswith("Eigen min")],
+            est_itc=[int(lines[i + 1]) for i, l in enumerate(lines) if l.strip() == "est itc"],
+            ppcg=[int(l.split()[3]) for l in lines if l.startswith("PPCG Iteration count")])
         dumps = {}
         if dump:
             # the reference pads TeaLeaf dat names with blanks (build_field.cpp:55-73)
@@ -167,7 +191,7 @@ def run_reference_tea(deck_text, dump=False, threads=1, timeout=900):
                 a = np.fromfile(os.path.join(td, fn + ".bin"), dtype=np.float64).reshape(size[1], size[0])
                 dumps[name] = a[:, :size[0] - xpad]
     # summary columns: step, vol, mass, density, ie, temp
-    return np.array(summ), np.array(iters), np.array(errs), dumps
+    return np.array(summ), np.array(iters), np.array(errs), dumps, {k: np.array(v) for k, v in poly.items()}
 
 
 def tea():
@@ -177,10 +201,10 @@ def tea():
         kw["states"] = tea_states(kw["states"])
         deck = apps.tea_deck(**kw)
         text = apps.tea_deck_text(deck)
-        summ, iters, errs, dumps = run_reference_tea(text, dump=True)
+        summ, iters, errs, dumps, poly = run_reference_tea(text, dump=True)
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, deck=text, summaries=summ, iters=iters, errors=errs,
-                            **{"f_" + k: v for k, v in dumps.items()})
+                            **{"f_" + k: v for k, v in dumps.items()}, **{"poly_" + k: v for k, v in poly.items()})
         print("wrote", path, summ.shape, iters, errs)
 
 

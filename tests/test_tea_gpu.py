@@ -7,7 +7,11 @@ and density are compared bit for bit and the iteration counts exactly. CG:
 alpha and beta come from FP64 dot products whose summation order differs from
 the reference's, so u carries rounding differences of a few ulps per
 iteration; the iteration counts must still match exactly, the fields hold to
-1e-10 of their maximum and the field summaries to 1e-12 relative."""
+1e-10 of their maximum and the field summaries to 1e-12 relative. Chebyshev
+and PPCG: the same bars, plus the iteration at which the polynomial phase
+took over, Chebyshev's iteration estimate and the PPCG inner-iteration count
+exactly, and the eigenvalue bounds (from the CG coefficients through the QL
+eigenvalue solve) to 1e-10 relative."""
 import glob
 import os
 
@@ -36,7 +40,22 @@ CASES = {
     "tea_cg_plain_100x70": dict(x_cells=100, y_cells=70, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=1,
                                 max_iters=5000, eps=1e-10, solver=1, preconditioner=0, summary_frequency=1,
                                 states=seeded.tea_config4_states(100, 70, 7)),
+    "tea_cheby_plain_96": dict(x_cells=96, y_cells=96, xmax=10.0, ymax=10.0, initial_timestep=0.04, end_step=3,
+                               max_iters=5000, eps=1e-10, solver=2, preconditioner=0, summary_frequency=1,
+                               states=seeded.tea_config4_states(96, 96, 4)),
+    "tea_cheby_jacdiag_80x64": dict(x_cells=80, y_cells=64, xmax=10.0, ymax=10.0, initial_timestep=0.04,
+                                    end_step=2, max_iters=5000, eps=1e-10, solver=2, preconditioner=1,
+                                    summary_frequency=1, states=seeded.tea_config4_states(80, 64, 11)),
+    "tea_ppcg_plain_96": dict(x_cells=96, y_cells=96, xmax=10.0, ymax=10.0, initial_timestep=0.04, end_step=3,
+                              max_iters=5000, eps=1e-10, solver=3, preconditioner=0, summary_frequency=1,
+                              states=seeded.tea_config4_states(96, 96, 4)),
+    "tea_ppcg_jacdiag_64": dict(x_cells=64, y_cells=64, xmax=10.0, ymax=10.0, initial_timestep=0.04, end_step=2,
+                                max_iters=5000, eps=1e-10, solver=3, preconditioner=1, summary_frequency=1,
+                                ch_cg_presteps=10, ch_cg_epslim=0.5, ppcg_inner_steps=12,
+                                states=seeded.tea_config4_states(64, 64, 5)),
 }
+REL_EIG = 1e-10
+COL = {k: i for i, k in enumerate(apps.TEA_SOLVE_COLS)}
 
 
 def as_reference_columns(s):
@@ -54,6 +73,15 @@ def test_matches_reference_golden(gpu_runtime, path, tmp_path):
     assert apps.tea_deck_text(deck) == str(g["deck"])
     summ, solves, _ = apps.tealeaf(deck, dump_dir=str(tmp_path))
     assert np.array_equal(solves[:, 0].astype(np.int64), g["iters"])
+    if kw["solver"] in (2, 3):
+        switched = solves[:, COL["switch_iteration"]] > 0
+        assert np.array_equal(solves[switched, COL["switch_iteration"]].astype(np.int64), g["poly_switch"])
+        eig = solves[switched][:, [COL["eigmin"], COL["eigmax"]]]
+        np.testing.assert_allclose(eig, g["poly_eig"], rtol=REL_EIG, atol=0)
+        if kw["solver"] == 2:
+            assert np.array_equal(solves[switched, COL["est_itc"]].astype(np.int64), g["poly_est_itc"])
+        else:
+            assert np.array_equal(solves[:, COL["ppcg_inner_iterations"]].astype(np.int64), g["poly_ppcg"])
     ours = as_reference_columns(summ)
     ref = g["summaries"]
     assert ours.shape == ref.shape
