@@ -95,7 +95,11 @@ int ops_b200_halo_transfer(int group);
 int ops_b200_timers(double *cpu, double *et);
 
 /* ops_decl_const / ops_update_const (ops/c/include/ops_lib_core.h:947,971):
- * flushes queued loops, then updates every kernel constant of that name. */
+ * flushes queued loops, then updates every kernel constant of that name.
+ * "<app>/<name>" (app = the kernels' prefix: laplace2d, cloverleaf,
+ * cloverleaf3d, tealeaf) updates that app's constant only; a bare name of a
+ * struct type whose layout differs between apps (field, grid, states) is
+ * rejected with OPS_B200_ERR_ARG, since its size would be ambiguous. */
 int ops_b200_decl_const(const char *name, int dim, const char *type, const void *data);
 int ops_b200_update_const(const char *name, int dim, const char *type, const void *data);
 
@@ -212,6 +216,29 @@ typedef struct ops_b200_clover_deck {
  * to <dump_dir>/<name>.bin at the end. */
 int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int warmup_steps, double *summaries,
                             int max_summaries, int *n_summaries, double *device_seconds, const char *dump_dir);
+
+/* CloverLeaf 3D hydro (apps/c/CloverLeaf_3D/clover_leaf.cpp:133-213): the
+ * clover.in values of the 3D app (read_input.cpp:37-276; the reference's
+ * defaults are timestep_rise 1.05, max_timestep 1.0, end_time 10.0). */
+typedef struct ops_b200_clover3d_state {
+  double density, energy, xvel, yvel, zvel;
+  int geometry;                           /* 1 cuboid, 2 sphere, 3 point       */
+  double xmin, xmax, ymin, ymax, zmin, zmax, radius;
+} ops_b200_clover3d_state;
+
+typedef struct ops_b200_clover3d_deck {
+  int x_cells, y_cells, z_cells;
+  double xmin, ymin, zmin, xmax, ymax, zmax;
+  double initial_timestep, timestep_rise, max_timestep, end_time;
+  int end_step, summary_frequency;
+  int number_of_states;                   /* 1..16; state 0 is the background */
+  ops_b200_clover3d_state states[16];
+} ops_b200_clover3d_deck;
+
+/* Runs the 3D deck to completion; outputs as ops_b200_app_cloverleaf (8
+ * doubles per field summary, kinetic energy over the eight nodes of a cell). */
+int ops_b200_app_cloverleaf3d(const ops_b200_clover3d_deck *deck, int warmup_steps, double *summaries,
+                              int max_summaries, int *n_summaries, double *device_seconds, const char *dump_dir);
 
 /* TeaLeaf 2D implicit heat conduction (apps/c/TeaLeaf/diffuse.cpp:78-148,
  * tea_solve.cpp:37-418). The deck holds the tea.in values the reference

@@ -58,6 +58,24 @@ class CloverDeck(ctypes.Structure):
                 ("states", CloverState * 16)]
 
 
+class Clover3DState(ctypes.Structure):
+    _fields_ = [("density", ctypes.c_double), ("energy", ctypes.c_double), ("xvel", ctypes.c_double),
+                ("yvel", ctypes.c_double), ("zvel", ctypes.c_double), ("geometry", ctypes.c_int),
+                ("xmin", ctypes.c_double), ("xmax", ctypes.c_double), ("ymin", ctypes.c_double),
+                ("ymax", ctypes.c_double), ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
+                ("radius", ctypes.c_double)]
+
+
+class Clover3DDeck(ctypes.Structure):
+    _fields_ = [("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int), ("z_cells", ctypes.c_int),
+                ("xmin", ctypes.c_double), ("ymin", ctypes.c_double), ("zmin", ctypes.c_double),
+                ("xmax", ctypes.c_double), ("ymax", ctypes.c_double), ("zmax", ctypes.c_double),
+                ("initial_timestep", ctypes.c_double), ("timestep_rise", ctypes.c_double),
+                ("max_timestep", ctypes.c_double), ("end_time", ctypes.c_double), ("end_step", ctypes.c_int),
+                ("summary_frequency", ctypes.c_int), ("number_of_states", ctypes.c_int),
+                ("states", Clover3DState * 16)]
+
+
 class TeaDeck(ctypes.Structure):
     _fields_ = [("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int), ("xmin", ctypes.c_double),
                 ("ymin", ctypes.c_double), ("xmax", ctypes.c_double), ("ymax", ctypes.c_double),
@@ -146,6 +164,7 @@ def _declare(L):
         "ops_b200_kernel_stats": ([P, i], i),
         "ops_b200_app_laplace2d": ([i, i, i, i, P, P, P, P], i),
         "ops_b200_app_cloverleaf": ([P, i, P, i, P, P, cp], i),
+        "ops_b200_app_cloverleaf3d": ([P, i, P, i, P, P, cp], i),
         "ops_b200_app_tealeaf": ([P, P, i, P, P, i, P, P, cp], i),
         "ops_b200_tridMultiDimBatch": ([i, i, P, i, i, i, i], i),
         "ops_b200_tridMultiDimBatch_Inc": ([i, i, P, i, i, i, i, i], i),

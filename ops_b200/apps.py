@@ -96,6 +96,79 @@ def cloverleaf(deck, warmup_steps=0, dump_dir=None, max_summaries=100000):
 
 
 # ---------------------------------------------------------------------------
+# CloverLeaf 3D
+# ---------------------------------------------------------------------------
+# apps/c/CloverLeaf_3D/read_input.cpp:44-80 defaults, overridden by the deck.
+CLOVER3D_DEFAULTS = dict(x_cells=10, y_cells=10, z_cells=10, xmin=0.0, ymin=0.0, zmin=0.0, xmax=100.0, ymax=100.0,
+                         zmax=100.0, initial_timestep=0.1, timestep_rise=1.05, max_timestep=1.0, end_time=10.0,
+                         end_step=640000, summary_frequency=10)
+GEOMETRY3D = {"cuboid": 1, "sphere": 2, "point": 3}
+
+
+def clover3d_deck(**kw):
+    """A 3D deck from keyword values; `states` is a list of dicts with density,
+    energy and optionally xvel, yvel, zvel, geometry, xmin..zmax, radius."""
+    from ._lib import Clover3DDeck
+    d = Clover3DDeck()
+    vals = dict(CLOVER3D_DEFAULTS)
+    vals.update({k: v for k, v in kw.items() if k != "states"})
+    for k, v in vals.items():
+        setattr(d, k, v)
+    states = kw["states"]
+    d.number_of_states = len(states)
+    for i, s in enumerate(states):
+        st = d.states[i]
+        st.density, st.energy = s["density"], s["energy"]
+        st.xvel, st.yvel, st.zvel = s.get("xvel", 0.0), s.get("yvel", 0.0), s.get("zvel", 0.0)
+        g = s.get("geometry", 0)
+        st.geometry = GEOMETRY3D.get(g, g) if isinstance(g, str) else g
+        for k in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "radius"):
+            setattr(st, k, s.get(k, 0.0))
+    return d
+
+
+def clover3d_deck_text(deck):
+    """The 3D deck as clover.in text for the reference build. The reference
+    reads checkpoint_frequency as a divisor every step (clover_leaf.cpp:204)
+    and leaves it 0 when absent, so the text always sets it (its checkpoint
+    hook does nothing in a build without HDF5)."""
+    g = lambda v: repr(float(v))
+    lines = ["*clover"]
+    for i in range(deck.number_of_states):
+        s = deck.states[i]
+        line = f" state {i + 1} density={g(s.density)} energy={g(s.energy)}"
+        for k in ("xvel", "yvel", "zvel"):
+            if getattr(s, k) != 0.0:
+                line += f" {k}={g(getattr(s, k))}"
+        if i > 0:
+            geo = {1: "cuboid", 2: "sphere", 3: "point"}[s.geometry]
+            line += (f" geometry={geo} xmin={g(s.xmin)} xmax={g(s.xmax)} ymin={g(s.ymin)} ymax={g(s.ymax)}"
+                     f" zmin={g(s.zmin)} zmax={g(s.zmax)}")
+            if s.geometry == 2:
+                line += f" radius={g(s.radius)}"
+        lines.append(line)
+    lines += [f" x_cells={deck.x_cells}", f" y_cells={deck.y_cells}", f" z_cells={deck.z_cells}",
+              f" xmin={g(deck.xmin)}", f" ymin={g(deck.ymin)}", f" zmin={g(deck.zmin)}", f" xmax={g(deck.xmax)}",
+              f" ymax={g(deck.ymax)}", f" zmax={g(deck.zmax)}", f" initial_timestep={g(deck.initial_timestep)}",
+              f" timestep_rise={g(deck.timestep_rise)}", f" max_timestep={g(deck.max_timestep)}",
+              f" end_time={g(deck.end_time)}", f" end_step={deck.end_step}",
+              f" summary_frequency={deck.summary_frequency}", " checkpoint_frequency=10", "*endclover", ""]
+    return "\n".join(lines)
+
+
+def cloverleaf3d(deck, warmup_steps=0, dump_dir=None, max_summaries=100000):
+    """Runs a CloverLeaf 3D deck on the GPU. Returns (summaries[n, 8], device_seconds);
+    columns as cloverleaf()."""
+    out = np.zeros((max_summaries, 8))
+    n = ctypes.c_int(0)
+    secs = ctypes.c_double(0.0)
+    check(lib().ops_b200_app_cloverleaf3d(ctypes.byref(deck), warmup_steps, out.ctypes.data, max_summaries,
+                                          ctypes.byref(n), ctypes.byref(secs),
+                                          dump_dir.encode() if dump_dir else None))
+    return out[:n.value].copy(), secs.value
+
+
+# ---------------------------------------------------------------------------
 # TeaLeaf
 # ---------------------------------------------------------------------------
 # read_input.cpp:70-103 defaults (Jacobi, no preconditioner, conductivity).

@@ -428,7 +428,7 @@ struct Clover {
       kdt = kldt;
     }
     dt_temp = op_min(op_min(dt_temp, (dtold * dtrise)), dtmax);
-    r.decl_const("dt", 1, "double", &dt_temp);
+    r.decl_const("cloverleaf/dt", 1, "double", &dt_temp);
     dt = dt_temp;
     if (dt < dtmin) throw Error(E_STATE, "cloverleaf: small timestep (time_step.cpp:123-126)");
     dtold = dt;
@@ -637,20 +637,20 @@ struct Clover {
   // clover_leaf.cpp:133-160 + start.cpp:44-112
   void setup(const ops_b200_clover_deck &deck) {
     read_input(deck);
-    r.decl_const("g_small", 1, "double", &g_small);
-    r.decl_const("g_big", 1, "double", &g_big);
-    r.decl_const("dtc_safe", 1, "double", &dtc_safe);
-    r.decl_const("dtu_safe", 1, "double", &dtu_safe);
-    r.decl_const("dtv_safe", 1, "double", &dtv_safe);
-    r.decl_const("dtdiv_safe", 1, "double", &dtdiv_safe);
-    r.decl_const("field", 1, "field_type", &field);
-    r.decl_const("grid", 1, "grid_type", &grid);
-    r.decl_const("number_of_states", 1, "int", &number_of_states);
-    r.decl_const("states", number_of_states, "state_type", states);
-    r.decl_const("g_circ", 1, "int", &g_circ);
-    r.decl_const("g_point", 1, "int", &g_point);
-    r.decl_const("g_rect", 1, "int", &g_rect);
-    r.decl_const("dt", 1, "double", &dt);
+    r.decl_const("cloverleaf/g_small", 1, "double", &g_small);
+    r.decl_const("cloverleaf/g_big", 1, "double", &g_big);
+    r.decl_const("cloverleaf/dtc_safe", 1, "double", &dtc_safe);
+    r.decl_const("cloverleaf/dtu_safe", 1, "double", &dtu_safe);
+    r.decl_const("cloverleaf/dtv_safe", 1, "double", &dtv_safe);
+    r.decl_const("cloverleaf/dtdiv_safe", 1, "double", &dtdiv_safe);
+    r.decl_const("cloverleaf/field", 1, "field_type", &field);
+    r.decl_const("cloverleaf/grid", 1, "grid_type", &grid);
+    r.decl_const("cloverleaf/number_of_states", 1, "int", &number_of_states);
+    r.decl_const("cloverleaf/states", number_of_states, "state_type", states);
+    r.decl_const("cloverleaf/g_circ", 1, "int", &g_circ);
+    r.decl_const("cloverleaf/g_point", 1, "int", &g_point);
+    r.decl_const("cloverleaf/g_rect", 1, "int", &g_rect);
+    r.decl_const("cloverleaf/dt", 1, "double", &dt);
     clover_time = 0.0;
     step = 0;
     dtold = dtinit;

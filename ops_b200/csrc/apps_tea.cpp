@@ -848,13 +848,13 @@ struct Tea {
     step = 0;
     dt = dtinit;
     build_field();
-    r.decl_const("field", 1, "field_type", &field);
-    r.decl_const("grid", 1, "grid_type", &grid);
-    r.decl_const("number_of_states", 1, "int", &number_of_states);
-    r.decl_const("states", number_of_states, "state_type", states);
-    r.decl_const("g_circ", 1, "int", &g_circ);
-    r.decl_const("g_point", 1, "int", &g_point);
-    r.decl_const("g_rect", 1, "int", &g_rect);
+    r.decl_const("tealeaf/field", 1, "field_type", &field);
+    r.decl_const("tealeaf/grid", 1, "grid_type", &grid);
+    r.decl_const("tealeaf/number_of_states", 1, "int", &number_of_states);
+    r.decl_const("tealeaf/states", number_of_states, "state_type", states);
+    r.decl_const("tealeaf/g_circ", 1, "int", &g_circ);
+    r.decl_const("tealeaf/g_point", 1, "int", &g_point);
+    r.decl_const("tealeaf/g_rect", 1, "int", &g_rect);
     initialise_chunk();
     generate();
     set_fields({FIELD_DENSITY, FIELD_ENERGY0, FIELD_ENERGY1});

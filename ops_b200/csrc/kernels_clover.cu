@@ -705,7 +705,7 @@ REG(reset_field_kernel1) REG(reset_field_kernel2) REG(field_summary_kernel)
 // Named constants (ops_decl_const in clover_leaf.cpp:147-160).
 struct ConstReg {
   ConstReg() {
-#define C(name, member) Runtime::register_const(name, &cc, offsetof(Consts, member), sizeof(Consts::member))
+#define C(name, member) Runtime::register_const("cloverleaf/" name, &cc, offsetof(Consts, member), sizeof(Consts::member))
     C("g_small", g_small); C("g_big", g_big); C("dtc_safe", dtc_safe); C("dtu_safe", dtu_safe);
     C("dtv_safe", dtv_safe); C("dtdiv_safe", dtdiv_safe); C("dt", dt); C("field", field); C("grid", grid);
     C("number_of_states", number_of_states); C("g_circ", g_circ); C("g_point", g_point); C("g_rect", g_rect);

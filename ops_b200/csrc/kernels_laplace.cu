@@ -61,9 +61,9 @@ OPSB_REGISTER_LOOP(apply_stencil);
 
 struct ConstReg {
   ConstReg() {
-    Runtime::register_const("imax", &c_lap, offsetof(Consts, imax), sizeof(int));
-    Runtime::register_const("jmax", &c_lap, offsetof(Consts, jmax), sizeof(int));
-    Runtime::register_const("pi", &c_lap, offsetof(Consts, pi), sizeof(double));
+    Runtime::register_const("laplace2d/imax", &c_lap, offsetof(Consts, imax), sizeof(int));
+    Runtime::register_const("laplace2d/jmax", &c_lap, offsetof(Consts, jmax), sizeof(int));
+    Runtime::register_const("laplace2d/pi", &c_lap, offsetof(Consts, pi), sizeof(double));
   }
 };
 static ConstReg const_reg;

@@ -376,7 +376,7 @@ REG(tea_leaf_ppcg_inner1_kernel) REG(tea_leaf_ppcg_inner2_kernel) REG(tea_leaf_p
 
 struct ConstReg {
   ConstReg() {
-#define C(name, member) Runtime::register_const(name, &tc, offsetof(Consts, member), sizeof(Consts::member))
+#define C(name, member) Runtime::register_const("tealeaf/" name, &tc, offsetof(Consts, member), sizeof(Consts::member))
     C("field", field); C("grid", grid); C("number_of_states", number_of_states); C("g_circ", g_circ);
     C("g_point", g_point); C("g_rect", g_rect); C("states", states);
 #undef C

@@ -23,7 +23,7 @@ void cuda_check(cudaError_t e, const char *what) {
 namespace {
 struct Registry {
   std::map<std::string, std::unique_ptr<LoopInfo>> loops;
-  struct ConstSlot { const void *symbol; size_t offset, bytes; };
+  struct ConstSlot { std::string scope; const void *symbol; size_t offset, bytes; };
   std::multimap<std::string, ConstSlot> consts;
   std::vector<ChainRule> chains;
 };
@@ -50,8 +50,17 @@ const LoopInfo *Runtime::find_loop(const std::string &kernel) {
   auto it = m.find(kernel);
   return it == m.end() ? nullptr : it->second.get();
 }
-void Runtime::register_const(const std::string &name, const void *symbol, size_t offset, size_t bytes) {
-  registry().consts.insert({name, {symbol, offset, bytes}});
+// Constant slots are registered as "<app>/<name>" (the app prefix of the
+// kernels that read them) and looked up by <name>.
+static void split_const_name(const std::string &q, std::string &scope, std::string &name) {
+  size_t k = q.find('/');
+  scope = k == std::string::npos ? std::string() : q.substr(0, k);
+  name = k == std::string::npos ? q : q.substr(k + 1);
+}
+void Runtime::register_const(const std::string &qualified, const void *symbol, size_t offset, size_t bytes) {
+  std::string scope, name;
+  split_const_name(qualified, scope, name);
+  registry().consts.insert({name, {scope, symbol, offset, bytes}});
 }
 void Runtime::register_chain(const ChainRule &rule) { registry().chains.push_back(rule); }
 
@@ -235,12 +244,27 @@ int Runtime::decl_reduction(int size, const char *type, const char *name) {
 void Runtime::decl_const(const char *name, int dim, const char *type, const void *data) {
   require(inited_, E_STATE, "ops_decl_const before ops_init");
   execute();  // ops_update_const flushes the queue first (ops_lazy.cpp semantics)
-  auto range = registry().consts.equal_range(name ? name : "");
+  // "<app>/<name>" updates that app's slot only; a bare name updates every
+  // app's slot of that name.
+  std::string scope, key;
+  split_const_name(name ? name : "", scope, key);
+  auto range = registry().consts.equal_range(key);
   int ts = type_size_of(type);
+  // Struct-typed constants (CloverLeaf's field_type, for one) have no scalar
+  // size: the registered slot size is copied, so a bare name must not match
+  // slots of different sizes (2D and 3D field_type, say).
+  if (ts <= 0) {
+    size_t seen = 0;
+    for (auto it = range.first; it != range.second; ++it) {
+      if (!scope.empty() && it->second.scope != scope) continue;
+      require(seen == 0 || seen == it->second.bytes, E_ARG,
+              "constant '" + key + "' has different layouts in several apps: qualify it as <app>/" + key);
+      seen = it->second.bytes;
+    }
+  }
   bool any = false;
   for (auto it = range.first; it != range.second; ++it) {
-    // Struct-typed constants (e.g. CloverLeaf's field_type) have no scalar
-    // type size; the registered slot size is used then.
+    if (!scope.empty() && it->second.scope != scope) continue;
     size_t bytes = ts > 0 ? (size_t)ts * dim : it->second.bytes;
     bytes = std::min(bytes, it->second.bytes);
     OPSB_CUDA(cudaMemcpyToSymbolAsync(it->second.symbol, data, bytes, it->second.offset, cudaMemcpyHostToDevice,
@@ -288,6 +312,7 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         require(dt.plane < (1LL << 31), E_UNSUPPORTED, "dat " + dt.name + " has a plane of 2^31 elements or more");
         require(dt.block == blk, E_ARG, "dat " + dt.name + " is declared on another block");
         require(dt.locked == 0, E_STATE, "dat " + dt.name + " is used in a loop while its raw pointer is held (ops_lib_core.cpp:2321)");
+        check_in_allocation(d, a, dt);
         if (a.acc != ACC_READ) dt.host.clear();
         break;
       }
@@ -327,6 +352,37 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
   qrec_.push_back(std::move(rec));
   loops_enqueued_++;
   if (queue_.size() >= 4096) execute();
+}
+
+// Every point a loop argument can touch, the range widened by its stencil's
+// offsets along the dimensions the stencil walks, must lie in the dat's
+// allocation [base + d_m, base + d_m + size): the reference leaves this to
+// the application, a device kernel here would read or write outside its
+// buffer. Folded (stride 0) dimensions address index 0.
+void Runtime::check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) const {
+  const Stencil &st = stencils_[a.stencil];
+  for (int k = 0; k < d.dim; k++)
+    if (d.range[2 * k + 1] <= d.range[2 * k]) return;  // empty range: nothing is touched
+  for (int k = 0; k < d.dim; k++) {
+    long long lo, hi;
+    if (st.stride[k]) {
+      int omin = 0, omax = 0;
+      for (int p = 0; p < st.points; p++) {
+        int o = st.offs[(size_t)p * st.dims + k];
+        if (p == 0 || o < omin) omin = o;
+        if (p == 0 || o > omax) omax = o;
+      }
+      lo = (long long)d.range[2 * k] + omin;
+      hi = (long long)d.range[2 * k + 1] - 1 + omax;
+    } else {
+      lo = hi = 0;
+    }
+    const long long first = (long long)dt.base[k] + dt.d_m[k], last = first + dt.size[k] - 1;
+    require(lo >= first && hi <= last, E_ARG,
+            "loop " + d.loop->kernel + ": dat " + dt.name + " accessed at [" + std::to_string(lo) + ", " +
+                std::to_string(hi) + "] in dimension " + std::to_string(k) + ", allocated [" +
+                std::to_string(first) + ", " + std::to_string(last) + "]");
+  }
 }
 
 // A loop that only reads some dats and writes others is redundant when an
@@ -416,7 +472,10 @@ void Runtime::build_params(const Desc &d, LoopParams &lp, int *nred_out) {
       case ARG_DAT: {
         const Dat &dt = *dats_[a.dat];
         const Stencil &st = stencils_[a.stencil];
-        v.ptr = a.opt ? dt.origin_ptr() : nullptr;
+        // an optional argument keeps its storage pointer, as ops_arg_dat_opt
+        // does (ops_lib_core.cpp:1107-1113): kernels test their own flags,
+        // which need not agree with the argument's
+        v.ptr = dt.origin_ptr();
         v.sx = st.stride[0] ? 1 : 0;
         v.sy = st.stride[1] ? (int)dt.pitch : 0;
         v.sz = st.stride[2] ? (int)dt.plane : 0;

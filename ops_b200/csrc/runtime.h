@@ -274,6 +274,7 @@ class Runtime {
   unsigned long long ver_counter_ = 0;
   long long loops_skipped_ = 0;
   bool redundant(const Desc &d, LoopRecord &rec);
+  void check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) const;
   long long kernels_launched_ = 0, graphs_launched_ = 0, loops_enqueued_ = 0;
 };
 
@@ -339,6 +340,12 @@ inline void par_loop_named(const char *kernel, const char *name, int block, int 
   const LoopInfo *li = Runtime::find_loop(kernel);
   if (!li) throw Error(E_NOTFOUND, std::string("no registered loop kernel named ") + kernel);
   Runtime::get().par_loop(li, name, block, dim, range, args.begin(), (int)args.size());
+}
+inline void par_loop_named(const char *kernel, const char *name, int block, int dim, const int *range,
+                           const std::vector<Arg> &args) {
+  const LoopInfo *li = Runtime::find_loop(kernel);
+  if (!li) throw Error(E_NOTFOUND, std::string("no registered loop kernel named ") + kernel);
+  Runtime::get().par_loop(li, name, block, dim, range, args.data(), (int)args.size());
 }
 
 // ops_par_loop(kernel, name, block, dim, range, args...) for a functor K.

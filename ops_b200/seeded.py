@@ -64,6 +64,29 @@ def clover_config2_states(x_cells, y_cells, seed=2):
     return [dict(density=0.2, energy=1.0)] + clover_rectangles(x_cells, y_cells, seed)
 
 
+def clover3d_cuboids(x_cells, y_cells, z_cells, seed, n=3, lo=0.0, hi=10.0):
+    """n seeded cuboids with corners on grid planes, density U[0.5, 2] and
+    energy U[1, 3]: cuboid i draws counters 12i..12i+7 of stream `seed`."""
+    states = []
+    cells = (x_cells, y_cells, z_cells)
+    for i in range(n):
+        u = u01(seed, np.arange(12 * i, 12 * i + 8, dtype=np.uint64))
+        box = {}
+        for a, (name, c) in enumerate(zip("xyz", cells)):
+            w = max(1, int(c * (0.1 + 0.3 * u[a])))
+            c0 = int(u[3 + a] * (c - w))
+            d = (hi - lo) / c
+            box[name + "min"] = lo + c0 * d
+            box[name + "max"] = lo + (c0 + w) * d
+        states.append(dict(density=float(0.5 + 1.5 * u[6]), energy=float(1.0 + 2.0 * u[7]), geometry="cuboid", **box))
+    return states
+
+
+def clover3d_states(x_cells, y_cells, z_cells, seed=6):
+    """Background rho=0.2, e=1.0 plus three seeded cuboids."""
+    return [dict(density=0.2, energy=1.0)] + clover3d_cuboids(x_cells, y_cells, z_cells, seed)
+
+
 def normal(seed, k):
     """Standard normal doubles (Box-Muller on counter pairs 2k, 2k+1)."""
     k = np.asarray(k, dtype=np.uint64)

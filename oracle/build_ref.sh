@@ -77,6 +77,11 @@ build_app cloverleaf "$CL" \
   "clover_leaf.cpp initialise_chunk.cpp generate.cpp ideal_gas.cpp update_halo.cpp field_summary.cpp viscosity.cpp calc_dt.cpp PdV.cpp revert.cpp accelerate.cpp flux_calc.cpp advec_cell.cpp advec_mom.cpp reset_field.cpp" \
   "start.cpp time_step.cpp build_field.cpp read_input.cpp initialise.cpp advection.cpp" "" &
 
+CL3=$REF/apps/c/CloverLeaf_3D
+build_app cloverleaf3d "$CL3" \
+  "clover_leaf.cpp initialise_chunk.cpp generate.cpp ideal_gas.cpp update_halo.cpp field_summary.cpp viscosity.cpp calc_dt.cpp PdV.cpp revert.cpp accelerate.cpp flux_calc.cpp advec_cell.cpp advec_mom.cpp reset_field.cpp" \
+  "start.cpp time_step.cpp build_field.cpp read_input.cpp initialise.cpp advection.cpp" "" &
+
 # halo transfer cases: a driver of our own on the reference's public API,
 # compiled against libops_seq.a with the reference's template loop path
 # (ops_seq_v2.h, no translation)

@@ -111,6 +111,62 @@ if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "clover":
     clover()
 
 
+# CloverLeaf 3D decks: (name, x, y, z cells, end_step, cuboid seed,
+# max_timestep); uneven extents so that an axis mix-up shows, and a large
+# max_timestep in the second so that the CFL limit sets dt
+CLOVER3D_CASES = [
+    ("clover3d_24x20x16_s40", 24, 20, 16, 40, 6, 0.04),
+    ("clover3d_18x14x22_s30", 18, 14, 22, 30, 9, 1.0),
+]
+DUMP3D_FIELDS = ["density0", "energy0", "pressure", "xvel0", "yvel0", "zvel0"]
+
+
+def run_reference_clover3d(deck_text, dump=False, threads=1, timeout=600):
+    """Runs the reference CloverLeaf 3D build on a deck; returns (summaries, dts, dumps)."""
+    exe = oracle.reference_binary("cloverleaf3d")
+    if exe is None:
+        raise SystemExit("oracle/_ref/bin/cloverleaf3d missing: run oracle/build_ref.sh")
+    with tempfile.TemporaryDirectory() as td:
+        with open(os.path.join(td, "clover.in"), "w") as f:
+            f.write(deck_text)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        if dump:
+            env["ORACLE_DUMP_DIR"] = td
+        r = subprocess.run([exe], cwd=td, capture_output=True, text=True, timeout=timeout, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
+        out = open(os.path.join(td, "clover.out")).read()
+        summ = [[float(x) for x in l.split()[1:9]] for l in out.splitlines() if l.strip().startswith("step:")]
+        dts = [float(l.split()[7]) for l in r.stdout.splitlines() if l.strip().startswith("Step ")]
+        dumps = {}
+        if dump:
+            for name in DUMP3D_FIELDS:
+                meta = open(os.path.join(td, name + ".meta")).read().split("\n")
+                size = [int(x) for x in meta[1].split()[1:]]
+                xpad = int(meta[4].split()[1])
+                a = np.fromfile(os.path.join(td, name + ".bin"), dtype=np.float64).reshape(size[2], size[1], size[0])
+                dumps[name] = a[:, :, :size[0] - xpad]
+    # columns: step, vol, mass, density, pressure, ie, ke, total
+    return np.array(summ), np.array(dts), dumps
+
+
+def clover3d():
+    from ops_b200 import apps, seeded
+    for name, nx, ny, nz, steps, seed, max_dt in CLOVER3D_CASES:
+        deck = apps.clover3d_deck(x_cells=nx, y_cells=ny, z_cells=nz, xmax=10.0, ymax=10.0, zmax=10.0,
+                                  initial_timestep=0.04, timestep_rise=1.5, max_timestep=max_dt, end_step=steps,
+                                  summary_frequency=1, states=seeded.clover3d_states(nx, ny, nz, seed))
+        text = apps.clover3d_deck_text(deck)
+        summ, dts, dumps = run_reference_clover3d(text, dump=True)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, deck=text, summaries=summ, dts=dts, **{"f_" + k: v for k, v in dumps.items()})
+        print("wrote", path, summ.shape, len(dts), os.path.getsize(path))
+
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "clover3d":
+    clover3d()
+
+
 # TeaLeaf decks: (name, deck keywords)
 TEA_CASES = [
     ("tea_kat_jacobi", dict(x_cells=10, y_cells=10, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=10,
