@@ -7,6 +7,8 @@ configurations with synthetic seeded inputs:
            (CloverLeaf) on 3840x3840 cells, FP64, gamma 1.4; background
            rho=0.2, e=1.0 plus 4 seeded rectangles; a step is one hydro
            cycle with CFL dt and a field summary read back every step.
+  clover3d the 3D CloverLeaf hydro on 256^3 cells, FP64; background rho=0.2,
+           e=1.0 plus 3 seeded cuboids; a step is one hydro cycle.
   laplace  2D Laplace Jacobi, single block 4096x4096 FP64, 5-point stencil,
            seeded U[0,1) Dirichlet ring, interior 0; a step is one iteration
            (apply_stencil + max|delta| reduction read back + copy).
@@ -389,6 +391,132 @@ def reference_clover(args, world, rank):
         "config": {"workload": "cloverleaf2d_3840x3840_fp64", "grid": [CL_N, CL_N]},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
                          "sample": f"{steps} steps of the reference OpenMP build at {CL_N}^2 on {threads} threads"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ---------------------------------------------------------------------------
+# CloverLeaf 3D
+# ---------------------------------------------------------------------------
+CL3_N = 256
+
+
+def clover3d_deck(steps, n=CL3_N):
+    from ops_b200 import apps, seeded
+    return apps.clover3d_deck(x_cells=n, y_cells=n, z_cells=n, xmax=10.0, ymax=10.0, zmax=10.0,
+                              initial_timestep=0.04, timestep_rise=1.5, max_timestep=0.04, end_step=steps,
+                              summary_frequency=1, states=seeded.clover3d_states(n, n, n, 6))
+
+
+def cpu_reference_clover3d(steps, threads, n=CL3_N):
+    import oracle
+    from ops_b200 import apps
+    exe = oracle.reference_binary("cloverleaf3d")
+    if exe is None:
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+    with tempfile.TemporaryDirectory() as td:
+        with open(os.path.join(td, "clover.in"), "w") as f:
+            f.write(apps.clover3d_deck_text(clover3d_deck(steps, n)))
+        r = subprocess.run([exe], cwd=td, capture_output=True, text=True, env=env, timeout=900, check=True)
+    secs = [float(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Total Wall time")][-1]
+    return n ** 3 * steps / secs, secs
+
+
+def bench_clover3d(args, world, rank, local, pg):
+    from ops_b200 import apps
+    from ops_b200 import ops as O
+
+    peaks, peak_kind = load_peaks()
+    O.ops_init(local, 0)
+    N = args.grid or CL3_N
+    cells = N ** 3
+    K, W = args.steps, args.warmup
+
+    barrier(pg, local)
+    O.reset_counters()
+    with ClockSampler(local) as cs:
+        summ, secs = apps.cloverleaf3d(clover3d_deck(W + K, N), warmup_steps=W)
+    clocks = cs.summary()
+    barrier(pg, local)
+    secs = max_over_ranks(pg, secs, local)
+
+    kp = min(K, 10)
+    O.set_kernel_timing(1)
+    O.clear_kernel_timing()
+    apps.cloverleaf3d(clover3d_deck(kp, N))
+    stats = O.kernel_stats()
+    O.set_kernel_timing(0)
+    launches_per_step = sum(v[0] for v in stats.values()) / kp
+    dom, (n, ms, by) = max(stats.items(), key=lambda kv: kv[1][1])
+    achieved = (by / n) / (ms / n * 1e-3) / 1e9
+    tot_ms = sum(v[1] for v in stats.values())
+    tot_by = sum(v[2] for v in stats.values())
+
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    apps.cloverleaf3d(clover3d_deck(K, N))
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(pg, t1 - t0, local)
+
+    line = {
+        "metric": "cell-updates/s",
+        "value": world * cells * K / secs,
+        "unit": "cell-updates/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": secs * 1e3 / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (background rho=0.2 e=1.0 + 3 SplitMix64-seeded cuboids, seed 6)",
+        "config": {"workload": f"cloverleaf3d_{N}^3_fp64", "grid": [N, N, N], "gamma": 1.4,
+                   "cell_update": "one cell advanced one hydro timestep",
+                   "step": "timestep + PdV + accelerate + flux_calc + 3 advection sweeps + reset_field"
+                           " + field_summary (5 FP64 sums read back)",
+                   "l2": "inputs larger than L2 (about 40 fields of 140 MB)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": dom,
+                     "alg_bytes_per_launch": by / n, "avg_launch_ms": ms / n, "peak_source": f"{peak_kind} hbm_gbs",
+                     "step_effective_gbs": tot_by / (tot_ms * 1e-3) / 1e9,
+                     "step_alg_bytes_per_cell": tot_by / kp / cells},
+        "e2e": {"value": world * cells * K / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": 0.0,
+                "d2h_bytes_per_step": 6 * 8 + 3 * 8,
+                "note": "one C-ABI call: deck in, device set-up (generate), K cycles each reading dt and the"
+                        " 5-value field summary back"},
+        "gpu_launches": int(round(launches_per_step * K)),
+        "clocks": clocks,
+        "final_summary": {"vol": summ[-1, 2], "mass": summ[-1, 3], "ie": summ[-1, 4], "ke": summ[-1, 5],
+                          "press": summ[-1, 6]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        base = cpu_reference_clover3d(args.cpu_clover_steps, threads, N)
+        if base:
+            line["cpu_baseline"] = {"value": base[0], "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                                    "sample": f"reference CloverLeaf 3D OpenMP build, {N}^3, {args.cpu_clover_steps}"
+                                              f" steps (hydro loop wall time {base[1]:.2f} s)"}
+    return line
+
+
+def reference_clover3d(args, world, rank):
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, args.cpu_clover_steps))
+    N = args.grid or CL3_N
+    base = cpu_reference_clover3d(steps, threads, N)
+    if base is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/bin/cloverleaf3d was not built"}
+    v, secs = base
+    return {
+        "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": steps, "warmup": 0, "ms_per_step": secs * 1e3 / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (background rho=0.2 e=1.0 + 3 SplitMix64-seeded cuboids, seed 6)",
+        "config": {"workload": f"cloverleaf3d_{N}^3_fp64", "grid": [N, N, N]},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                         "sample": f"{steps} steps of the reference OpenMP build at {N}^3 on {threads} threads"},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -825,6 +953,7 @@ def bench_learned(args, world, rank, local, pg):
 
 
 WORKLOADS = {"laplace": (bench_laplace, reference_laplace), "clover": (bench_clover, reference_clover),
+             "clover3d": (bench_clover3d, reference_clover3d),
              "adi": (bench_adi, reference_adi), "tea": (bench_tea, reference_tea),
              "learned": (bench_learned, reference_tea)}
 
@@ -848,7 +977,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"laplace": 200, "clover": 200, "adi": 50, "tea": 3, "learned": 2}.get(args.workload, 20)
+        args.steps = {"laplace": 200, "clover": 200, "clover3d": 100, "adi": 50, "tea": 3,
+                      "learned": 2}.get(args.workload, 20)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_setup(args)

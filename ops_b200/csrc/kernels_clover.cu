@@ -19,6 +19,9 @@ using D = ACC2<double>;
 using I = ACC2<int>;
 
 #define CL_LOOP(NAME) static constexpr const char *kname = "cloverleaf/" #NAME
+// Resident CTAs per SM (register budget) where the default of 8 (32
+// registers) spills more than the extra occupancy gains; measured per
+// kernel on the 3840^2 deck.
 
 // ---- initialise_chunk_kernel.h -------------------------------------------
 struct initialise_chunk_kernel_xx {  // :30
@@ -218,6 +221,7 @@ UH_PAIR(update_halo_kernel4_minus_2_b, 0, -2, 1, FIELD_VOL_FLUX_Y, FIELD_MASS_FL
 // ---- viscosity_kernel.h:5 ----------------------------------------------------
 struct viscosity_kernel {
   CL_LOOP(viscosity_kernel);
+  static constexpr int min_blocks = 6;
   __device__ void operator()(const D &xvel0, const D &yvel0, const D &celldx, const D &celldy, const D &pressure,
                              const D &density0, D &viscosity) const {
     double ugrad = (xvel0(1, 0) + xvel0(1, 1)) - (xvel0(0, 0) + xvel0(0, 1));
@@ -312,6 +316,7 @@ struct calc_dt_kernel_print {  // :74
 // ---- PdV_kernel.h ------------------------------------------------------------
 struct PdV_kernel_predict {  // :7
   CL_LOOP(PdV_kernel_predict);
+  static constexpr int min_blocks = 6;
   __device__ void operator()(const D &xarea, const D &xvel0, const D &yarea, const D &yvel0, D &volume_change,
                              const D &volume, const D &pressure, const D &density0, D &density1,
                              const D &viscosity, const D &energy0, D &energy1) const {
@@ -330,6 +335,7 @@ struct PdV_kernel_predict {  // :7
 };
 struct PdV_kernel_nopredict {  // :45
   CL_LOOP(PdV_kernel_nopredict);
+  static constexpr int min_blocks = 6;
   __device__ void operator()(const D &xarea, const D &xvel0, const D &xvel1, const D &yarea, const D &yvel0,
                              const D &yvel1, D &volume_change, const D &volume, const D &pressure,
                              const D &density0, D &density1, const D &viscosity, const D &energy0,
@@ -360,6 +366,7 @@ struct revert_kernel {
 // ---- accelerate_kernel.h:8 ---------------------------------------------------
 struct accelerate_kernel {
   CL_LOOP(accelerate_kernel);
+  static constexpr int min_blocks = 4;
   __device__ void operator()(const D &density0, const D &volume, D &stepbymass, const D &xvel0, D &xvel1,
                              const D &xarea, const D &pressure, const D &yvel0, D &yvel1, const D &yarea,
                              const D &viscosity) const {
@@ -470,6 +477,7 @@ struct advec_cell_kernel3_xdir {  // :28
 };
 struct advec_cell_kernel4_xdir {  // :106
   CL_LOOP(advec_cell_kernel4_xdir);
+  static constexpr int min_blocks = 4;
   __device__ void operator()(D &density1, D &energy1, const D &mass_flux_x, const D &vol_flux_x, const D &pre_vol,
                              const D &post_vol, D &pre_mass, D &post_mass, D &advec_vol, D &post_ener,
                              const D &ener_flux) const {
@@ -508,6 +516,7 @@ struct advec_cell_kernel3_ydir {  // :142
 };
 struct advec_cell_kernel4_ydir {  // :205
   CL_LOOP(advec_cell_kernel4_ydir);
+  static constexpr int min_blocks = 4;
   __device__ void operator()(D &density1, D &energy1, const D &mass_flux_y, const D &vol_flux_y, const D &pre_vol,
                              const D &post_vol, D &pre_mass, D &post_mass, D &advec_vol, D &post_ener,
                              const D &ener_flux) const {
@@ -654,6 +663,7 @@ struct reset_field_kernel2 {  // :13
 // ---- field_summary_kernel.h:4 -------------------------------------------------
 struct field_summary_kernel {
   CL_LOOP(field_summary_kernel);
+  static constexpr int min_blocks = 6;
   __device__ void operator()(const D &volume, const D &density0, const D &energy0, const D &pressure, const D &xvel0,
                              const D &yvel0, RED<double> &vol, RED<double> &mass, RED<double> &ie, RED<double> &ke,
                              RED<double> &press) const {

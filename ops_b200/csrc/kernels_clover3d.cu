@@ -21,6 +21,13 @@ using D = ACC3<double>;
 using I = ACC3<int>;
 
 #define C3_LOOP(NAME) static constexpr const char *kname = "cloverleaf3d/" #NAME
+// Kernels with many live values (the 8-point velocity gathers, the limiter
+// arithmetic) get a larger register budget: C3_HEAVY_MINB resident CTAs of
+// 256 threads per SM instead of the default 4.
+#ifndef C3_HEAVY_MINB
+#define C3_HEAVY_MINB 4
+#endif
+#define C3_HEAVY static constexpr int min_blocks = C3_HEAVY_MINB
 
 // Offset `o` along axis AX (0 = x, 1 = y, 2 = z).
 template <int AX, class A>
@@ -333,6 +340,7 @@ UH2(update_halo_kernel5_minus_2_front, 0, 0, -2, 1, FZ)
 // ---- viscosity_kernel.h:7 --------------------------------------------------------
 struct viscosity_kernel {
   C3_LOOP(viscosity_kernel);
+  C3_HEAVY;
   __device__ void operator()(const D &xvel0, const D &yvel0, const D &celldx, const D &celldy, const D &pressure,
                              const D &density0, D &viscosity, const D &zvel0, const D &celldz, const D &xarea,
                              const D &yarea, const D &zarea) const {
@@ -392,6 +400,7 @@ struct viscosity_kernel {
 // ---- calc_dt_kernel.h -------------------------------------------------------------
 struct calc_dt_kernel {  // :7
   C3_LOOP(calc_dt_kernel);
+  C3_HEAVY;
   __device__ void operator()(const D &celldx, const D &celldy, const D &soundspeed, const D &viscosity,
                              const D &density0, const D &xvel0, const D &xarea, const D &volume, const D &yvel0,
                              const D &yarea, D &dt_min, const D &celldz, const D &zvel0, const D &zarea) const {
@@ -471,6 +480,7 @@ struct calc_dt_kernel_print {  // :61
 // the timestep, :7) and the corrector (old and new velocities, :70).
 struct PdV_kernel_predict {
   C3_LOOP(PdV_kernel_predict);
+  C3_HEAVY;
   __device__ void operator()(const D &xarea, const D &xvel0, const D &yarea, const D &yvel0, D &volume_change,
                              const D &volume, const D &pressure, const D &density0, D &density1,
                              const D &viscosity, const D &energy0, D &energy1, const D &zarea,
@@ -507,6 +517,7 @@ struct PdV_kernel_predict {
 };
 struct PdV_kernel_nopredict {
   C3_LOOP(PdV_kernel_nopredict);
+  C3_HEAVY;
   __device__ void operator()(const D &xarea, const D &xvel0, const D &xvel1, const D &yarea, const D &yvel0,
                              const D &yvel1, D &volume_change, const D &volume, const D &pressure,
                              const D &density0, D &density1, const D &viscosity, const D &energy0, D &energy1,
@@ -554,6 +565,7 @@ struct revert_kernel {
 // ---- accelerate_kernel.h:7 --------------------------------------------------------------
 struct accelerate_kernel {
   C3_LOOP(accelerate_kernel);
+  C3_HEAVY;
   __device__ void operator()(const D &density0, const D &volume, D &stepbymass, const D &xvel0, D &xvel1,
                              const D &xarea, const D &pressure, const D &yvel0, D &yvel1, const D &yarea,
                              const D &viscosity, const D &zvel0, D &zvel1, const D &zarea) const {
@@ -727,6 +739,7 @@ __device__ __forceinline__ void advec_cell_flux(const D &vol_flux, const D &pre_
 }
 struct advec_cell_kernel3_xdir {
   C3_LOOP(advec_cell_kernel3_xdir);
+  C3_HEAVY;
   __device__ void operator()(const D &vol_flux_x, const D &pre_vol, const I &xx, const D &vertexdx,
                              const D &density1, const D &energy1, D &mass_flux_x, D &ener_flux) const {
     advec_cell_flux<0>(vol_flux_x, pre_vol, xx, vertexdx, density1, energy1, mass_flux_x, ener_flux, c3.field.x_max);
@@ -734,6 +747,7 @@ struct advec_cell_kernel3_xdir {
 };
 struct advec_cell_kernel3_ydir {
   C3_LOOP(advec_cell_kernel3_ydir);
+  C3_HEAVY;
   __device__ void operator()(const D &vol_flux_y, const D &pre_vol, const I &yy, const D &vertexdy,
                              const D &density1, const D &energy1, D &mass_flux_y, D &ener_flux) const {
     advec_cell_flux<1>(vol_flux_y, pre_vol, yy, vertexdy, density1, energy1, mass_flux_y, ener_flux, c3.field.y_max);
@@ -741,6 +755,7 @@ struct advec_cell_kernel3_ydir {
 };
 struct advec_cell_kernel3_zdir {
   C3_LOOP(advec_cell_kernel3_zdir);
+  C3_HEAVY;
   __device__ void operator()(const D &vol_flux_z, const D &pre_vol, const I &zz, const D &vertexdz,
                              const D &density1, const D &energy1, D &mass_flux_z, D &ener_flux) const {
     advec_cell_flux<2>(vol_flux_z, pre_vol, zz, vertexdz, density1, energy1, mass_flux_z, ener_flux, c3.field.z_max);
@@ -953,6 +968,7 @@ struct reset_field_kernel2 {  // :13
 // ---- field_summary_kernel.h:4 -------------------------------------------------------------
 struct field_summary_kernel {
   C3_LOOP(field_summary_kernel);
+  C3_HEAVY;
   __device__ void operator()(const D &volume, const D &density0, const D &energy0, const D &pressure, const D &xvel0,
                              const D &yvel0, const D &zvel0, RED<double> &vol, RED<double> &mass, RED<double> &ie,
                              RED<double> &ke, RED<double> &press) const {

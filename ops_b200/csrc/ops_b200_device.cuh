@@ -287,12 +287,27 @@ struct Exec<K, void (C::*)(P...) const> {
   }
 };
 
-// Resident 256-thread CTAs per SM the register allocation must allow: 4
-// (at most 64 registers a thread) unless a kernel states `min_blocks`. These
-// loops are latency-bound streams, so occupancy is worth a few spills.
-template <class K, class = void> struct LoopMinBlocks { static constexpr int value = 4; };
+// Resident 256-thread CTAs per SM the register allocation must allow: 8
+// (a full SM, at most 32 registers a thread) unless a kernel states
+// `min_blocks`. The loops are latency-bound streams whose loads cannot be
+// hoisted over the previous point's stores, so the bytes in flight per SM
+// grow with the resident threads: occupancy is worth a few spills.
+#ifndef OPSB_MIN_BLOCKS
+#define OPSB_MIN_BLOCKS 8
+#endif
+template <class K, class = void> struct LoopMinBlocks { static constexpr int value = OPSB_MIN_BLOCKS; };
 template <class K> struct LoopMinBlocks<K, std::void_t<decltype(K::min_blocks)>> {
   static constexpr int value = K::min_blocks;
+};
+
+// Rows a thread keeps in flight in the 2D row loop (memory-level
+// parallelism of the streaming loops); a kernel may state `row_unroll`.
+#ifndef OPSB_ROW_UNROLL
+#define OPSB_ROW_UNROLL 2
+#endif
+template <class K, class = void> struct LoopRowUnroll { static constexpr int value = OPSB_ROW_UNROLL; };
+template <class K> struct LoopRowUnroll<K, std::void_t<decltype(K::row_unroll)>> {
+  static constexpr int value = K::row_unroll;
 };
 
 // The generic loop kernel. blockDim = (BX, BY); blocks tile x exactly and
@@ -309,7 +324,8 @@ __global__ void __launch_bounds__(256, LoopMinBlocks<K>::value) exec_loop(const 
   const long long nrows = (long long)ny * nz;
   if (x < lp.end[0]) {
     if (nz == 1) {
-#pragma unroll 2
+      constexpr int kUnroll = LoopRowUnroll<K>::value;
+#pragma unroll (kUnroll)
       for (int y = lp.start[1] + blockIdx.y * blockDim.y + threadIdx.y; y < lp.end[1]; y += gridDim.y * blockDim.y)
         E::call(k, t, lp, x, y, lp.start[2], typename E::Seq{});
     } else {
