@@ -1,0 +1,225 @@
+// Batched execution of boundary-copy loops.
+//
+// The reference apps refresh their reflective boundaries with dozens of thin
+// loops per call (CloverLeaf 2D update_halo.cpp queues up to 40, the 3D app
+// up to 84), each copying (or negating) a strip of halo cells from a mirror
+// point inside the domain. One launch each leaves the GPU idle between
+// launches of a few microseconds of work. A run of such loops in the queue
+// (kernels registered with a CopyLoopSpec) is executed instead as a few
+// launches of one copy kernel over a list of strips: every (loop, field)
+// pair becomes a strip; a strip goes into the first batch after every
+// earlier strip it conflicts with (same dat, and its write box meets the
+// other's write or read box, or its read box meets the other's write box),
+// so batches hold only independent strips and keep the queue's order where
+// it matters. Each strip checks its field flag on the device (the flags are
+// this flush's staged globals), so the batches depend only on the queue's
+// structure and stay valid when a captured graph replays them with other
+// flags. The values moved are the same doubles the loops would move: the
+// results are identical.
+#include <unordered_map>
+
+#include "runtime.h"
+
+namespace opsb {
+
+namespace {
+std::map<std::string, CopyLoopSpec> &copy_specs() {
+  static std::map<std::string, CopyLoopSpec> m;
+  return m;
+}
+std::unordered_map<const LoopInfo *, const CopyLoopSpec *> &copy_spec_cache() {
+  static std::unordered_map<const LoopInfo *, const CopyLoopSpec *> m;
+  return m;
+}
+
+struct CopyStrip {
+  double *p;          // logical origin of the dat
+  const int *flag;    // device flag word, or nullptr (always copy)
+  long long src;      // element offset of the mirror point
+  long long pitch, plane;
+  int x0, y0, z0, nx, ny, nz;
+  long long first;    // first cell number of this strip in its batch
+  int neg, pad;
+};
+
+__global__ void copy_batch_kernel(const CopyStrip *__restrict__ s, int n, long long total) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+       c += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n - 1;  // last strip with first <= c
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (s[mid].first <= c) lo = mid;
+      else hi = mid - 1;
+    }
+    const CopyStrip &e = s[lo];
+    if (e.flag && *e.flag != 1) continue;
+    long long k = c - e.first;
+    int x = (int)(k % e.nx);
+    long long r = k / e.nx;
+    int y = (int)(r % e.ny);
+    int z = (int)(r / e.ny);
+    double *q = e.p + (long long)(e.x0 + x) + (long long)(e.y0 + y) * e.pitch + (long long)(e.z0 + z) * e.plane;
+    const double v = q[e.src];
+    *q = e.neg ? -v : v;
+  }
+}
+
+struct Box {
+  int lo[3], hi[3];  // inclusive
+};
+bool meet(const Box &a, const Box &b) {
+  for (int k = 0; k < 3; k++)
+    if (a.hi[k] < b.lo[k] || b.hi[k] < a.lo[k]) return false;
+  return true;
+}
+
+struct Planned {
+  std::vector<std::vector<CopyStrip>> batches;
+  long long cells = 0;
+};
+
+// Strips of queue items [i, i + n) grouped into batches (see the file comment).
+bool plan(const std::vector<Desc> &q, size_t i, int n, Planned &out) {
+  Runtime &rt = Runtime::get();
+  struct Item { CopyStrip s; Box w, r; const char *data; int batch; };
+  std::vector<Item> items;
+  for (int j = 0; j < n; j++) {
+    const Desc &d = q[i + j];
+    const CopyLoopSpec *sp = find_copy_loop(d.loop);
+    if (!sp) return false;
+    const int *flags = nullptr;
+    if (sp->flags_arg >= 0) flags = reinterpret_cast<const int *>(rt.gbl_device() + d.gbl_off[sp->flags_arg]);
+    for (int f = 0; f < sp->nfields; f++) {
+      const Arg &a = d.args[sp->arg[f]];
+      Dat &dt = rt.dat(a.dat);
+      if (dt.elem_size != 8) return false;
+      Item it;
+      CopyStrip &s = it.s;
+      s.p = reinterpret_cast<double *>(dt.origin_ptr());
+      s.flag = flags ? flags + sp->flag[f] : nullptr;
+      s.pitch = dt.pitch;
+      s.plane = dt.plane;
+      s.src = sp->off[0] + sp->off[1] * dt.pitch + sp->off[2] * dt.plane;
+      s.x0 = d.range[0]; s.y0 = d.range[2]; s.z0 = d.range[4];
+      s.nx = d.range[1] - d.range[0]; s.ny = d.range[3] - d.range[2]; s.nz = d.range[5] - d.range[4];
+      s.neg = sp->neg;
+      s.pad = 0;
+      if (s.nx <= 0 || s.ny <= 0 || s.nz <= 0) continue;
+      for (int k = 0; k < 3; k++) {
+        it.w.lo[k] = d.range[2 * k];
+        it.w.hi[k] = d.range[2 * k + 1] - 1;
+        it.r.lo[k] = it.w.lo[k] + sp->off[k];
+        it.r.hi[k] = it.w.hi[k] + sp->off[k];
+      }
+      if (meet(it.w, it.r)) return false;  // a strip reading its own cells: keep the loop
+      it.data = dt.data_d;
+      it.batch = 0;
+      for (const Item &e : items)
+        if (e.data == it.data && e.batch >= it.batch && (meet(it.w, e.w) || meet(it.w, e.r) || meet(it.r, e.w)))
+          it.batch = e.batch + 1;
+      items.push_back(it);
+    }
+  }
+  int nb = 0;
+  for (const Item &e : items) nb = std::max(nb, e.batch + 1);
+  out.batches.assign(nb, {});
+  out.cells = 0;
+  for (Item &e : items) {
+    std::vector<CopyStrip> &b = out.batches[e.batch];
+    long long first = b.empty() ? 0 : b.back().first + (long long)b.back().nx * b.back().ny * b.back().nz;
+    e.s.first = first;
+    b.push_back(e.s);
+    out.cells += (long long)e.s.nx * e.s.ny * e.s.nz;
+  }
+  return true;
+}
+
+// Device copies of strip lists, kept by content: a captured graph keeps
+// pointing at them, so they are never rewritten or freed.
+std::unordered_map<uint64_t, CopyStrip *> &strip_cache() {
+  static std::unordered_map<uint64_t, CopyStrip *> m;
+  return m;
+}
+uint64_t hash_bytes(const void *p, size_t n) {
+  const unsigned char *c = static_cast<const unsigned char *>(p);
+  uint64_t h = 0xCBF29CE484222325ULL;
+  for (size_t k = 0; k < n; k++) h = (h ^ c[k]) * 0x100000001B3ULL;
+  return h ^ n;
+}
+CopyStrip *device_strips(const std::vector<CopyStrip> &b, bool may_upload) {
+  const size_t bytes = b.size() * sizeof(CopyStrip);
+  const uint64_t h = hash_bytes(b.data(), bytes);
+  auto it = strip_cache().find(h);
+  if (it != strip_cache().end()) return it->second;
+  if (!may_upload) return nullptr;
+  CopyStrip *d = nullptr;
+  OPSB_CUDA(cudaMalloc(&d, bytes));
+  // ordered before the batch's launch on the same stream; the pageable
+  // source is staged before the call returns
+  OPSB_CUDA(cudaMemcpyAsync(d, b.data(), bytes, cudaMemcpyHostToDevice, Runtime::get().stream()));
+  strip_cache()[h] = d;
+  return d;
+}
+
+bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  OPSB_CUDA(cudaStreamIsCapturing(s, &st));
+  return st != cudaStreamCaptureStatusNone;
+}
+
+int match_copy_run(const std::vector<Desc> &q, size_t i) {
+  size_t j = i;
+  while (j < q.size() && !q[j].loop->internal && find_copy_loop(q[j].loop)) j++;
+  int n = (int)(j - i);
+  if (n < 2) return 0;
+  Planned pl;
+  if (!plan(q, i, n, pl)) return 0;
+  // While a graph is being captured nothing may be uploaded; the strips of
+  // this structure were uploaded when it ran uncaptured the first time.
+  if (capturing(Runtime::get().stream()))
+    for (const auto &b : pl.batches)
+      if (!device_strips(b, false)) return 0;
+  return n;
+}
+
+void launch_copy_run(const std::vector<Desc> &q, size_t i, int n, cudaStream_t s) {
+  Planned pl;
+  if (!plan(q, i, n, pl)) throw Error(E_STATE, "copy batch: plan failed after a match");
+  const bool cap = capturing(s);
+  for (const auto &b : pl.batches) {
+    if (b.empty()) continue;
+    CopyStrip *d = device_strips(b, !cap);
+    if (!d) throw Error(E_STATE, "copy batch: strips missing during capture");
+    long long total = b.back().first + (long long)b.back().nx * b.back().ny * b.back().nz;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
+    copy_batch_kernel<<<blocks, 256, 0, s>>>(d, (int)b.size(), total);
+    OPSB_CUDA(cudaGetLastError());
+    Runtime::get().count_kernels(1);
+  }
+}
+
+struct CopyChainReg {
+  CopyChainReg() {
+    ChainRule r;
+    r.name = "runtime/copy_batch";
+    r.match = match_copy_run;
+    r.launch = launch_copy_run;
+    Runtime::register_chain(r);
+  }
+};
+CopyChainReg copy_chain_reg;
+}  // namespace
+
+void register_copy_loop(const std::string &kernel, const CopyLoopSpec &spec) { copy_specs()[kernel] = spec; }
+
+const CopyLoopSpec *find_copy_loop(const LoopInfo *loop) {
+  auto &c = copy_spec_cache();
+  auto it = c.find(loop);
+  if (it != c.end()) return it->second;
+  auto f = copy_specs().find(loop->kernel);
+  const CopyLoopSpec *sp = f == copy_specs().end() ? nullptr : &f->second;
+  c[loop] = sp;
+  return sp;
+}
+
+}  // namespace opsb

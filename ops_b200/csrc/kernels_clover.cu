@@ -147,6 +147,14 @@ struct ideal_gas_kernel {
 // copy from (OX, OY) when their flag is set.
 template <int OX, int OY>
 struct uh_cells {
+  static CopyLoopSpec copy_spec() {
+    CopyLoopSpec c;
+    c.nfields = 7;
+    for (int f = 0; f < 7; f++) c.arg[f] = f, c.flag[f] = FIELD_DENSITY0 + f;
+    c.flags_arg = 7;
+    c.off[0] = OX; c.off[1] = OY;
+    return c;
+  }
   __device__ void operator()(D &density0, D &density1, D &energy0, D &energy1, D &pressure, D &viscosity,
                              D &soundspeed, const int *fields) const {
     if (fields[FIELD_DENSITY0] == 1) density0(0, 0) = density0(OX, OY);
@@ -162,16 +170,27 @@ struct uh_cells {
 // from (OX, OY) when flag F0 / F1 is set.
 template <int OX, int OY, int NEG, int F0, int F1>
 struct uh_pair {
+  static CopyLoopSpec copy_spec() {
+    CopyLoopSpec c;
+    c.nfields = 2;
+    c.arg[0] = 0; c.arg[1] = 1; c.flag[0] = F0; c.flag[1] = F1;
+    c.flags_arg = 2;
+    c.neg = NEG;
+    c.off[0] = OX; c.off[1] = OY;
+    return c;
+  }
   __device__ void operator()(D &a, D &b, const int *fields) const {
     if (fields[F0] == 1) a(0, 0) = NEG ? -a(OX, OY) : a(OX, OY);
     if (fields[F1] == 1) b(0, 0) = NEG ? -b(OX, OY) : b(OX, OY);
   }
 };
 
-#define UH_CELLS(NAME, OX, OY) \
-  struct NAME : uh_cells<OX, OY> { CL_LOOP(NAME); };
-#define UH_PAIR(NAME, OX, OY, NEG, F0, F1) \
-  struct NAME : uh_pair<OX, OY, NEG, F0, F1> { CL_LOOP(NAME); };
+#define UH_CELLS(NAME, OX, OY)                     \
+  struct NAME : uh_cells<OX, OY> { CL_LOOP(NAME); }; \
+  OPSB_REGISTER_COPY_LOOP(NAME);
+#define UH_PAIR(NAME, OX, OY, NEG, F0, F1)                     \
+  struct NAME : uh_pair<OX, OY, NEG, F0, F1> { CL_LOOP(NAME); }; \
+  OPSB_REGISTER_COPY_LOOP(NAME);
 
 UH_CELLS(update_halo_kernel1_b2, 0, 3)
 UH_CELLS(update_halo_kernel1_b1, 0, 1)

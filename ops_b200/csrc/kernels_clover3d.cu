@@ -216,6 +216,14 @@ struct ideal_gas_kernel {
 // The seven cell-centred fields, copied from the mirror point (OX, OY, OZ).
 template <int OX, int OY, int OZ>
 struct uh1 {
+  static CopyLoopSpec copy_spec() {
+    CopyLoopSpec c;
+    c.nfields = 7;
+    for (int f = 0; f < 7; f++) c.arg[f] = f, c.flag[f] = FIELD_DENSITY0 + f;
+    c.flags_arg = 7;
+    c.off[0] = OX; c.off[1] = OY; c.off[2] = OZ;
+    return c;
+  }
   __device__ void operator()(D &density0, D &density1, D &energy0, D &energy1, D &pressure, D &viscosity,
                              D &soundspeed, const int *fields) const {
     if (fields[FIELD_DENSITY0] == 1) density0(0, 0, 0) = density0(OX, OY, OZ);
@@ -231,15 +239,26 @@ struct uh1 {
 // (NEG = 1, the velocity or flux normal to the face) from (OX, OY, OZ).
 template <int OX, int OY, int OZ, int NEG, int F0, int F1>
 struct uh2 {
+  static CopyLoopSpec copy_spec() {
+    CopyLoopSpec c;
+    c.nfields = 2;
+    c.arg[0] = 0; c.arg[1] = 1; c.flag[0] = F0; c.flag[1] = F1;
+    c.flags_arg = 2;
+    c.neg = NEG;
+    c.off[0] = OX; c.off[1] = OY; c.off[2] = OZ;
+    return c;
+  }
   __device__ void operator()(D &a, D &b, const int *fields) const {
     if (fields[F0] == 1) a(0, 0, 0) = NEG ? -(a(OX, OY, OZ)) : a(OX, OY, OZ);
     if (fields[F1] == 1) b(0, 0, 0) = NEG ? -(b(OX, OY, OZ)) : b(OX, OY, OZ);
   }
 };
-#define UH1(NAME, OX, OY, OZ) \
-  struct NAME : uh1<OX, OY, OZ> { C3_LOOP(NAME); };
-#define UH2(NAME, OX, OY, OZ, NEG, ...) \
-  struct NAME : uh2<OX, OY, OZ, NEG, __VA_ARGS__> { C3_LOOP(NAME); };
+#define UH1(NAME, OX, OY, OZ)                     \
+  struct NAME : uh1<OX, OY, OZ> { C3_LOOP(NAME); }; \
+  OPSB_REGISTER_COPY_LOOP(NAME);
+#define UH2(NAME, OX, OY, OZ, NEG, ...)                               \
+  struct NAME : uh2<OX, OY, OZ, NEG, __VA_ARGS__> { C3_LOOP(NAME); }; \
+  OPSB_REGISTER_COPY_LOOP(NAME);
 UH1(update_halo_kernel1_b2, 0, 3, 0)
 UH1(update_halo_kernel1_b1, 0, 1, 0)
 UH1(update_halo_kernel1_t2, 0, -3, 0)

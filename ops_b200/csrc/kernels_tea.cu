@@ -144,6 +144,14 @@ struct set_field_kernel {
 // ---- update_halo_kernels.h: reflective copies of the six halo fields ---------
 template <int OX, int OY>
 struct uh_tea {
+  static CopyLoopSpec copy_spec() {
+    CopyLoopSpec c;
+    c.nfields = 6;
+    for (int f = 0; f < 6; f++) c.arg[f] = f, c.flag[f] = FIELD_DENSITY + f;
+    c.flags_arg = 6;
+    c.off[0] = OX; c.off[1] = OY;
+    return c;
+  }
   __device__ void operator()(D &density, D &energy0, D &energy1, D &u, D &p, D &sd, const int *fields) const {
     if (fields[FIELD_DENSITY] == 1) density(0, 0) = density(OX, OY);
     if (fields[FIELD_ENERGY0] == 1) energy0(0, 0) = energy0(OX, OY);
@@ -153,8 +161,9 @@ struct uh_tea {
     if (fields[FIELD_SD] == 1) sd(0, 0) = sd(OX, OY);
   }
 };
-#define UH_TEA(NAME, OX, OY) \
-  struct NAME : uh_tea<OX, OY> { TL_LOOP(NAME); };
+#define UH_TEA(NAME, OX, OY)                     \
+  struct NAME : uh_tea<OX, OY> { TL_LOOP(NAME); }; \
+  OPSB_REGISTER_COPY_LOOP(NAME);
 UH_TEA(update_halo_kernel1_b2, 0, 3)
 UH_TEA(update_halo_kernel1_b1, 0, 1)
 UH_TEA(update_halo_kernel1_t2, 0, -3)

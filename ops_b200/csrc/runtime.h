@@ -123,6 +123,21 @@ struct LoopStats {
   long long count = 0;
 };
 
+// A loop kernel whose every point only copies, for each listed argument f,
+//   if (flags == nullptr || flags[flag[f]] == 1) a_f(0,0,0) = (neg ? -1 : 1) * a_f(off)
+// with `flags` the int array of global argument `flags_arg` (-1: no flags).
+// Runs of such loops are executed as batches of independent copies
+// (copy_batch.cu) instead of one launch each.
+struct CopyLoopSpec {
+  int nfields = 0;
+  int arg[8] = {0}, flag[8] = {0};
+  int flags_arg = -1;
+  int neg = 0;
+  int off[3] = {0, 0, 0};
+};
+void register_copy_loop(const std::string &kernel, const CopyLoopSpec &spec);
+const CopyLoopSpec *find_copy_loop(const LoopInfo *loop);
+
 class Runtime {
  public:
   static Runtime &get();
@@ -200,6 +215,7 @@ class Runtime {
   int diags() const { return diags_; }
   void reset_counters() { kernels_launched_ = graphs_launched_ = loops_enqueued_ = 0; }
   char *red_scratch() const { return red_scratch_; }
+  char *gbl_device() const { return gbl_dev_; }  // this flush's staged globals (Desc::gbl_off)
   unsigned int *red_counters() const { return red_counters_; }
   static constexpr int kMaxRedBlocks = 65536;
   static constexpr int kNumCounters = 256;
@@ -332,6 +348,11 @@ struct LoopRegistrar {
   LoopRegistrar() { Runtime::register_loop(make_loop_info<K>(K::kname)); }
 };
 #define OPSB_REGISTER_LOOP(K) static ::opsb::LoopRegistrar<K> opsb_reg_##K
+template <class K>
+struct CopyLoopRegistrar {
+  CopyLoopRegistrar() { register_copy_loop(K::kname, K::copy_spec()); }
+};
+#define OPSB_REGISTER_COPY_LOOP(K) static ::opsb::CopyLoopRegistrar<K> opsb_copy_reg_##K
 
 // ops_par_loop by registered kernel name (what translated app code and the
 // C++ app drivers call; no template instantiation at the call site).
