@@ -132,6 +132,7 @@ struct generate_chunk_kernel {
 // ---- ideal_gas_kernel.h:4 ----------------------------------------------------
 struct ideal_gas_kernel {
   CL_LOOP(ideal_gas_kernel);
+  static constexpr bool touch_next_row = true;
   __device__ void operator()(const D &density, const D &energy, D &pressure, D &soundspeed) const {
     double v = 1.0 / density(0, 0);
     pressure(0, 0) = (1.4 - 1.0) * density(0, 0) * energy(0, 0);
@@ -385,6 +386,7 @@ struct revert_kernel {
 // ---- accelerate_kernel.h:8 ---------------------------------------------------
 struct accelerate_kernel {
   CL_LOOP(accelerate_kernel);
+  static constexpr bool touch_next_row = true;
   static constexpr int min_blocks = 4;
   __device__ void operator()(const D &density0, const D &volume, D &stepbymass, const D &xvel0, D &xvel1,
                              const D &xarea, const D &pressure, const D &yvel0, D &yvel1, const D &yarea,
@@ -485,6 +487,7 @@ struct YView {
 
 struct advec_cell_kernel3_xdir {  // :28
   CL_LOOP(advec_cell_kernel3_xdir);
+  static constexpr bool touch_next_row = true;
   __device__ void operator()(const D &vol_flux_x, const D &pre_vol, const I &xx, const D &vertexdx, const D &density1,
                              const D &energy1, D &mass_flux_x, D &ener_flux) const {
     double mf, ef;
@@ -496,6 +499,7 @@ struct advec_cell_kernel3_xdir {  // :28
 };
 struct advec_cell_kernel4_xdir {  // :106
   CL_LOOP(advec_cell_kernel4_xdir);
+  static constexpr bool touch_next_row = true;
   static constexpr int min_blocks = 4;
   __device__ void operator()(D &density1, D &energy1, const D &mass_flux_x, const D &vol_flux_x, const D &pre_vol,
                              const D &post_vol, D &pre_mass, D &post_mass, D &advec_vol, D &post_ener,
@@ -524,6 +528,7 @@ struct advec_cell_kernel2_ydir {  // :133
 };
 struct advec_cell_kernel3_ydir {  // :142
   CL_LOOP(advec_cell_kernel3_ydir);
+  static constexpr bool touch_next_row = true;
   __device__ void operator()(const D &vol_flux_y, const D &pre_vol, const I &yy, const D &vertexdy, const D &density1,
                              const D &energy1, D &mass_flux_y, D &ener_flux) const {
     double mf, ef;
@@ -682,6 +687,7 @@ struct reset_field_kernel2 {  // :13
 // ---- field_summary_kernel.h:4 -------------------------------------------------
 struct field_summary_kernel {
   CL_LOOP(field_summary_kernel);
+  static constexpr bool touch_next_row = true;
   static constexpr int min_blocks = 6;
   __device__ void operator()(const D &volume, const D &density0, const D &energy0, const D &pressure, const D &xvel0,
                              const D &yvel0, RED<double> &vol, RED<double> &mass, RED<double> &ie, RED<double> &ke,

@@ -45,6 +45,7 @@ __host__ __device__ __forceinline__ double op_sign(double a, double b) { return 
 // one point wide along a dimension is only ever offset along the other.
 template <class T>
 struct ACC2 {
+  using value_type = T;
   T *p;
   int sy;
   ACC2() = default;
@@ -243,6 +244,9 @@ __device__ void finish_grid_reduction(const ArgView &a, const LoopParams &lp, in
   }
 }
 
+template <class A> struct is_acc2 : std::false_type {};
+template <class T> struct is_acc2<ACC2<T>> : std::true_type {};
+
 template <class K, class Sig> struct Exec;
 
 template <class K, class C, class... P>
@@ -258,6 +262,22 @@ struct Exec<K, void (C::*)(P...) const> {
   __device__ static __forceinline__ void call(const K &k, Tup &t, const LoopParams &lp, int x, int y, int z,
                                               std::index_sequence<I...>) {
     k(get_leaf<I, Slot<std::decay_t<P>>>(t).at(lp.a[I], x, y, z)...);
+  }
+  // L2 prefetch hint for the centre point of every read-only accessor at
+  // (x, y): a thread asks for its next row before working on this one.
+  template <size_t... I>
+  __device__ static __forceinline__ void touch_all(const LoopParams &lp, int x, int y, std::index_sequence<I...>) {
+    (touch_one<I>(lp, x, y), ...);
+  }
+  template <size_t I>
+  __device__ static __forceinline__ void touch_one(const LoopParams &lp, int x, int y) {
+    using RP = std::remove_reference_t<std::tuple_element_t<I, std::tuple<P...>>>;
+    if constexpr (std::is_const<RP>::value && is_acc2<std::remove_const_t<RP>>::value) {
+      using T = typename std::remove_const_t<RP>::value_type;
+      const ArgView &a = lp.a[I];
+      const T *p = reinterpret_cast<const T *>(a.ptr) + (x * a.sx + y * a.sy);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
   }
   template <size_t... I>
   __device__ static __forceinline__ void finish_all(Tup &t, const LoopParams &lp, double *smem, int nblocks,
@@ -310,6 +330,14 @@ template <class K> struct LoopRowUnroll<K, std::void_t<decltype(K::row_unroll)>>
   static constexpr int value = K::row_unroll;
 };
 
+// Next-row prefetch hints (Exec::touch_all) in the 2D row loop: they help
+// the loops whose reads are few and far between stores and slow down the
+// rest, so a kernel opts in with `touch_next_row` (measured per kernel).
+template <class K, class = void> struct LoopTouch { static constexpr bool value = false; };
+template <class K> struct LoopTouch<K, std::void_t<decltype(K::touch_next_row)>> {
+  static constexpr bool value = K::touch_next_row;
+};
+
 // The generic loop kernel. blockDim = (BX, BY); blocks tile x exactly and
 // stride over the remaining (y, z) rows.
 template <class K>
@@ -326,8 +354,12 @@ __global__ void __launch_bounds__(256, LoopMinBlocks<K>::value) exec_loop(const 
     if (nz == 1) {
       constexpr int kUnroll = LoopRowUnroll<K>::value;
 #pragma unroll (kUnroll)
-      for (int y = lp.start[1] + blockIdx.y * blockDim.y + threadIdx.y; y < lp.end[1]; y += gridDim.y * blockDim.y)
+      for (int y = lp.start[1] + blockIdx.y * blockDim.y + threadIdx.y; y < lp.end[1]; y += gridDim.y * blockDim.y) {
+        if constexpr (LoopTouch<K>::value)
+          if (y + (int)(gridDim.y * blockDim.y) < lp.end[1])
+            E::touch_all(lp, x, y + gridDim.y * blockDim.y, typename E::Seq{});
         E::call(k, t, lp, x, y, lp.start[2], typename E::Seq{});
+      }
     } else {
       for (long long r = (long long)blockIdx.y * blockDim.y + threadIdx.y; r < nrows;
            r += (long long)gridDim.y * blockDim.y) {

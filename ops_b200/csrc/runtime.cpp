@@ -86,11 +86,11 @@ Runtime::~Runtime() {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   for (auto &d : dats_)
     if (d && d->data_d) cudaFree(d->data_d);
-  for (auto &r : reductions_)
-    if (r.slot_d) cudaFree(r.slot_d);
+  if (red_arena_) cudaFree(red_arena_);
   if (gbl_dev_) cudaFree(gbl_dev_);
   if (red_scratch_) cudaFree(red_scratch_);
   if (red_counters_) cudaFree(red_counters_);
+  if (red_host_) cudaFreeHost(red_host_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -112,6 +112,9 @@ void Runtime::init(int device, int diags) {
   OPSB_CUDA(cudaMalloc(&red_scratch_, scratch));
   OPSB_CUDA(cudaMalloc(&red_counters_, kNumCounters * sizeof(unsigned int)));
   OPSB_CUDA(cudaMemset(red_counters_, 0, kNumCounters * sizeof(unsigned int)));
+  OPSB_CUDA(cudaMalloc(&red_arena_, kRedArenaBytes));
+  OPSB_CUDA(cudaMemset(red_arena_, 0, kRedArenaBytes));
+  OPSB_CUDA(cudaMallocHost(&red_host_, kRedArenaBytes));
   const char *g = getenv("OPS_B200_GRAPHS");
   if (g) graphs_on_ = atoi(g);
   const char *f = getenv("OPS_B200_FUSION");
@@ -235,8 +238,12 @@ int Runtime::decl_reduction(int size, const char *type, const char *name) {
   r.elem = type_size_of(r.type.c_str());
   require(r.elem > 0, E_ARG, "unknown reduction type " + r.type);
   r.name = name ? name : "";
-  OPSB_CUDA(cudaMalloc(&r.slot_d, std::max(size, 64)));
-  OPSB_CUDA(cudaMemset(r.slot_d, 0, std::max(size, 64)));
+  auto span = [](int bytes) { return (size_t)((std::max(bytes, 64) + 63) / 64 * 64); };
+  size_t off = reductions_.empty() ? 0 : (size_t)(reductions_.back().slot_d - red_arena_) + span(reductions_.back().size);
+  require(off + span(size) <= kRedArenaBytes, E_UNSUPPORTED, "reduction handles exceed the 64 KiB arena");
+  r.slot_d = red_arena_ + off;
+  OPSB_CUDA(cudaMemsetAsync(r.slot_d, 0, span(size), stream_));
+  red_dirty_ = true;
   reductions_.push_back(r);
   return r.index;
 }
@@ -633,6 +640,7 @@ void Runtime::launch_items(std::vector<Desc> &q) {
 }
 
 void Runtime::run_queue(std::vector<Desc> &q) {
+  red_dirty_ = true;
   elide_copies(q);
   // OPSB_TRACE_QUEUE=1: every flushed loop to stderr (kernel, range, per dat
   // arg: name, access, stencil points), for analysing loop chains
@@ -714,8 +722,14 @@ void Runtime::execute() {
 void Runtime::reduction_result(int handle, void *out) {
   Reduction &r = reduction(handle);
   execute();
-  OPSB_CUDA(cudaMemcpyAsync(out, r.slot_d, r.size, cudaMemcpyDeviceToHost, stream_));
-  OPSB_CUDA(cudaStreamSynchronize(stream_));
+  if (red_dirty_) {
+    const Reduction &last = reductions_.back();
+    const size_t used = (size_t)(last.slot_d - red_arena_) + (size_t)last.size;
+    OPSB_CUDA(cudaMemcpyAsync(red_host_, red_arena_, used, cudaMemcpyDeviceToHost, stream_));
+    OPSB_CUDA(cudaStreamSynchronize(stream_));
+    red_dirty_ = false;
+  }
+  memcpy(out, red_host_ + (r.slot_d - red_arena_), r.size);
   r.initialized = 0;  // ops_reduction_result_char resets the handle (ops_lib_core.cpp:1143)
 }
 
@@ -799,7 +813,6 @@ void Runtime::release_to(const Mark &m) {
     dats_.pop_back();
   }
   while (reductions_.size() > m.reductions) {
-    if (reductions_.back().slot_d) cudaFree(reductions_.back().slot_d);
     reductions_.pop_back();
   }
   stencils_.resize(std::min(stencils_.size(), m.stencils));

@@ -219,6 +219,7 @@ class Runtime {
   unsigned int *red_counters() const { return red_counters_; }
   static constexpr int kMaxRedBlocks = 65536;
   static constexpr int kNumCounters = 256;
+  static constexpr size_t kRedArenaBytes = 1 << 16;
 
   // Declarations made by one app call are released when it returns.
   struct Mark { size_t blocks, dats, stencils, reductions; };
@@ -260,6 +261,12 @@ class Runtime {
 
   char *red_scratch_ = nullptr;
   unsigned int *red_counters_ = nullptr;
+  // Reduction handles live in one device arena; a result request copies the
+  // whole arena once to pinned memory and serves further requests from
+  // there until loops run again.
+  char *red_arena_ = nullptr;
+  char *red_host_ = nullptr;
+  bool red_dirty_ = true;
 
   struct GraphEntry {
     int seen = 0;
