@@ -72,6 +72,16 @@ int ops_b200_decl_dat(int block, int dim, const int *size, const int *base, cons
  * (ops/c/src/core/ops_lib_core.cpp:640,689). `stride` may be NULL. */
 int ops_b200_decl_stencil(int dims, int points, const int *stencil, const char *name);
 int ops_b200_decl_strided_stencil(int dims, int points, const int *stencil, const int *stride, const char *name);
+/* ops_decl_restrict_stencil / ops_decl_prolong_stencil
+ * (ops/c/src/core/ops_lib_core.cpp:740-833): at loop point x a restrict
+ * stencil addresses the (fine) dat at x * stride + offset, a prolong stencil
+ * the (coarse) dat at floor(x / stride) + offset, per dimension -- the
+ * addressing the reference generates for them in its MPI backend
+ * (ops_translator_legacy/c/ops_gen_mpi_lazy.py:283-315), which is the only
+ * one that gives them a meaning. Only loop kernels built with `mgrid = true`
+ * accept them (OPS_B200_ERR_UNSUPPORTED otherwise). */
+int ops_b200_decl_restrict_stencil(int dims, int points, const int *stencil, const int *stride, const char *name);
+int ops_b200_decl_prolong_stencil(int dims, int points, const int *stencil, const int *stride, const char *name);
 
 /* ops_decl_reduction_handle (ops/c/src/core/ops_lib_core.cpp:1119). */
 int ops_b200_decl_reduction_handle(int size, const char *type, const char *name);

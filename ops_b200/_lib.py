@@ -138,6 +138,8 @@ def _declare(L):
         "ops_b200_decl_dat": ([i, i, P, P, P, P, P, i, cp, cp], i),
         "ops_b200_decl_stencil": ([i, i, P, cp], i),
         "ops_b200_decl_strided_stencil": ([i, i, P, P, cp], i),
+        "ops_b200_decl_restrict_stencil": ([i, i, P, P, cp], i),
+        "ops_b200_decl_prolong_stencil": ([i, i, P, P, cp], i),
         "ops_b200_decl_reduction_handle": ([i, cp, cp], i),
         "ops_b200_decl_halo": ([i, i, P, P, P, P, P], i),
         "ops_b200_decl_halo_group": ([i, P], i),

@@ -102,6 +102,20 @@ int ops_b200_decl_strided_stencil(int dims, int points, const int *stencil, cons
   });
 }
 
+int ops_b200_decl_restrict_stencil(int dims, int points, const int *stencil, const int *stride, const char *name) {
+  return guarded([&] {
+    if (!stencil) throw opsb::Error(opsb::E_ARG, "stencil offsets required");
+    return rt().decl_mgrid_stencil(dims, points, stencil, stride, 2, name);
+  });
+}
+
+int ops_b200_decl_prolong_stencil(int dims, int points, const int *stencil, const int *stride, const char *name) {
+  return guarded([&] {
+    if (!stencil) throw opsb::Error(opsb::E_ARG, "stencil offsets required");
+    return rt().decl_mgrid_stencil(dims, points, stencil, stride, 1, name);
+  });
+}
+
 int ops_b200_decl_reduction_handle(int size, const char *type, const char *name) {
   return guarded([&] { return rt().decl_reduction(size, type, name); });
 }

@@ -92,7 +92,7 @@ bool plan(const std::vector<Desc> &q, size_t i, int n, Planned &out) {
     for (int f = 0; f < sp->nfields; f++) {
       const Arg &a = d.args[sp->arg[f]];
       Dat &dt = rt.dat(a.dat);
-      if (dt.elem_size != 8) return false;
+      if (dt.elem_size != 8 || rt.stencil(a.stencil).type != 0) return false;
       Item it;
       CopyStrip &s = it.s;
       s.p = reinterpret_cast<double *>(dt.origin_ptr());

@@ -68,7 +68,7 @@ LoopInfo &swap_outside_info() {
 }
 
 bool zero_point_stencil(const Stencil &s) {
-  if (s.points != 1) return false;
+  if (s.points != 1 || s.type != 0) return false;
   for (int v : s.offs)
     if (v != 0) return false;
   return true;

@@ -94,6 +94,8 @@ struct ArgView {
   int dim;          // components (reduction width for REDUCE)
   int red_index;    // REDUCE: index among this loop's reduction args
   int first;        // REDUCE: 1 when the handle starts from the identity in this loop
+  int mg;           // DAT: 0 plain, 1 prolong, 2 restrict stencil (multigrid)
+  int ms[3];        // DAT: the multigrid stencil's stride per dimension
 };
 
 struct LoopParams {
@@ -211,6 +213,20 @@ struct Slot<IDX> {
   }
 };
 
+// Multigrid stencils address a dat of another resolution: a restrict
+// stencil reads the fine dat at x * stride, a prolong stencil the coarse dat
+// at floor(x / stride), stencil offsets added after (the addressing the
+// reference generates for them, ops_translator_legacy/c/ops_gen_mpi_lazy.py:283-315,
+// for non-negative loop starts).
+__device__ __forceinline__ int mg_index(int x, int mode, int s) {
+  if (mode == 2) return x * s;
+  if (mode == 1) return x >= 0 ? x / s : -((s - 1 - x) / s);
+  return x;
+}
+template <class P> struct is_accessor_slot : std::false_type {};
+template <class T> struct is_accessor_slot<ACC2<T>> : std::true_type {};
+template <class T> struct is_accessor_slot<ACC3<T>> : std::true_type {};
+
 // Pointer parameters are globals (ops_arg_gbl): READ as const T*, RW as T*.
 template <class T>
 struct Slot<T *> {
@@ -247,6 +263,13 @@ __device__ void finish_grid_reduction(const ArgView &a, const LoopParams &lp, in
 template <class A> struct is_acc2 : std::false_type {};
 template <class T> struct is_acc2<ACC2<T>> : std::true_type {};
 
+// Kernels that may be given restrict/prolong stencils state `mgrid = true`
+// (their accessors then map the point's index per argument).
+template <class K, class = void> struct LoopMgridOk { static constexpr bool value = false; };
+template <class K> struct LoopMgridOk<K, std::void_t<decltype(K::mgrid)>> {
+  static constexpr bool value = K::mgrid;
+};
+
 template <class K, class Sig> struct Exec;
 
 template <class K, class C, class... P>
@@ -261,7 +284,18 @@ struct Exec<K, void (C::*)(P...) const> {
   template <size_t... I>
   __device__ static __forceinline__ void call(const K &k, Tup &t, const LoopParams &lp, int x, int y, int z,
                                               std::index_sequence<I...>) {
-    k(get_leaf<I, Slot<std::decay_t<P>>>(t).at(lp.a[I], x, y, z)...);
+    k(slot_at<I>(t, lp, x, y, z)...);
+  }
+  template <size_t I>
+  __device__ static __forceinline__ decltype(auto) slot_at(Tup &t, const LoopParams &lp, int x, int y, int z) {
+    using PT = std::decay_t<std::tuple_element_t<I, std::tuple<P...>>>;
+    auto &sl = get_leaf<I, Slot<PT>>(t);
+    if constexpr (LoopMgridOk<K>::value && is_accessor_slot<PT>::value) {
+      const ArgView &a = lp.a[I];
+      return sl.at(a, mg_index(x, a.mg, a.ms[0]), mg_index(y, a.mg, a.ms[1]), mg_index(z, a.mg, a.ms[2]));
+    } else {
+      return sl.at(lp.a[I], x, y, z);
+    }
   }
   // L2 prefetch hint for the centre point of every read-only accessor at
   // (x, y): a thread asks for its next row before working on this one.

@@ -228,6 +228,18 @@ int Runtime::decl_stencil(int dims, int points, const int *offs, const int *stri
   return s.index;
 }
 
+int Runtime::decl_mgrid_stencil(int dims, int points, const int *offs, const int *mgrid_stride, int type,
+                                const char *name) {
+  require(type == 1 || type == 2, E_ARG, "multigrid stencil type must be 1 (prolong) or 2 (restrict)");
+  require(mgrid_stride != nullptr, E_ARG, "multigrid stencils need a stride");
+  for (int i = 0; i < dims && i < 3; i++) require(mgrid_stride[i] >= 1, E_ARG, "multigrid stride must be >= 1");
+  int h = decl_stencil(dims, points, offs, nullptr, name);
+  Stencil &st = stencils_[h];
+  st.type = type;
+  for (int i = 0; i < 3; i++) st.mgrid[i] = i < dims ? mgrid_stride[i] : 1;
+  return h;
+}
+
 int Runtime::decl_reduction(int size, const char *type, const char *name) {
   require(inited_, E_STATE, "ops_decl_reduction_handle before ops_init");
   require(size > 0, E_ARG, "reduction size must be positive");
@@ -319,6 +331,8 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         require(dt.plane < (1LL << 31), E_UNSUPPORTED, "dat " + dt.name + " has a plane of 2^31 elements or more");
         require(dt.block == blk, E_ARG, "dat " + dt.name + " is declared on another block");
         require(dt.locked == 0, E_STATE, "dat " + dt.name + " is used in a loop while its raw pointer is held (ops_lib_core.cpp:2321)");
+        require(stencils_[a.stencil].type == 0 || loop->mgrid_ok, E_UNSUPPORTED,
+                "loop " + loop->kernel + " is not built for restrict/prolong stencils (mgrid)");
         check_in_allocation(d, a, dt);
         if (a.acc != ACC_READ) dt.host.clear();
         break;
@@ -379,8 +393,17 @@ void Runtime::check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) co
         if (p == 0 || o < omin) omin = o;
         if (p == 0 || o > omax) omax = o;
       }
-      lo = (long long)d.range[2 * k] + omin;
-      hi = (long long)d.range[2 * k + 1] - 1 + omax;
+      long long x0 = d.range[2 * k], x1 = (long long)d.range[2 * k + 1] - 1;
+      if (st.type == 2) {  // restrict: x * stride
+        x0 *= st.mgrid[k];
+        x1 *= st.mgrid[k];
+      } else if (st.type == 1) {  // prolong: floor(x / stride)
+        auto fl = [](long long v, long long q) { return v >= 0 ? v / q : -((q - 1 - v) / q); };
+        x0 = fl(x0, st.mgrid[k]);
+        x1 = fl(x1, st.mgrid[k]);
+      }
+      lo = x0 + omin;
+      hi = x1 + omax;
     } else {
       lo = hi = 0;
     }
@@ -488,6 +511,8 @@ void Runtime::build_params(const Desc &d, LoopParams &lp, int *nred_out) {
         v.sz = st.stride[2] ? (int)dt.plane : 0;
         v.ay = (int)dt.pitch;
         v.az = (int)dt.plane;
+        v.mg = st.type;
+        for (int k = 0; k < 3; k++) v.ms[k] = st.mgrid[k];
         break;
       }
       case ARG_GBL:

@@ -68,6 +68,8 @@ struct Stencil {
   int index = 0, dims = 0, points = 0;
   std::vector<int> offs;   // points*dims
   int stride[3] = {1, 1, 1};
+  int type = 0;            // 0 plain, 1 prolong, 2 restrict (ops_stencil_core::type)
+  int mgrid[3] = {1, 1, 1};  // ops_stencil_core::mgrid_stride
   std::string name;
 };
 
@@ -95,6 +97,7 @@ struct LoopInfo {
   int ndim = 2;             // accessor dimensionality (0 when the kernel has none)
   int copy_dst = -1, copy_src = -1;  // pure copy kernels: which args are dst/src
   int internal = 0;         // runtime-internal item (not launched through exec_loop)
+  int mgrid_ok = 0;         // the kernel maps multigrid (restrict/prolong) stencils
   void (*launch)(const LoopParams &, dim3, dim3, cudaStream_t) = nullptr;
 };
 
@@ -151,6 +154,9 @@ class Runtime {
   int decl_dat(int block, int dim, const int *size, const int *base, const int *d_m, const int *d_p,
                const void *data, int type_size, const char *type, const char *name);
   int decl_stencil(int dims, int points, const int *offs, const int *stride, const char *name);
+  // ops_decl_restrict_stencil (type 2) / ops_decl_prolong_stencil (type 1)
+  // (ops/c/src/core/ops_lib_core.cpp:740-833)
+  int decl_mgrid_stencil(int dims, int points, const int *offs, const int *mgrid_stride, int type, const char *name);
   int decl_reduction(int size, const char *type, const char *name);
   // ops_decl_halo / ops_decl_halo_group / ops_halo_transfer
   // (ops/c/src/core/ops_lib_core.cpp:998-1040, ops_device_singlenode_common.cpp:262-346)
@@ -344,6 +350,7 @@ LoopInfo make_loop_info(const char *kernel) {
   li.copy_dst = CopyTrait<K>::dst;
   li.copy_src = CopyTrait<K>::src;
   li.launch = &launch_exec<K>;
+  li.mgrid_ok = LoopMgridOk<K>::value ? 1 : 0;
   return li;
 }
 

@@ -84,7 +84,12 @@ __device__ __forceinline__ double recip(double x) {
 // L + 1 elements to spread the chunks over the shared-memory banks.
 constexpr int kTileThreads = 256;
 
-constexpr size_t kTileSmem = 110 * 1024;  // per CTA, so that two CTAs share an SM
+#ifndef TRID_CTAS_PER_SM
+#define TRID_CTAS_PER_SM 2
+#endif
+constexpr int kCtasPerSm = TRID_CTAS_PER_SM;
+// shared memory per CTA, so that kCtasPerSm CTAs share an SM (227 KB)
+constexpr size_t kTileSmem = (size_t)(220 / kCtasPerSm) * 1024;
 
 template <class T>
 size_t tile_smem(int L, int n) {
@@ -101,7 +106,7 @@ __device__ __forceinline__ void cp_async(T *dst, const T *src) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(kTileThreads, 2) trid_tile_kernel(const Sys *__restrict__ sys,
+__global__ void __launch_bounds__(kTileThreads, kCtasPerSm) trid_tile_kernel(const Sys *__restrict__ sys,
                                                                     const Work *__restrict__ work, int nwork, int L,
                                                                     int nmax) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -362,7 +367,7 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
     OPSB_CUDA(cudaFuncSetAttribute(trid_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = smem;
   }
-  const int per_sm = std::max(1, std::min(2, (int)(233472 / (smem + 1024))));
+  const int per_sm = std::max(1, std::min(kCtasPerSm, (int)(233472 / (smem + 1024))));
   const int grid = std::min(nwork, 148 * per_sm);
   trid_tile_kernel<T><<<grid, kTileThreads, smem, stream>>>(B.sys, B.work, nwork, L, maxn);
   OPSB_CUDA(cudaGetLastError());

@@ -81,8 +81,10 @@ def ops_decl_block(dims, name):
     return ops_block(check(lib().ops_b200_decl_block(dims, name.encode())), dims, name)
 
 
-def ops_decl_dat(block, dim, size, base, d_m, d_p, data, type_, name):
-    """ops_decl_dat; `data` (numpy array or None) holds the full extent."""
+def ops_decl_dat(block, dim, size, base, d_m, d_p, data, type_, name, stride=None):
+    """ops_decl_dat; `data` (numpy array or None) holds the full extent.
+    `stride` (the multigrid overload's coarsening factor) only matters to the
+    reference's MPI decomposition and is accepted and ignored here."""
     dtype, ts = _TYPES[type_]
     buf = None
     if data is not None:
@@ -100,6 +102,18 @@ def ops_decl_stencil(dims, points, sten, name):
 
 def ops_decl_strided_stencil(dims, points, sten, stride, name):
     return ops_stencil(check(lib().ops_b200_decl_strided_stencil(dims, points, _iarr(sten), _iarr(stride),
+                                                                 name.encode())), dims, points, name)
+
+
+def ops_decl_restrict_stencil(dims, points, sten, stride, name):
+    """ops_decl_restrict_stencil: at loop point x, the dat at x * stride + offset."""
+    return ops_stencil(check(lib().ops_b200_decl_restrict_stencil(dims, points, _iarr(sten), _iarr(stride),
+                                                                  name.encode())), dims, points, name)
+
+
+def ops_decl_prolong_stencil(dims, points, sten, stride, name):
+    """ops_decl_prolong_stencil: at loop point x, the dat at floor(x / stride) + offset."""
+    return ops_stencil(check(lib().ops_b200_decl_prolong_stencil(dims, points, _iarr(sten), _iarr(stride),
                                                                  name.encode())), dims, points, name)
 
 
