@@ -114,7 +114,13 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+# device the timing collectives use: the rank's GPU under NCCL, the host
+# under gloo (the reference arm, and the CPU tests of this path)
+_DIST_DEVICE = "cpu"
+
+
 def dist_setup(args):
+    global _DIST_DEVICE
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -127,6 +133,9 @@ def dist_setup(args):
         backend = "nccl" if args.impl == "ours" else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
+            _DIST_DEVICE = f"cuda:{local}"
+        else:
+            _DIST_DEVICE = "cpu"
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
@@ -136,7 +145,7 @@ def max_over_ranks(pg, value, local):
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([value], dtype=torch.float64, device=_DIST_DEVICE)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -145,9 +154,11 @@ def barrier(pg, local):
     if pg is None:
         return
     import torch
-    torch.cuda.synchronize(local)
+    if _DIST_DEVICE.startswith("cuda"):
+        torch.cuda.synchronize(local)
     pg.barrier()
-    torch.cuda.synchronize(local)
+    if _DIST_DEVICE.startswith("cuda"):
+        torch.cuda.synchronize(local)
 
 
 # ---------------------------------------------------------------------------
