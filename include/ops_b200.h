@@ -391,7 +391,7 @@ typedef struct ops_b200_heat_stats {
   int iterations;          /* CG iterations (method 0: as TeaLeaf prints them) */
   int updates;             /* reliable updates (method 2) */
   int converged;
-  int fallbacks;           /* learned -> Jacobi switches (method 3) */
+  int fallbacks;           /* preconditioner -> Jacobi switches (methods 3, 5) */
   double initial_residual; /* ||u0 - A u|| at entry */
   double final_residual;   /* ||u0 - A u|| at exit, FP64 */
   double seconds;          /* device time of the solve */
@@ -403,14 +403,25 @@ typedef struct ops_b200_heat_stats {
 #define OPS_B200_HEAT_MIXED 2        /* FP32 Jacobi-PCG under FP64 reliable updates */
 #define OPS_B200_HEAT_FCG_LEARNED 3  /* flexible CG, learned preconditioner `net`, Jacobi fallback */
 #define OPS_B200_HEAT_FCG_JACOBI 4   /* the same flexible CG with Jacobi (no network) */
+#define OPS_B200_HEAT_FCG_MG 5       /* the same flexible CG, one native multigrid V-cycle per iteration */
 
 /* Solves A u = u0. `net` names a learned preconditioner (method 3); window:
- * method 3 falls back to Jacobi when ||r|| has not halved over `window`
+ * methods 3 and 5 fall back to Jacobi when ||r|| has not halved over `window`
  * iterations (0 = only on lost positive curvature). r_out (device, may be
  * NULL) receives u0 - A u at exit. Synchronous on `stream`. Not reentrant:
  * one solve at a time per process (a shared workspace is kept per size). */
 int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, double eps, int max_iters, int window,
                         double *r_out, ops_b200_heat_stats *stats, void *stream);
+
+/* Native multigrid preconditioner of method 5: z = M r, one FP32 V-cycle
+ * over a hierarchy of 2 x 2 aggregates (coarse mass = sum of the aggregate's,
+ * coarse face weight = half the sum of the fine faces it covers, coarsening
+ * down to at most 16 x 16 cells), two damped-Jacobi sweeps (omega 0.8) before
+ * and after each coarse correction, 64 sweeps on the coarsest level. The
+ * hierarchy is built from sys (Kx, Ky, rx, ry; u0 and u are not read); r and
+ * z are device fields laid out like sys's (same pitch). *levels (may be
+ * NULL) receives the number of levels. Synchronous on `stream`. */
+int ops_b200_heat_mg_apply(const ops_b200_heat_system *sys, const double *r, double *z, int *levels, void *stream);
 
 /* ---- learned multigrid preconditioner (no reference counterpart) ---------
  * A 4-level U-Net-shaped CNN (16/32/64/64 channels, 3x3 BF16 convolutions on

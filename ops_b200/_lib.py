@@ -173,6 +173,7 @@ def _declare(L):
         "ops_b200_trid_batch": ([i, i, i, P, P], i),
         "ops_b200_conv3x3_bf16": ([P, P, P, P, P, i, i, i, i, i, i, P], i),
         "ops_b200_heat_solve": ([P, i, i, ctypes.c_double, i, i, P, P, P], i),
+        "ops_b200_heat_mg_apply": ([P, P, P, P, P], i),
         "ops_b200_lmg_create": ([ctypes.c_ulonglong], i),
         "ops_b200_lmg_destroy": ([i], i),
         "ops_b200_lmg_num_params": ([], i),

@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
 # Sources whose arithmetic may contract to FMA (no bit-parity requirement).
-FMAD_OK = {"tridiag.cu"}
+FMAD_OK = {"tridiag.cu", "heat_mg.cu"}
 
 
 def _sources():

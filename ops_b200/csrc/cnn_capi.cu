@@ -60,6 +60,7 @@ extern "C" int ops_b200_conv3x3_bf16(const void *x, const void *w, const float *
 #include <vector>
 
 #include "heat_pcg.h"
+#include "heat_mg.h"
 #include "lmg.h"
 
 namespace opsb {
@@ -71,6 +72,7 @@ struct HeatWorkspace {
   double *buf = nullptr;
   double *r = nullptr, *w = nullptr, *p = nullptr, *z = nullptr, *Mi = nullptr;
   heat::Solver solver;
+  heat::Multigrid mg;
   ~HeatWorkspace() { cudaFree(buf); }
   void ensure(int x, int y, long long pt, cudaStream_t s) {
     if (x == nx && y == ny && pt == pitch && buf) return;
@@ -137,7 +139,7 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
   return capi_guard([&] {
     if (!sys || !sys->Kx || !sys->Ky || !sys->u0 || !sys->u) throw Error(E_ARG, "heat system: null field");
     if (sys->nx < 1 || sys->ny < 1 || sys->pitch < sys->nx + 2) throw Error(E_ARG, "heat system: bad shape");
-    if (method < OPS_B200_HEAT_PCG || method > OPS_B200_HEAT_FCG_JACOBI) throw Error(E_ARG, "heat system: method");
+    if (method < OPS_B200_HEAT_PCG || method > OPS_B200_HEAT_FCG_MG) throw Error(E_ARG, "heat system: method");
     if (!(eps > 0.0) || max_iters < 0) throw Error(E_ARG, "heat system: eps > 0 and max_iters >= 0 required");
     std::lock_guard<std::mutex> lk(g_mu);
     // the iteration chunks are replayed from CUDA graphs, which cannot be
@@ -192,6 +194,10 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
           np->apply(lf, z, ss);
           return np->launches() - before;
         };
+      } else if (method == OPS_B200_HEAT_FCG_MG) {
+        heat::Multigrid *mg = &ws.mg;
+        mg->setup(sys->nx, sys->ny, sys->pitch, sys->Kx, sys->Ky, sys->rx, sys->ry, s);
+        M = [mg](const double *r, double *z, cudaStream_t ss) -> long long { return mg->apply(r, z, ss); };
       }
       ws.solver.fcg(f, sys->rx, sys->ry, eps, max_iters, M, window, s, &st);
     }
@@ -218,6 +224,24 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
       stats->seconds = ms * 1e-3;
       stats->launches = ws.solver.launches();
     }
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_heat_mg_apply(const ops_b200_heat_system *sys, const double *r, double *z, int *levels,
+                                      void *stream) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!sys || !sys->Kx || !sys->Ky || !r || !z) throw Error(E_ARG, "heat multigrid: null field");
+    if (sys->nx < 1 || sys->ny < 1 || sys->pitch < sys->nx + 2) throw Error(E_ARG, "heat multigrid: bad shape");
+    std::lock_guard<std::mutex> lk(g_mu);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!s) s = own_stream();
+    HeatWorkspace &ws = workspace();
+    ws.mg.setup(sys->nx, sys->ny, sys->pitch, sys->Kx, sys->Ky, sys->rx, sys->ry, s);
+    ws.mg.apply(r, z, s);
+    OPSB_CUDA(cudaStreamSynchronize(s));
+    if (levels) *levels = ws.mg.levels();
     return 0;
   });
 }

@@ -22,7 +22,7 @@ import numpy as np
 from . import seeded
 from ._lib import HeatBatch, HeatStats, HeatSystem, check, lib
 
-PCG, PCG_TRUE, MIXED, FCG_LEARNED, FCG_JACOBI = 0, 1, 2, 3, 4
+PCG, PCG_TRUE, MIXED, FCG_LEARNED, FCG_JACOBI, FCG_MG = 0, 1, 2, 3, 4, 5
 
 
 def _vp(t):
@@ -78,6 +78,20 @@ def solve(Kx, Ky, u0, u, rx, ry, method=PCG_TRUE, net=-1, eps=1e-10, max_iters=1
                                     None if r_out is None else interior(r_out, pitch), ctypes.byref(st),
                                     None if stream is None else ctypes.c_void_p(stream)))
     return {k: getattr(st, k) for k, _ in HeatStats._fields_}
+
+
+def mg_apply(Kx, Ky, r, z, rx, ry, stream=None):
+    """z = M r with the library's native multigrid preconditioner (one V-cycle
+    of the hierarchy built from Kx, Ky, rx, ry); padded (ny + 2, nx + 2) FP64
+    CUDA tensors. Returns the number of levels."""
+    ny, nx = Kx.shape[0] - 2, Kx.shape[1] - 2
+    pitch = nx + 2
+    sysd = HeatSystem(nx, ny, pitch, interior(Kx, pitch), interior(Ky, pitch), interior(r, pitch),
+                      interior(z, pitch), rx, ry)
+    levels = ctypes.c_int(0)
+    check(lib().ops_b200_heat_mg_apply(ctypes.byref(sysd), interior(r, pitch), interior(z, pitch),
+                                       ctypes.byref(levels), None if stream is None else ctypes.c_void_p(stream)))
+    return levels.value
 
 
 class Net:
