@@ -17,6 +17,8 @@ configurations with synthetic seeded inputs:
            sweeps.
   learned  the same heat solve with the learned multigrid preconditioner in
            flexible CG (trained on the GPU first), next to plain Jacobi-PCG.
+  mg       the same heat solve with the native FP32 aggregation-multigrid
+           V-cycle as the flexible-CG preconditioner, next to plain Jacobi-PCG.
   tea      implicit heat conduction (TeaLeaf CG, Jacobi preconditioner) on
            4096x4096 with 16 seeded density rectangles; a step is one implicit
            timestep solved to residual 1e-10, FP64 PCG beside FP32-inner /
@@ -815,15 +817,17 @@ def reference_tea(args, world, rank):
     # FP64 Jacobi-PCG iterations to ||r|| < 1e-10 ||r0|| at 4096^2, measured by this
     # repository's solver on the B200: the TeaLeaf deck (tea) and the
     # cell-centre rasterised fields of the learned workload (learned)
-    iters = args.tea_ref_iters or {"tea": 1712, "learned": 1355}.get(args.workload, 1712)
+    iters = args.tea_ref_iters or {"tea": 1712, "learned": 1355, "mg": 1355}.get(args.workload, 1712)
     v = per_it * iters
     return {
         "impl": "reference", "metric": "time to 1e-10 residual", "value": v, "unit": "s", "n_gpus": world,
         "steps": 1, "warmup": 0, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (rho=1 background + 16 SplitMix64-seeded rectangles, seed 4)",
-        "config": {"workload": (f"tealeaf2d_learned_fcg_{N}x{N}" if args.workload == "learned"
-                                else f"tealeaf2d_cg_jacdiag_{N}x{N}"), "grid": [N, N], "eps": 1e-10},
+        "config": {"workload": {"learned": f"tealeaf2d_learned_fcg_{N}x{N}",
+                                "mg": f"tealeaf2d_multigrid_fcg_{N}x{N}"}.get(args.workload,
+                                                                             f"tealeaf2d_cg_jacdiag_{N}x{N}"),
+                   "grid": [N, N], "eps": 1e-10},
         "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference",
                          "sample": f"reference OpenMP TeaLeaf, CG capped at 2 and {2 + args.cpu_tea_iters} iterations;"
                                    f" seconds per iteration x {iters} iterations (the FP64 PCG"
@@ -975,10 +979,99 @@ def bench_learned(args, world, rank, local, pg):
     return line
 
 
+# ---------------------------------------------------------------------------
+# Native multigrid preconditioner in flexible CG vs plain Jacobi-PCG
+# ---------------------------------------------------------------------------
+def bench_mg(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    from ops_b200 import lmg
+    from ops_b200 import ops as O
+
+    peaks, peak_kind = load_peaks()
+    O.ops_init(local, 0)
+    N = args.grid or TEA_N
+    rx = 0.004 / (10.0 / N) ** 2          # the implicit timestep of the 4096^2 heat problem (dt = 0.004)
+    K, W = args.steps, args.warmup
+    rho, en = lmg.density_field(N, 4)
+    Kx, Ky, u0 = lmg.padded_problem(rho, en)
+    kx, ky, b = (torch.from_numpy(a).cuda(local) for a in (Kx, Ky, u0))
+    u = torch.empty_like(b)
+
+    def run(method):
+        u.copy_(b)
+        return lmg.solve(kx, ky, b, u, rx, rx, method=method, eps=1e-10, window=40, max_iters=20000)
+
+    for _ in range(W):
+        run(lmg.FCG_MG)
+    barrier(pg, local)
+    with ClockSampler(local) as cs:
+        mg = [run(lmg.FCG_MG) for _ in range(K)]
+    clocks = cs.summary()
+    u_mg = u.clone()
+    plain = [run(lmg.PCG_TRUE) for _ in range(max(1, min(K, 2)))]
+    err = float(torch.linalg.norm(u_mg - u) / torch.linalg.norm(u))
+    t_mg = max_over_ranks(pg, float(np.median([s["seconds"] for s in mg])), local)
+    t_plain = max_over_ranks(pg, float(np.median([s["seconds"] for s in plain])), local)
+    it = mg[0]["iterations"]
+    # algorithmic bytes of one iteration, per cell: the FP64 flexible-CG
+    # kernels (w = A p with p.w, p.r: Kx Ky p r w 40; u, r update: 48; z.w: 16;
+    # p = z + beta p: 24) and the FP32 V-cycle's fine level (106: r in FP64 and
+    # its FP32 copy, five streaming passes, z out in FP64) plus its coarse
+    # levels (a third of the fine level's 5 x 20 bytes in FP32)
+    per_cell = 128 + 106 + 100 / 3
+    alg = per_cell * N * N * it
+    ach = alg / t_mg / 1e9
+
+    hk = [torch.from_numpy(a).pin_memory() for a in (Kx, Ky, u0)]
+    barrier(pg, local)
+    te = time.perf_counter()
+    dk = [t.cuda(local, non_blocking=True) for t in hk]
+    du = dk[2].clone()
+    st_e2e = lmg.solve(dk[0], dk[1], dk[2], du, rx, rx, method=lmg.FCG_MG, eps=1e-10, window=40)
+    host_u = du.cpu()
+    e2e_s = max_over_ranks(pg, time.perf_counter() - te, local)
+    del host_u
+    line = {
+        "metric": "time to 1e-10 residual (multigrid FCG)", "value": t_mg, "unit": "s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": t_mg * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 solve / f32 V-cycle",
+        "data": "synthetic (rho=1 background + 16 SplitMix64-seeded rectangles, rho log-uniform [0.1,100], seed 4)",
+        "config": {"workload": f"tealeaf2d_multigrid_fcg_{N}x{N}", "grid": [N, N], "rx": rx, "eps": 1e-10,
+                   "preconditioner": "2x2 aggregation, coarse faces x 1/2, 2+2 damped-Jacobi sweeps (0.8),"
+                                     " 16x16 coarsest level, one V-cycle per FCG iteration",
+                   "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+        "multigrid_fcg": {"seconds": t_mg, "iterations": it, "fallbacks": mg[0]["fallbacks"],
+                          "final_residual_ratio": mg[0]["final_residual"] / mg[0]["initial_residual"],
+                          "rel_l2_vs_fp64_pcg_solution": err},
+        "plain_pcg": {"seconds": t_plain, "iterations": plain[0]["iterations"],
+                      "time_ratio_mg_vs_plain": t_mg / t_plain},
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": ach / peaks["hbm_gbs"], "traffic": None,
+                     "kernel": "whole solve (every kernel of the FCG iterations and V-cycles)",
+                     "alg_bytes_per_cell_iteration": per_cell, "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 3 * (N + 2) ** 2 * 8,
+                "d2h_bytes_per_step": (N + 2) ** 2 * 8, "solve_seconds": st_e2e["seconds"],
+                "note": "Kx, Ky, u0 from pinned host memory, one multigrid-FCG solve through ops_b200_heat_solve,"
+                        " solution back to the host"},
+        "gpu_launches": int(mg[0]["launches"]), "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        base = cpu_reference_tea(args.cpu_tea_iters, threads, N)
+        if base:
+            line["cpu_baseline"] = {
+                "value": base[0] * plain[0]["iterations"], "unit": "s", "cores": threads, "kind": "reference",
+                "sample": f"reference TeaLeaf OpenMP build, same {N}^2 deck, seconds per CG iteration from runs"
+                          f" capped at 2 and {2 + args.cpu_tea_iters} iterations, times the FP64 PCG count"}
+    return line
+
+
 WORKLOADS = {"laplace": (bench_laplace, reference_laplace), "clover": (bench_clover, reference_clover),
              "clover3d": (bench_clover3d, reference_clover3d),
              "adi": (bench_adi, reference_adi), "tea": (bench_tea, reference_tea),
-             "learned": (bench_learned, reference_tea)}
+             "learned": (bench_learned, reference_tea), "mg": (bench_mg, reference_tea)}
 
 
 def main():
@@ -1001,7 +1094,7 @@ def main():
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"laplace": 200, "clover": 200, "clover3d": 100, "adi": 50, "tea": 3,
-                      "learned": 2}.get(args.workload, 20)
+                      "learned": 2, "mg": 10}.get(args.workload, 20)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_setup(args)

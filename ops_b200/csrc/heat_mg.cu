@@ -114,9 +114,20 @@ __global__ void __launch_bounds__(BX *BY) k_post_first(LV L, const float *__rest
                                                        const float *__restrict__ e, long long eP,
                                                        float *__restrict__ zout, double *__restrict__ z64,
                                                        long long fp, float omega) {
-  auto zf = [&](int xx, int yy) { return zin[(long long)yy * L.P + xx] + e[(long long)(yy >> 1) * eP + (xx >> 1)]; };
   MG_CELLS(L) {
     const long long i = (long long)y * L.P + x;
+    // the cell's aggregate value and, across the aggregate's edge on each
+    // axis, the neighbouring aggregate's (the other side shares the cell's)
+    const float *ec = e + (long long)(y >> 1) * eP + (x >> 1);
+    const float e0 = ec[0];
+    const float ew = (x & 1) ? e0 : (x > 0 ? ec[-1] : 0.f);
+    const float ee = (x & 1) ? (x < L.nx - 1 ? ec[1] : 0.f) : e0;
+    const float es = (y & 1) ? e0 : (y > 0 ? ec[-eP] : 0.f);
+    const float en = (y & 1) ? (y < L.ny - 1 ? ec[eP] : 0.f) : e0;
+    auto zf = [&](int xx, int yy) {
+      const float zv = zin[(long long)yy * L.P + xx];
+      return zv + (xx < x ? ew : xx > x ? ee : yy < y ? es : yy > y ? en : e0);
+    };
     float c;
     const float s = resid<UNIT>(L, x, y, r[i], zf, c);
     const float v = zf(x, y) + omega * s / c;
@@ -240,7 +251,16 @@ __global__ void k_coarsen(LV F, int cnx, int cny, long long cP, float *__restric
 
 Multigrid::~Multigrid() { release(); }
 
+void Multigrid::drop_graph() {
+  if (exec_) cudaGraphExecDestroy(exec_);
+  exec_ = nullptr;
+  g_r_ = nullptr;
+  g_z_ = nullptr;
+  g_s_ = nullptr;
+}
+
 void Multigrid::release() {
+  drop_graph();
   cudaFree(buf_);
   buf_ = nullptr;
   buf_elems_ = 0;
@@ -266,7 +286,7 @@ void Multigrid::setup(int nx, int ny, long long pitch, const double *Kx, const d
     y = (y + 1) / 2;
   }
   if (lv.size() != lv_.size() || lv[0].nx != (lv_.empty() ? -1 : lv_[0].nx) ||
-      lv[0].ny != (lv_.empty() ? -1 : lv_[0].ny) || elems > buf_elems_) {
+      lv[0].ny != (lv_.empty() ? -1 : lv_[0].ny) || elems > buf_elems_ || pitch != fpitch_) {
     release();
     OPSB_CUDA(cudaMalloc(&buf_, elems * sizeof(float)));
     buf_elems_ = elems;
@@ -310,6 +330,39 @@ void Multigrid::setup(int nx, int ny, long long pitch, const double *Kx, const d
 
 long long Multigrid::apply(const double *r, double *z, cudaStream_t s) {
   if (lv_.empty()) throw Error(E_STATE, "multigrid: apply before setup");
+  if (exec_ && r == g_r_ && z == g_z_ && s == g_s_) {
+    OPSB_CUDA(cudaGraphLaunch(exec_, s));
+    return g_n_;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  OPSB_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return enqueue(r, z, s);  // the caller's capture records the launches
+  drop_graph();
+  OPSB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  long long n = 0;
+  cudaGraph_t g = nullptr;
+  try {
+    n = enqueue(r, z, s);
+  } catch (...) {
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  OPSB_CUDA(cudaStreamEndCapture(s, &g));
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  OPSB_CUDA(e);
+  exec_ = ex;
+  g_r_ = r;
+  g_z_ = z;
+  g_s_ = s;
+  g_n_ = n;
+  OPSB_CUDA(cudaGraphLaunch(exec_, s));
+  return n;
+}
+
+long long Multigrid::enqueue(const double *r, double *z, cudaStream_t s) {
   const int nl = (int)lv_.size();
   const float w = kOmega;
   const dim3 blk(BX, BY);

@@ -28,7 +28,11 @@ namespace {
 constexpr int BX = 128, BY = 2, NT = BX * BY, kWarps = NT / 32;
 constexpr int kMaxBlocks = 4096;
 constexpr int kChunk = 16;          // iterations per replayed graph
-constexpr int kTargetBlocks = 148 * 8;
+// Grids are one wave of kResident blocks per SM; every kernel is held to the
+// registers that let kResident blocks stay resident (a kernel over budget
+// would run its grid in 1 1/3 waves).
+constexpr int kResident = 8;
+constexpr int kTargetBlocks = 148 * kResident;
 
 struct Scalars {
   double rro, rro_prev, pw, alpha, beta;
@@ -114,7 +118,7 @@ __device__ __forceinline__ T smvp(const T *__restrict__ Kx, const T *__restrict_
 
 // tea_leaf_cg_calc_w_reduce_kernel (tea_leaf_cg_kernels.h:8) + alpha = rro/pw.
 template <class T>
-__global__ void __launch_bounds__(NT) k_w(Geom g, const T *__restrict__ Kx, const T *__restrict__ Ky,
+__global__ void __launch_bounds__(NT, kResident) k_w(Geom g, const T *__restrict__ Kx, const T *__restrict__ Ky,
                                           const T *__restrict__ p, T *__restrict__ w, T rx, T ry, Scalars *s,
                                           double *part, unsigned *cnt) {
   __shared__ double sm[kWarps];
@@ -141,7 +145,7 @@ __global__ void __launch_bounds__(NT) k_w(Geom g, const T *__restrict__ Kx, cons
 // tea_leaf_dot_kernel (r.z), or tea_leaf_cg_calc_ur_r_reduce_kernel (r.r)
 // without preconditioner; then beta = rrn/rro and the stop test.
 template <class T, bool PREC, int STOP>
-__global__ void __launch_bounds__(NT) k_ur(Geom g, T *__restrict__ u, const T *__restrict__ p, T *__restrict__ r,
+__global__ void __launch_bounds__(NT, kResident) k_ur(Geom g, T *__restrict__ u, const T *__restrict__ p, T *__restrict__ r,
                                            const T *__restrict__ w, const T *__restrict__ Mi, T *__restrict__ z,
                                            Scalars *s, double *part, unsigned *cnt) {
   constexpr int NV = (STOP == STOP_TRUE && PREC) ? 2 : 1;
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(NT) k_ur(Geom g, T *__restrict__ u, const T *_
 
 // tea_leaf_axpby_kernel with alpha = beta, beta = 1 (tea_leaf_cg.cpp:188-214).
 template <class T>
-__global__ void __launch_bounds__(NT) k_p(Geom g, T *__restrict__ p, const T *__restrict__ z, const Scalars *s) {
+__global__ void __launch_bounds__(NT, kResident) k_p(Geom g, T *__restrict__ p, const T *__restrict__ z, const Scalars *s) {
   if (s->done) return;
   const T beta = (T)s->beta;
   HEAT_CELLS(g) {
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(NT) k_p(Geom g, T *__restrict__ p, const T *__
 // tea_leaf_common_residual_kernel + tea_leaf_norm2_kernel (tea_leaf_common.cpp:160-211):
 // r = u0 - A u, rr = r.r. The first call of a solve fixes ||r0|| and the
 // stop threshold eps * ||r0|| (tea_solve.cpp:105-114); later calls test against it.
-__global__ void __launch_bounds__(NT) k_resid(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
+__global__ void __launch_bounds__(NT, kResident) k_resid(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
                                               const double *__restrict__ u, const double *__restrict__ u0,
                                               double *__restrict__ r, double rx, double ry, double eps, Scalars *s,
                                               double *part, unsigned *cnt) {
@@ -231,7 +235,7 @@ __global__ void __launch_bounds__(NT) k_resid(Geom g, const double *__restrict__
 
 // cg_init (tea_leaf_cg.cpp:53-101): z = Mi r (or none), p = z (or r), rro = r.p.
 template <bool PREC>
-__global__ void __launch_bounds__(NT) k_init(Geom g, const double *__restrict__ r, const double *__restrict__ Mi,
+__global__ void __launch_bounds__(NT, kResident) k_init(Geom g, const double *__restrict__ r, const double *__restrict__ Mi,
                                              double *__restrict__ z, double *__restrict__ p, int max_iters,
                                              Scalars *s, double *part, unsigned *cnt) {
   __shared__ double sm[kWarps];
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(NT) k_init(Geom g, const double *__restrict__ 
 // FP64 check did not confirm. The next update is due once sqrt(rz) has fallen
 // by `delta`.
 template <bool PREC>
-__global__ void __launch_bounds__(NT) k_reinit32(Geom g, Geom g32, const double *__restrict__ r64,
+__global__ void __launch_bounds__(NT, kResident) k_reinit32(Geom g, Geom g32, const double *__restrict__ r64,
                                                  float *__restrict__ r, const float *__restrict__ Mi,
                                                  float *__restrict__ z, int first, double eps, double scale,
                                                  double delta, int max_iters, Scalars *s, double *part,
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(NT) k_reinit32(Geom g, Geom g32, const double 
 }
 
 // Reliable update, FP64 side: u += e, e = 0.
-__global__ void __launch_bounds__(NT) k_update(Geom g, Geom g32, double *__restrict__ u, float *__restrict__ e) {
+__global__ void __launch_bounds__(NT, kResident) k_update(Geom g, Geom g32, double *__restrict__ u, float *__restrict__ e) {
   HEAT_CELLS(g) {
     const long long i = (long long)y * g.pitch + x;
     const long long j = (long long)y * g32.pitch + x;
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(NT) k_update(Geom g, Geom g32, double *__restr
 }
 
 // FP32 copies of Kx, Ky, Mi over the interior and its one-cell ring.
-__global__ void __launch_bounds__(NT) k_to_float(Geom g, Geom g32, const double *__restrict__ a,
+__global__ void __launch_bounds__(NT, kResident) k_to_float(Geom g, Geom g32, const double *__restrict__ a,
                                                  const double *__restrict__ b, const double *__restrict__ c,
                                                  float *__restrict__ fa, float *__restrict__ fb,
                                                  float *__restrict__ fc) {
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(NT) k_to_float(Geom g, Geom g32, const double 
 // ---- flexible CG (Notay 2000, FCG with one-step truncation) ----------------
 // k_fw: w = A p, pw = p.w, pr = p.r -> alpha = pr / pw; a non-positive pw
 // (the preconditioned direction lost positive curvature) stops with done = 4.
-__global__ void __launch_bounds__(NT) k_fw(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
+__global__ void __launch_bounds__(NT, kResident) k_fw(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
                                            const double *__restrict__ p, const double *__restrict__ r,
                                            double *__restrict__ w, double rx, double ry, Scalars *s, double *part,
                                            unsigned *cnt) {
@@ -365,7 +369,7 @@ __global__ void __launch_bounds__(NT) k_fw(Geom g, const double *__restrict__ Kx
 }
 
 // u += alpha p, r -= alpha w, rr = r.r; stop when ||r|| < eps ||r0||.
-__global__ void __launch_bounds__(NT) k_fupd(Geom g, double *__restrict__ u, const double *__restrict__ p,
+__global__ void __launch_bounds__(NT, kResident) k_fupd(Geom g, double *__restrict__ u, const double *__restrict__ p,
                                              double *__restrict__ r, const double *__restrict__ w, Scalars *s,
                                              double *part, unsigned *cnt) {
   __shared__ double sm[kWarps];
@@ -394,7 +398,7 @@ __global__ void __launch_bounds__(NT) k_fupd(Geom g, double *__restrict__ u, con
 }
 
 // beta = -(z.w) / pw.
-__global__ void __launch_bounds__(NT) k_fzw(Geom g, const double *__restrict__ z, const double *__restrict__ w,
+__global__ void __launch_bounds__(NT, kResident) k_fzw(Geom g, const double *__restrict__ z, const double *__restrict__ w,
                                             Scalars *s, double *part, unsigned *cnt) {
   __shared__ double sm[kWarps];
   __shared__ int last;
@@ -413,7 +417,7 @@ __global__ void __launch_bounds__(NT) k_fzw(Geom g, const double *__restrict__ z
 }
 
 // p = z + beta p, or p = z on a restart.
-__global__ void __launch_bounds__(NT) k_fp(Geom g, double *__restrict__ p, const double *__restrict__ z,
+__global__ void __launch_bounds__(NT, kResident) k_fp(Geom g, double *__restrict__ p, const double *__restrict__ z,
                                            const Scalars *s, int restart) {
   const double beta = restart ? 0.0 : s->beta;
   HEAT_CELLS(g) {
@@ -423,7 +427,7 @@ __global__ void __launch_bounds__(NT) k_fp(Geom g, double *__restrict__ p, const
 }
 
 // z = Mi r (Jacobi).
-__global__ void __launch_bounds__(NT) k_jacobi(Geom g, const double *__restrict__ Mi, const double *__restrict__ r,
+__global__ void __launch_bounds__(NT, kResident) k_jacobi(Geom g, const double *__restrict__ Mi, const double *__restrict__ r,
                                                double *__restrict__ z) {
   HEAT_CELLS(g) {
     const long long i = (long long)y * g.pitch + x;
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(Geom g, const double *__restrict_
 
 // tea_leaf_common_init_diag_init_kernel (tea_leaf_common_kernels.h:38):
 // Mi = 1 / (1 + ry (Ky(0,1) + Ky(0,0)) + rx (Kx(1,0) + Kx(0,0))) on the interior.
-__global__ void __launch_bounds__(NT) k_diag(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
+__global__ void __launch_bounds__(NT, kResident) k_diag(Geom g, const double *__restrict__ Kx, const double *__restrict__ Ky,
                                              double rx, double ry, double *__restrict__ Mi) {
   HEAT_CELLS(g) {
     const long long i = (long long)y * g.pitch + x;
