@@ -14,6 +14,9 @@ Pipeline, all arithmetic on the GPU through the library's C-ABI:
      PCG residuals stalls FCG once the residuals leave that distribution),
   4. flexible CG with the trained network as preconditioner, falling back to
      Jacobi-PCG when the network stops helping.
+FCG_MG runs the same flexible CG with the library's native (non-learned)
+aggregation-multigrid V-cycle as preconditioner, the baseline the learned one
+is measured against; `mg_apply` applies that V-cycle once.
 Device buffers are torch CUDA tensors (allocation only)."""
 import ctypes
 
