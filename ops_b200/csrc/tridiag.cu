@@ -41,6 +41,8 @@ struct Sys {
   int nl0, nl1;    // line counts along the two non-solve dimensions (fastest first)
   long long ss;    // stride along the solve dimension (elements)
   long long s0, s1;
+  long long line0 = 0;  // line kernel: first line number of this system in the launch
+  long long scr0 = 0;   // line kernel: first scratch element of this system
 };
 
 struct Work {
@@ -318,15 +320,164 @@ __global__ void __launch_bounds__(kTileThreads, kCtasPerSm) trid_tile_kernel(con
   }
 }
 
+// Lines strided along the solve dimension and contiguous across lines (the
+// y and z sweeps): one thread per line runs the Thomas algorithm straight
+// from HBM, neighbouring threads reading neighbouring lines so every access
+// coalesces. The forward pass keeps c' and d' in a scratch array laid out
+// row-major over the system's lines (coalesced too) and the backward pass
+// reads them back: 72 bytes per FP64 unknown (80 for _Inc) against the
+// tile kernel's 40, but no staging, no barriers and several rows of loads in
+// flight per thread, which is what the strided sweeps lacked. The
+// rows in flight are 4 in FP64 and 8 in FP32 (one 32-byte sector of each
+// line per array; measured best for the 256^3 sweeps). The
+// arithmetic is the textbook Thomas elimination:
+//   c'_0 = c_0 / b_0, d'_0 = d_0 / b_0; for i >= 1, r = 1 / (b_i - a_i c'_{i-1}),
+//   c'_i = c_i r, d'_i = (d_i - a_i d'_{i-1}) r; x_{n-1} = d'_{n-1},
+//   x_i = d'_i - c'_i x_{i+1}.
+constexpr int kLineThreads = 128;
+template <class T>
+constexpr int line_unroll() { return sizeof(T) == 4 ? 8 : 4; }
+
+template <class T>
+__global__ void __launch_bounds__(kLineThreads) trid_line_kernel(const Sys *__restrict__ sys, int nsys,
+                                                                 long long total, T *__restrict__ scr_c,
+                                                                 T *__restrict__ scr_d) {
+  constexpr int kLineUnroll = line_unroll<T>();
+  for (long long g = (long long)blockIdx.x * kLineThreads + threadIdx.x; g < total;
+       g += (long long)gridDim.x * kLineThreads) {
+    int lo = 0, hi = nsys - 1;  // last system whose first line is <= g
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sys[mid].line0 <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    const Sys &s = sys[lo];
+    const long long k = g - s.line0, nlines = (long long)s.nl0 * s.nl1;
+    const int n = s.n;
+    const long long base = (k % s.nl0) * s.s0 + (k / s.nl0) * s.s1, ss = s.ss;
+    const T *a = reinterpret_cast<const T *>(s.a) + base;
+    const T *b = reinterpret_cast<const T *>(s.b) + base;
+    const T *c = reinterpret_cast<const T *>(s.c) + base;
+    const T *d = reinterpret_cast<const T *>(s.d) + base;
+    T *x = reinterpret_cast<T *>(s.d) + base;
+    T *u = s.u ? reinterpret_cast<T *>(s.u) + base : nullptr;
+    T *cp = scr_c + s.scr0 + k, *dp = scr_d + s.scr0 + k;
+    if (n <= 0) continue;
+    T r = recip(b[0]);
+    T pc = c[0] * r, pd = d[0] * r;
+    cp[0] = pc;
+    dp[0] = pd;
+    int i = 1;
+    for (; i + kLineUnroll <= n; i += kLineUnroll) {
+      T ai[kLineUnroll], bi[kLineUnroll], ci[kLineUnroll], di[kLineUnroll];
+#pragma unroll
+      for (int j = 0; j < kLineUnroll; j++) {
+        const long long q = (long long)(i + j) * ss;
+        ai[j] = a[q];
+        bi[j] = b[q];
+        ci[j] = c[q];
+        di[j] = d[q];
+      }
+#pragma unroll
+      for (int j = 0; j < kLineUnroll; j++) {
+        r = recip(bi[j] - ai[j] * pc);
+        pc = ci[j] * r;
+        pd = (di[j] - ai[j] * pd) * r;
+        cp[(long long)(i + j) * nlines] = pc;
+        dp[(long long)(i + j) * nlines] = pd;
+      }
+    }
+    for (; i < n; i++) {
+      const long long q = (long long)i * ss;
+      const T ai = a[q];
+      r = recip(b[q] - ai * pc);
+      pc = c[q] * r;
+      pd = (d[q] - ai * pd) * r;
+      cp[(long long)i * nlines] = pc;
+      dp[(long long)i * nlines] = pd;
+    }
+    T xv = pd;  // x_{n-1}
+    {
+      const long long q = (long long)(n - 1) * ss;
+      if (u) u[q] += xv;
+      else x[q] = xv;
+    }
+    int j = n - 2;
+    for (; j - kLineUnroll + 1 >= 0; j -= kLineUnroll) {
+      T cj[kLineUnroll], dj[kLineUnroll];
+#pragma unroll
+      for (int t = 0; t < kLineUnroll; t++) {
+        cj[t] = cp[(long long)(j - t) * nlines];
+        dj[t] = dp[(long long)(j - t) * nlines];
+      }
+#pragma unroll
+      for (int t = 0; t < kLineUnroll; t++) {
+        xv = dj[t] - cj[t] * xv;
+        const long long q = (long long)(j - t) * ss;
+        if (u) u[q] += xv;
+        else x[q] = xv;
+      }
+    }
+    for (; j >= 0; j--) {
+      xv = dp[(long long)j * nlines] - cp[(long long)j * nlines] * xv;
+      const long long q = (long long)j * ss;
+      if (u) u[q] += xv;
+      else x[q] = xv;
+    }
+  }
+}
+
 // Device copies of the work description, grown as needed.
 struct Buffers {
   Sys *sys = nullptr;
   Work *work = nullptr;
   size_t sys_cap = 0, work_cap = 0;
+  void *scr = nullptr;  // line kernel scratch (c' then d')
+  size_t scr_bytes = 0;
 };
 Buffers &buffers() {
   static Buffers b;
   return b;
+}
+
+// The y/z sweeps (solve dimension strided, lines contiguous) by the line
+// kernel; returns false when some system does not have that shape.
+template <class T>
+bool launch_lines(std::vector<Sys> systems, cudaStream_t stream, long long *kernels) {
+  long long lines = 0, unknowns = 0;
+  for (Sys &s : systems) {
+    if (s.ss == 1 || s.s0 != 1) return false;
+    s.line0 = lines;
+    s.scr0 = unknowns;
+    const long long nl = (long long)s.nl0 * s.nl1;
+    lines += s.n > 0 ? nl : 0;
+    unknowns += s.n > 0 ? nl * s.n : 0;
+  }
+  std::vector<Sys> live;  // systems with no rows or no lines take no part
+
+  for (const Sys &s : systems)
+    if (s.n > 0 && (long long)s.nl0 * s.nl1 > 0) live.push_back(s);
+  if (live.empty()) return true;
+  Buffers &B = buffers();
+  if (B.sys_cap < live.size()) {
+    if (B.sys) cudaFree(B.sys);
+    B.sys_cap = std::max<size_t>(live.size(), 64);
+    OPSB_CUDA(cudaMalloc(&B.sys, B.sys_cap * sizeof(Sys)));
+  }
+  const size_t need = 2 * (size_t)unknowns * sizeof(T);
+  if (B.scr_bytes < need) {
+    if (B.scr) cudaFree(B.scr);
+    B.scr = nullptr;
+    OPSB_CUDA(cudaMalloc(&B.scr, need));
+    B.scr_bytes = need;
+  }
+  OPSB_CUDA(cudaMemcpyAsync(B.sys, live.data(), live.size() * sizeof(Sys), cudaMemcpyHostToDevice, stream));
+  T *sc = static_cast<T *>(B.scr), *sd = sc + unknowns;
+  const int grid = (int)std::min<long long>((lines + kLineThreads - 1) / kLineThreads, 148LL * 16);
+  trid_line_kernel<T><<<grid, kLineThreads, 0, stream>>>(B.sys, (int)live.size(), lines, sc, sd);
+  OPSB_CUDA(cudaGetLastError());
+  if (kernels) (*kernels)++;
+  return true;
 }
 
 template <class T>
@@ -335,6 +486,7 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
   int maxn = 0;
   for (const Sys &s : systems) maxn = std::max(maxn, s.n);
   if (maxn == 0) return;
+  if (launch_lines<T>(systems, stream, kernels)) return;
   // lines per work item: the largest power of two (<= 64) whose tiles fit
   int L = 64;
   while (L > 1 && tile_smem<T>(L, maxn) > kTileSmem) L /= 2;
