@@ -52,11 +52,21 @@ class Multigrid {
   void setup(int nx, int ny, long long pitch, const double *Kx, const double *Ky, double rx, double ry,
              cudaStream_t s);
   // z = M r on the interior (FP64, `pitch` of the setup); returns the kernels
-  // launched.
+  // launched. The cycle's launches are captured into a CUDA graph on first
+  // use for a given (r, z, stream) and replayed from it afterwards; the
+  // graph reads the hierarchy through its pointers, so a later setup of the
+  // same shape (new coefficients, same storage) keeps it valid.
   long long apply(const double *r, double *z, cudaStream_t s);
   int levels() const { return (int)lv_.size(); }
 
  private:
+  long long enqueue(const double *r, double *z, cudaStream_t s);
+  void drop_graph();
+  cudaGraphExec_t exec_ = nullptr;
+  const double *g_r_ = nullptr;
+  double *g_z_ = nullptr;
+  cudaStream_t g_s_ = nullptr;
+  long long g_n_ = 0;
   struct Level {
     int nx = 0, ny = 0;
     long long pitch = 0;  // elements; rows of the face arrays hold nx + 1
