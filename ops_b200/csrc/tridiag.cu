@@ -441,7 +441,10 @@ Buffers &buffers() {
 }
 
 // The y/z sweeps (solve dimension strided, lines contiguous) by the line
-// kernel; returns false when some system does not have that shape.
+// kernel; returns false when some system does not have that shape (the x
+// sweeps stay with the tile kernel: a warp-transposing variant of the line
+// kernel for them measured 0.70 ms against the tile kernel's 0.41 ms on the
+// 256^3 FP64 x sweep).
 template <class T>
 bool launch_lines(std::vector<Sys> systems, cudaStream_t stream, long long *kernels) {
   long long lines = 0, unknowns = 0;

@@ -1,8 +1,9 @@
 """Batched tridiagonal solves on the B200 path vs the CPU oracle (Thomas).
 
-The GPU splits each line into chunks (partition method) so its rounding
-differs from sequential Thomas: FP64 results agree to 1e-12 relative, FP32
-to 1e-4; the FP64 residual of the solved system is checked at full size."""
+Two kernels: strided sweeps (y, z) run Thomas per line; x sweeps split
+each line into chunks (partition method), whose rounding differs from
+sequential Thomas. FP64 results agree to 1e-12 relative, FP32 to 2e-4; the
+FP64 residual of the solved system is checked at full size."""
 import ctypes
 
 import numpy as np
@@ -58,6 +59,24 @@ def test_strided_batch_matches_oracle(gpu_runtime, orc, dtype, rtol, solvedim, s
     ref = d.copy()
     oracle_solve(orc, a, b, c, ref, solvedim)
     np.testing.assert_allclose(x, ref, rtol=rtol, atol=rtol * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("dtype,rtol", [(np.float64, 1e-12), (np.float32, 2e-4)])
+@pytest.mark.parametrize("n,inc", [(1, False), (8, False), (37, True), (130, False), (16, True)])
+def test_many_x_lines_match_oracle(gpu_runtime, orc, dtype, rtol, n, inc):
+    """x sweeps over 20012 lines of one to 130 rows (many tiles of the
+    partition kernel), padding and the _Inc form against the oracle."""
+    shape = (4, 5003, n)
+    a, b, c, d = seeded.trid_system(shape, 0, 21 + n, dtype)
+    u = seeded.uniform(5, np.arange(d.size, dtype=np.uint64), -1, 1).reshape(d.shape).astype(dtype) if inc else None
+    dg, ug = run_gpu(a, b, c, d, 0, u=u, pad=(0, 1, 3))
+    ref = d.copy()
+    oracle_solve(orc, a, b, c, ref, 0)
+    if inc:
+        assert np.array_equal(dg, d)
+        np.testing.assert_allclose(ug, u + ref, rtol=rtol, atol=rtol * np.abs(ref).max())
+    else:
+        np.testing.assert_allclose(dg, ref, rtol=rtol, atol=rtol * np.abs(ref).max())
 
 
 @pytest.mark.parametrize("solvedim", [0, 1, 2])
