@@ -69,8 +69,18 @@ def _iarr(v):
     return a
 
 
+# what the diagnostic and timing output report: the diagnostics level given
+# to ops_init and the blocks and dats declared since
+_STATE = {"diags": 0, "blocks": [], "dats": []}
+
+
 def ops_init(device=0, diags=0):
+    """ops_init. As in the reference, diags > 1 times every loop (per-kernel
+    CUDA-event timing, read by ops_timing_output) and diags > 2 enables
+    ops_diagnostic_output."""
     check(lib().ops_b200_init(device, diags))
+    _STATE["diags"] = diags
+    check(lib().ops_b200_set_kernel_timing(1 if diags > 1 else 0))
 
 
 def ops_exit():
@@ -78,7 +88,9 @@ def ops_exit():
 
 
 def ops_decl_block(dims, name):
-    return ops_block(check(lib().ops_b200_decl_block(dims, name.encode())), dims, name)
+    b = ops_block(check(lib().ops_b200_decl_block(dims, name.encode())), dims, name)
+    _STATE["blocks"].append(b)
+    return b
 
 
 def ops_decl_dat(block, dim, size, base, d_m, d_p, data, type_, name, stride=None):
@@ -92,7 +104,10 @@ def ops_decl_dat(block, dim, size, base, d_m, d_p, data, type_, name, stride=Non
     h = check(lib().ops_b200_decl_dat(block.index, dim, _iarr(size), _iarr(base), _iarr(d_m), _iarr(d_p),
                                       buf.ctypes.data if buf is not None else None, ts, type_.encode(),
                                       name.encode()))
-    return ops_dat(h, block, dim, size, d_m, d_p, type_, name)
+    d = ops_dat(h, block, dim, size, d_m, d_p, type_, name)
+    d.base = list(base)
+    _STATE["dats"].append(d)
+    return d
 
 
 def ops_decl_stencil(dims, points, sten, name):
@@ -279,10 +294,6 @@ def reset_counters():
     check(lib().ops_b200_reset_counters())
 
 
-__all__ = [n for n in dir() if n.startswith("ops_")] + ["OpsError", "set_option", "counters", "reset_counters",
-                                                          "set_kernel_timing", "kernel_time", "clear_kernel_timing"]
-
-
 def ops_tridMultiDimBatch(ndim, solvedim, rng, a, b, c, d, params=None):
     """ops_tridMultiDimBatch: solve along `solvedim` over `rng`, result in d."""
     check(lib().ops_b200_tridMultiDimBatch(ndim, solvedim, _iarr(rng), a.index, b.index, c.index, d.index))
@@ -307,3 +318,139 @@ def trid_batch(elem_size, solvedim, systems, stream=None):
             t.dims[k] = s["dims"][k] if k < t.ndim else 1
             t.pads[k] = s["pads"][k] if k < t.ndim else 1
     check(lib().ops_b200_trid_batch(elem_size, solvedim, len(systems), arr, stream))
+
+
+# ---- output, timing and host-data calls of the reference's single-process
+# backend (ops/c/src/core/ops_dummy_singlenode.cpp, ops_lib_core.cpp)
+
+def ops_printf(fmt, *args):
+    """ops_printf (ops_dummy_singlenode.cpp:413): printf on the one process."""
+    print(fmt % args if args else fmt, end="", flush=True)
+
+
+def ops_fprintf(stream, fmt, *args):
+    """ops_fprintf (ops_dummy_singlenode.cpp:457): fprintf to an open text stream."""
+    stream.write(fmt % args if args else fmt)
+
+
+def ops_partition(routine=None, opts=None):
+    """ops_partition / ops_partition_opts (ops_dummy_singlenode.cpp:892-899):
+    nothing to partition with one process on one GPU."""
+    return None
+
+
+def ops_timing_output(stream=None):
+    """ops_timing_output (ops_lib_core.cpp:1468-1626): with diags > 1, one
+    line per loop kernel (name, launches, mean seconds per call with its
+    spread, MPI time, bandwidth) and the total kernel time. Here every launch
+    is timed with CUDA events on the runtime stream; the spread and the MPI
+    time are 0 (the per-launch times are not kept, and there is no MPI), and
+    the bandwidth is the loop's algorithmic bytes over its time in GiB/s,
+    the reference's unit."""
+    import sys
+    stream = stream or sys.stdout
+    if _STATE["diags"] <= 1:
+        return
+    st = kernel_stats()
+    if not st:
+        return
+    width = max(len(k) for k in st)
+    stream.write("\n\n%s  Count Time     MPI-time     Bandwidth(GB/s)\n" % "Name".ljust(width))
+    stream.write("-" * (width + 31) + "\n")
+    total = 0.0
+    for name, (count, ms, byt) in st.items():
+        t = ms * 1e-3
+        bw = byt / (t * 1024 ** 3) if t > 0 else 0.0
+        stream.write("%s%-5d %-6f (%-6f) %-6f (%-6f)  %-13.2f\n" % (name.ljust(width + 2), count, t, 0.0, 0.0, 0.0, bw))
+        total += t
+    stream.write("Total kernel time: %g\n" % total)
+
+
+def ops_diagnostic_output():
+    """ops_diagnostic_output (ops_lib_core.cpp:1214-1262): with diags > 2, the
+    declared blocks and dats with their sizes, bases, halo depths and memory."""
+    if _STATE["diags"] <= 2:
+        return
+    ops_printf("\n OPS diagnostic output\n --------------------\n")
+    ops_printf("\n block dimension\n -------------------\n")
+    for b in _STATE["blocks"]:
+        ops_printf(" %15s %15dD \n", b.name, b.dims)
+    ops_printf("\n %15s %15s %15s %10s %10s %10s %15s %15s\n", "data", "item/point", "[block_size]", "[base]",
+               "[d_m]", "[d_p]", "memory(MBytes)", "block")
+    ops_printf(" " + "-" * 73 + "\n")
+    tot = 0.0
+    for d in _STATE["dats"]:
+        nd = d.block.dims
+        mem = float(np.prod(d.size[:nd])) * d.dim * np.dtype(d.dtype).itemsize
+        tot += mem
+        br = lambda v: "".join("[%d]" % x for x in v[:nd])  # noqa: E731
+        ops_printf(" %15s %15d %s %s %s %s  %15.3f  %15s\n", d.name, d.dim, br(d.size), br(getattr(d, "base", [0] * nd)),
+                   br(d.d_m), br(d.d_p), mem / (1024.0 * 1024.0), d.block.name)
+    ops_printf(" Total Memory Allocated for ops_dats (GBytes) : %.3f\n", tot / (1024.0 ** 3))
+
+
+def ops_get_data(dat):
+    """ops_get_data (ops_lib_core.cpp:2366): the reference copies the device
+    copy of the dat to its host storage. Dats here live on the device only;
+    this returns the host copy of the full extent (as ops_dat_fetch_data)."""
+    return ops_dat_fetch_data(dat)
+
+
+def ops_put_data(dat, data):
+    """ops_put_data (ops_lib_core.cpp:2382): the reference uploads the dat's
+    host storage to the device; here the host data is passed in (the full
+    extent, as ops_dat_set_data)."""
+    ops_dat_set_data(dat, data)
+
+
+def ops_print_dat_to_txtfile(dat, file_name):
+    """ops_print_dat_to_txtfile (ops_lib_core.cpp:1272-1420): appends the
+    dat's name, dim, extent, element size and every value of the full extent
+    (x fastest; FP64 as " %3.10lf", FP32 as "%e ", integers as "%d ") to a
+    text file, one row of x per line."""
+    vals = ops_dat_fetch_data(dat)
+    nd = dat.block.dims
+    es = np.dtype(dat.dtype).itemsize
+    with open(file_name, "a") as fp:
+        fp.write("ops_dat:  %s \n" % dat.name)
+        fp.write("ops_dat dim:  %d \n" % dat.dim)
+        fp.write("block Dims : %d " % nd + "".join("[%d]" % x for x in dat.size[:nd]) + "\n")
+        fp.write("elem size %d \n" % (es * dat.dim))
+        if np.issubdtype(vals.dtype, np.floating):
+            fmt = " %3.10lf" if vals.dtype == np.float64 else "%e "
+        else:
+            fmt = "%d "
+        rows = vals.reshape(-1, dat.size[0] * dat.dim)
+        for row in rows:
+            fp.write("".join(fmt % v for v in row) + "\n")
+
+
+class ops_tridsolver_params:
+    """ops_tridsolver_params (ops/c/include/ops_tridiag.h:45-72): strategy and
+    tuning of Tridsolver's multi-process solves. The reference's
+    single-process backends ignore every setter (ops_tridiag.cpp:48-76); so
+    does this one. The values given are kept for callers that read them
+    back (None until set)."""
+    GATHER_SCATTER, ALLGATHER, JACOBI, PCR, LATENCY_HIDING_INTERLEAVED, LATENCY_HIDING_TWO_STEP = range(6)
+
+    def __init__(self, block, strategy=None):
+        self.block, self.strategy = block, strategy
+        self.jacobi = self.batch_size = self.cuda_opts = self.cuda_sync = None
+
+    def set_jacobi_params(self, rtol, atol, maxiter):
+        self.jacobi = (rtol, atol, maxiter)
+
+    def set_batch_size(self, batch_size):
+        self.batch_size = batch_size
+
+    def set_cuda_opts(self, opt_x, opt_y, opt_z):
+        self.cuda_opts = (opt_x, opt_y, opt_z)
+
+    def set_cuda_sync(self, sync):
+        self.cuda_sync = sync
+
+
+__all__ = [n for n in dir() if n.startswith("ops_")] + ["OpsError", "set_option", "counters", "reset_counters",
+                                                          "set_kernel_timing", "kernel_time", "clear_kernel_timing",
+                                                          "trid_batch", "OPS_READ", "OPS_WRITE", "OPS_RW", "OPS_INC",
+                                                          "OPS_MIN", "OPS_MAX", "OPS_HOST", "OPS_DEVICE"]

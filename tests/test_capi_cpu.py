@@ -48,3 +48,23 @@ def test_calls_before_init_are_rejected():
     assert b"ops_b200_init" in L.ops_b200_last_error()
     assert L.ops_b200_has_kernel(b"laplace2d/apply_stencil") == 1
     assert L.ops_b200_has_kernel(b"nope/none") == 0
+
+
+def test_single_process_api_calls_without_gpu(capsys):
+    """ops_printf / ops_fprintf / ops_partition / ops_tridsolver_params need
+    no device: printing, a no-op partition, setters that steer nothing."""
+    import io
+
+    from ops_b200 import ops as O
+    O.ops_printf("%d cells, %s\n", 42, "ok")
+    assert capsys.readouterr().out == "42 cells, ok\n"
+    s = io.StringIO()
+    O.ops_fprintf(s, "x=%.2f\n", 1.5)
+    assert s.getvalue() == "x=1.50\n"
+    assert O.ops_partition("") is None
+    p = O.ops_tridsolver_params(None, O.ops_tridsolver_params.PCR)
+    p.set_jacobi_params(1e-10, 1e-12, 5)
+    p.set_batch_size(64)
+    p.set_cuda_opts(1, 2, 3)
+    p.set_cuda_sync(0)
+    assert (p.strategy, p.jacobi, p.batch_size, p.cuda_opts, p.cuda_sync) == (3, (1e-10, 1e-12, 5), 64, (1, 2, 3), 0)
