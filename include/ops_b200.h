@@ -391,7 +391,7 @@ typedef struct ops_b200_heat_stats {
   int iterations;          /* CG iterations (method 0: as TeaLeaf prints them) */
   int updates;             /* reliable updates (method 2) */
   int converged;
-  int fallbacks;           /* preconditioner -> Jacobi switches (methods 3, 5) */
+  int fallbacks;           /* switches to the fallback preconditioner (methods 3, 5, 6) */
   double initial_residual; /* ||u0 - A u|| at entry */
   double final_residual;   /* ||u0 - A u|| at exit, FP64 */
   double seconds;          /* device time of the solve */
@@ -404,10 +404,13 @@ typedef struct ops_b200_heat_stats {
 #define OPS_B200_HEAT_FCG_LEARNED 3  /* flexible CG, learned preconditioner `net`, Jacobi fallback */
 #define OPS_B200_HEAT_FCG_JACOBI 4   /* the same flexible CG with Jacobi (no network) */
 #define OPS_B200_HEAT_FCG_MG 5       /* the same flexible CG, one native multigrid V-cycle per iteration */
+#define OPS_B200_HEAT_FCG_LEARNED_MG 6 /* flexible CG, M(r) = V-cycle(r) + the correction of network `net`
+                                          (trained on targets e - V-cycle(r)); falls back to the V-cycle */
 
-/* Solves A u = u0. `net` names a learned preconditioner (method 3); window:
- * methods 3 and 5 fall back to Jacobi when ||r|| has not halved over `window`
- * iterations (0 = only on lost positive curvature). r_out (device, may be
+/* Solves A u = u0. `net` names a learned preconditioner (methods 3, 6);
+ * window: methods 3, 5 and 6 fall back (to Jacobi; method 6 to the V-cycle
+ * alone) when ||r|| has not halved over `window` iterations (0 = only on
+ * lost positive curvature). r_out (device, may be
  * NULL) receives u0 - A u at exit. Synchronous on `stream`. Not reentrant:
  * one solve at a time per process (a shared workspace is kept per size). */
 int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, double eps, int max_iters, int window,

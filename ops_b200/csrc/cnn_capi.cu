@@ -71,6 +71,7 @@ struct HeatWorkspace {
   long long pitch = 0;
   double *buf = nullptr;
   double *r = nullptr, *w = nullptr, *p = nullptr, *z = nullptr, *Mi = nullptr;
+  double *t = nullptr;  // the multigrid part of the learned-multigrid preconditioner
   heat::Solver solver;
   heat::Multigrid mg;
   ~HeatWorkspace() { cudaFree(buf); }
@@ -79,15 +80,32 @@ struct HeatWorkspace {
     cudaFree(buf);
     buf = nullptr;
     const size_t one = (size_t)pt * (y + 2);
-    OPSB_CUDA(cudaMalloc(&buf, 5 * one * sizeof(double)));
-    OPSB_CUDA(cudaMemsetAsync(buf, 0, 5 * one * sizeof(double), s));
-    double **f[5] = {&r, &w, &p, &z, &Mi};
-    for (int k = 0; k < 5; k++) *f[k] = buf + k * one + pt + 1;
+    OPSB_CUDA(cudaMalloc(&buf, 6 * one * sizeof(double)));
+    OPSB_CUDA(cudaMemsetAsync(buf, 0, 6 * one * sizeof(double), s));
+    double **f[6] = {&r, &w, &p, &z, &Mi, &t};
+    for (int k = 0; k < 6; k++) *f[k] = buf + k * one + pt + 1;
     nx = x;
     ny = y;
     pitch = pt;
   }
 };
+
+// z = z - r / D + t on the interior, D = diag(A) computed as the network
+// computes it (lmg.cu `coef`): the network's output r / D + s y becomes the
+// correction s y added to the multigrid cycle's t. With an untrained network
+// (y = 0) the result is t exactly.
+__global__ void k_learned_mg_combine(int nx, int ny, long long pitch, const double *__restrict__ Kx,
+                                     const double *__restrict__ Ky, double rx, double ry,
+                                     const double *__restrict__ r, const double *__restrict__ t,
+                                     double *__restrict__ z) {
+  for (int y = blockIdx.y * blockDim.y + threadIdx.y; y < ny; y += gridDim.y * blockDim.y)
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nx; x += gridDim.x * blockDim.x) {
+      const long long i = (long long)y * pitch + x;
+      const double a = rx * Kx[i], b = rx * Kx[i + 1], c = ry * Ky[i], d = ry * Ky[i + pitch];
+      const double D = 1.0 + a + b + c + d;
+      z[i] = (z[i] - r[i] / D) + t[i];
+    }
+}
 
 std::mutex g_mu;
 cudaStream_t own_stream() {
@@ -139,7 +157,7 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
   return capi_guard([&] {
     if (!sys || !sys->Kx || !sys->Ky || !sys->u0 || !sys->u) throw Error(E_ARG, "heat system: null field");
     if (sys->nx < 1 || sys->ny < 1 || sys->pitch < sys->nx + 2) throw Error(E_ARG, "heat system: bad shape");
-    if (method < OPS_B200_HEAT_PCG || method > OPS_B200_HEAT_FCG_MG) throw Error(E_ARG, "heat system: method");
+    if (method < OPS_B200_HEAT_PCG || method > OPS_B200_HEAT_FCG_LEARNED_MG) throw Error(E_ARG, "heat system: method");
     if (!(eps > 0.0) || max_iters < 0) throw Error(E_ARG, "heat system: eps > 0 and max_iters >= 0 required");
     std::lock_guard<std::mutex> lk(g_mu);
     // the iteration chunks are replayed from CUDA graphs, which cannot be
@@ -174,8 +192,8 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
       if (sys->nx < 1) throw Error(E_ARG, "heat system: bad shape");
       ws.solver.pcg_mixed(f, sys->rx, sys->ry, true, eps, 0.1, max_iters, s, &st);
     } else {
-      heat::Solver::Precond M;
-      if (method == OPS_B200_HEAT_FCG_LEARNED) {
+      heat::Solver::Precond M, fallback;
+      if (method == OPS_B200_HEAT_FCG_LEARNED || method == OPS_B200_HEAT_FCG_LEARNED_MG) {
         lmg::Net *np = &net_of(net);
         if (sys->nx % 8 || sys->ny % 8) throw Error(E_ARG, "learned preconditioner: nx and ny must be multiples of 8");
         lmg::Fields lf;
@@ -194,12 +212,29 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
           np->apply(lf, z, ss);
           return np->launches() - before;
         };
+        if (method == OPS_B200_HEAT_FCG_LEARNED_MG) {
+          heat::Multigrid *mg = &ws.mg;
+          mg->setup(sys->nx, sys->ny, sys->pitch, sys->Kx, sys->Ky, sys->rx, sys->ry, s);
+          fallback = [mg](const double *r, double *z, cudaStream_t ss) -> long long { return mg->apply(r, z, ss); };
+          const heat::Solver::Precond net_part = M;
+          const int nx = sys->nx, ny = sys->ny;
+          const long long pitch = sys->pitch;
+          const double *Kx = sys->Kx, *Ky = sys->Ky, rx = sys->rx, ry = sys->ry;
+          double *t = ws.t;
+          M = [=](const double *r, double *z, cudaStream_t ss) -> long long {
+            long long n = net_part(r, z, ss) + mg->apply(r, t, ss);
+            const dim3 blk(128, 2), grd((nx + 127) / 128, std::min((ny + 1) / 2, 4096));
+            k_learned_mg_combine<<<grd, blk, 0, ss>>>(nx, ny, pitch, Kx, Ky, rx, ry, r, t, z);
+            OPSB_CUDA(cudaGetLastError());
+            return n + 1;
+          };
+        }
       } else if (method == OPS_B200_HEAT_FCG_MG) {
         heat::Multigrid *mg = &ws.mg;
         mg->setup(sys->nx, sys->ny, sys->pitch, sys->Kx, sys->Ky, sys->rx, sys->ry, s);
         M = [mg](const double *r, double *z, cudaStream_t ss) -> long long { return mg->apply(r, z, ss); };
       }
-      ws.solver.fcg(f, sys->rx, sys->ry, eps, max_iters, M, window, s, &st);
+      ws.solver.fcg(f, sys->rx, sys->ry, eps, max_iters, M, window, s, &st, fallback ? &fallback : nullptr);
     }
     OPSB_CUDA(cudaEventRecord(e1, s));
     OPSB_CUDA(cudaEventSynchronize(e1));
@@ -209,7 +244,7 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
     cudaEventDestroy(e1);
     double fin = st.true_residual;
     if (r_out) fin = ws.solver.residual(f, sys->rx, sys->ry, r_out, s);
-    if (method == OPS_B200_HEAT_FCG_LEARNED) {
+    if (method == OPS_B200_HEAT_FCG_LEARNED || method == OPS_B200_HEAT_FCG_LEARNED_MG) {
       int err = 0;
       OPSB_CUDA(cudaMemcpy(&err, cnn::error_word(), sizeof(int), cudaMemcpyDeviceToHost));
       if (err) throw Error(E_TIMEOUT, "learned preconditioner: a convolution pipeline wait expired");

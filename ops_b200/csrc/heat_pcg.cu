@@ -762,7 +762,7 @@ double Solver::residual(const Field2D &f, double rx, double ry, double *outp, cu
 }
 
 void Solver::fcg(const Field2D &f, double rx, double ry, double eps, int max_iters, const Precond &M, int window,
-                 cudaStream_t st, SolveStats *out) {
+                 cudaStream_t st, SolveStats *out, const Precond *fallback) {
   validate(f);
   Impl &m = *m_;
   m.ensure_base();
@@ -779,6 +779,8 @@ void Solver::fcg(const Field2D &f, double rx, double ry, double eps, int max_ite
   auto precond = [&] {
     if (learned) {
       launches_ += M(f.r, f.z, st);
+    } else if (fallback && *fallback) {
+      launches_ += (*fallback)(f.r, f.z, st);
     } else {
       k_jacobi<<<grid, block, 0, st>>>(g, f.Mi, f.r, f.z);
       launches_ += 1;

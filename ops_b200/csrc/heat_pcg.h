@@ -60,8 +60,11 @@ class Solver {
                  cudaStream_t s, SolveStats *st);
   // z = M(r) on the interior of the solve's fields; returns kernels launched.
   using Precond = std::function<long long(const double *r, double *z, cudaStream_t s)>;
+  // On a restart (p.w <= 0, or no halving of ||r|| over `window`
+  // iterations) the solve continues with `fallback` when one is given, else
+  // with Jacobi.
   void fcg(const Field2D &f, double rx, double ry, double eps, int max_iters, const Precond &M, int window,
-           cudaStream_t s, SolveStats *st);
+           cudaStream_t s, SolveStats *st, const Precond *fallback = nullptr);
   // Mi = 1 / diag(A) on the interior (tea_leaf_common_init_diag_init_kernel).
   void diag(const Field2D &f, double rx, double ry, cudaStream_t s);
   // out = u0 - A u on the interior; returns ||out||.

@@ -16,7 +16,9 @@ Pipeline, all arithmetic on the GPU through the library's C-ABI:
      Jacobi-PCG when the network stops helping.
 FCG_MG runs the same flexible CG with the library's native (non-learned)
 aggregation-multigrid V-cycle as preconditioner, the baseline the learned one
-is measured against; `mg_apply` applies that V-cycle once.
+is measured against; `mg_apply` applies that V-cycle once. FCG_LEARNED_MG
+puts the two together: M(r) = V-cycle(r) + s y, the network trained (`fit`
+with base="mg") on the error the V-cycle leaves, e - V-cycle(r).
 Device buffers are torch CUDA tensors (allocation only)."""
 import ctypes
 
@@ -25,7 +27,7 @@ import numpy as np
 from . import seeded
 from ._lib import HeatBatch, HeatStats, HeatSystem, check, lib
 
-PCG, PCG_TRUE, MIXED, FCG_LEARNED, FCG_JACOBI, FCG_MG = 0, 1, 2, 3, 4, 5
+PCG, PCG_TRUE, MIXED, FCG_LEARNED, FCG_JACOBI, FCG_MG, FCG_LEARNED_MG = 0, 1, 2, 3, 4, 5, 6
 
 
 def _vp(t):
@@ -190,7 +192,7 @@ def generate_pairs(nfields, n, seed0=1000, snaps=(2, 8, 32), rx_range=(100.0, 10
 
 
 def generate_on_policy(net, nfields, n, seed0, snaps=(2, 4, 8, 16, 32, 64), rx_range=(100.0, 1000.0),
-                       device="cuda"):
+                       device="cuda", method=FCG_LEARNED):
     """Residual/error pairs along the learned FCG's own trajectory: like
     generate_pairs, but u_k comes from k iterations of flexible CG with the
     current network, so the pairs are the residuals the network meets when
@@ -213,7 +215,7 @@ def generate_on_policy(net, nfields, n, seed0, snaps=(2, 4, 8, 16, 32, 64), rx_r
         solve(kx, ky, b, ustar, 1.0, 1.0, method=PCG_TRUE, eps=1e-12, max_iters=100000)
         for k in snaps:
             u.copy_(b)
-            solve(kx, ky, b, u, 1.0, 1.0, method=FCG_LEARNED, net=net.h, eps=1e-30, window=0, max_iters=k, r_out=r)
+            solve(kx, ky, b, u, 1.0, 1.0, method=method, net=net.h, eps=1e-30, window=0, max_iters=k, r_out=r)
             R[j].copy_(r)
             E[j].copy_(ustar - u)
             KX[j].copy_(kx)
@@ -227,15 +229,37 @@ def generate_on_policy(net, nfields, n, seed0, snaps=(2, 4, 8, 16, 32, 64), rx_r
     return R, E, KX, KY
 
 
-def fit(net, n=64, nfields=300, steps=1500, rounds=3, lr=2e-3, batch=16, seed0=1000, log=None):
+def mg_targets(data):
+    """Targets that train the network as a correction to the multigrid
+    V-cycle: the network's output is r / D + s y (D = diag(A)), and method
+    FCG_LEARNED_MG applies V-cycle(r) + s y, so the pair (r, e) becomes
+    (r, e - V-cycle(r) + r / D). Pairs are for rx = ry = 1."""
+    import torch
+    R, E, KX, KY = data
+    E2 = E.clone()
+    z = torch.zeros_like(R[0])
+    for j in range(R.shape[0]):
+        z.zero_()
+        mg_apply(KX[j], KY[j], R[j], z, 1.0, 1.0)
+        kx, ky = KX[j], KY[j]
+        D = 1.0 + kx[1:-1, 1:-1] + kx[1:-1, 2:] + ky[1:-1, 1:-1] + ky[2:, 1:-1]
+        E2[j, 1:-1, 1:-1] = E[j, 1:-1, 1:-1] - z[1:-1, 1:-1] + R[j, 1:-1, 1:-1] / D
+    return R, E2, KX, KY
+
+
+def fit(net, n=64, nfields=300, steps=1500, rounds=3, lr=2e-3, batch=16, seed0=1000, log=None, base="jacobi"):
     """The training recipe: PCG pairs, then `rounds` rounds of on-policy pairs
     (half as many fields each, new seeds) added to the set, training after
-    each. Returns the loss history of every round."""
+    each. Returns the loss history of every round. base="mg" trains the
+    network as the correction of FCG_LEARNED_MG (targets by mg_targets,
+    on-policy pairs along that method's own iterates)."""
     import torch
-    data = generate_pairs(nfields, n, seed0=seed0)
+    retarget = mg_targets if base == "mg" else (lambda d: d)
+    method = FCG_LEARNED_MG if base == "mg" else FCG_LEARNED
+    data = retarget(generate_pairs(nfields, n, seed0=seed0))
     hists = [train(net, data, steps=steps, batch=batch, lr=lr, seed=0)]
     for rd in range(rounds):
-        extra = generate_on_policy(net, max(1, nfields // 2), n, seed0 + 100000 * (rd + 1))
+        extra = retarget(generate_on_policy(net, max(1, nfields // 2), n, seed0 + 100000 * (rd + 1), method=method))
         data = tuple(torch.cat([a, b]) for a, b in zip(data, extra))
         hists.append(train(net, data, steps=steps, batch=batch, lr=0.5 * lr, seed=rd + 1))
         if log:

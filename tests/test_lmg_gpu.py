@@ -125,3 +125,23 @@ def test_learned_fcg_beats_jacobi_pcg(trained):
         its_pcg.append(sp["iterations"])
         its_fcg.append(sl["iterations"])
     assert sum(its_fcg) < 0.8 * sum(its_pcg), (its_fcg, its_pcg)
+
+
+def test_untrained_learned_multigrid_is_the_vcycle(gpu_runtime):
+    """FCG_LEARNED_MG applies V-cycle(r) + (network output - r / D); with the
+    output layer at zero that is the V-cycle exactly, so the solve repeats
+    FCG_MG bit for bit."""
+    import torch
+    from ops_b200 import lmg
+    rho, en = lmg.density_field(96, 77)
+    kx, ky, b = (cuda(a) for a in lmg.padded_problem(rho, en))
+    net = lmg.Net(seed=3)
+    try:
+        u1, u2 = b.clone(), b.clone()
+        s1 = lmg.solve(kx, ky, b, u1, 300.0, 300.0, method=lmg.FCG_MG, eps=1e-10, window=40)
+        s2 = lmg.solve(kx, ky, b, u2, 300.0, 300.0, method=lmg.FCG_LEARNED_MG, net=net.h, eps=1e-10, window=40)
+        assert s1["converged"] and s2["converged"] and s2["fallbacks"] == 0
+        assert s1["iterations"] == s2["iterations"]
+        assert torch.equal(u1, u2)
+    finally:
+        net.close()
