@@ -872,6 +872,13 @@ def bench_learned(args, world, rank, local, pg):
     hists = lmg.fit(net, n=64, nfields=300, steps=1500, rounds=3)
     torch.cuda.synchronize(local)
     train_s = time.perf_counter() - t0
+    # the learned correction of the native V-cycle: PCG pairs retargeted to
+    # e - V-cycle(r), one on-policy round
+    t0 = time.perf_counter()
+    net_mg = lmg.Net(seed=5)
+    hists_mg = lmg.fit(net_mg, n=64, nfields=300, steps=1500, rounds=1, base="mg")
+    torch.cuda.synchronize(local)
+    train_mg_s = time.perf_counter() - t0
 
     rho, en = lmg.density_field(N, 4)
     Kx, Ky, u0 = lmg.padded_problem(rho, en)
@@ -880,24 +887,30 @@ def bench_learned(args, world, rank, local, pg):
 
     def run(method, window=40):
         u.copy_(b)
-        return lmg.solve(kx, ky, b, u, rx, rx, method=method, net=net.h, eps=1e-10, window=window, max_iters=20000)
+        h = net_mg.h if method == lmg.FCG_LEARNED_MG else net.h
+        return lmg.solve(kx, ky, b, u, rx, rx, method=method, net=h, eps=1e-10, window=window, max_iters=20000)
 
     for _ in range(W):
         run(lmg.PCG_TRUE)
         run(lmg.FCG_LEARNED)
         run(lmg.FCG_MG)
+        run(lmg.FCG_LEARNED_MG)
     barrier(pg, local)
     with ClockSampler(local) as cs:
         plain = [run(lmg.PCG_TRUE) for _ in range(K)]
         learned = [run(lmg.FCG_LEARNED) for _ in range(K)]
         multigrid = [run(lmg.FCG_MG) for _ in range(K)]
+        learned_mg = [run(lmg.FCG_LEARNED_MG) for _ in range(K)]
     clocks = cs.summary()
+    u_lmg = u.clone()
+    t_lmg = max_over_ranks(pg, float(np.median([s["seconds"] for s in learned_mg])), local)
     u_mg = u.clone()
     run(lmg.FCG_LEARNED)
     u_learned = u.clone()
     run(lmg.PCG_TRUE)
     err = float(torch.linalg.norm(u_learned - u) / torch.linalg.norm(u))
     err_mg = float(torch.linalg.norm(u_mg - u) / torch.linalg.norm(u))
+    err_lmg = float(torch.linalg.norm(u_lmg - u) / torch.linalg.norm(u))
     t_mg = max_over_ranks(pg, float(np.median([s["seconds"] for s in multigrid])), local)
     t_plain = max_over_ranks(pg, float(np.median([s["seconds"] for s in plain])), local)
     t_learned = max_over_ranks(pg, float(np.median([s["seconds"] for s in learned])), local)
@@ -928,9 +941,10 @@ def bench_learned(args, world, rank, local, pg):
         a, c, d = lmg.padded_problem(r_, e_)
         skx, sky, sb = (torch.from_numpy(v).cuda(local) for v in (a, c, d))
         row = {}
-        for name, m in (("pcg", lmg.PCG_TRUE), ("learned_fcg", lmg.FCG_LEARNED)):
+        for name, m, h in (("pcg", lmg.PCG_TRUE, net.h), ("learned_fcg", lmg.FCG_LEARNED, net.h),
+                           ("multigrid_fcg", lmg.FCG_MG, net.h), ("learned_mg_fcg", lmg.FCG_LEARNED_MG, net_mg.h)):
             su = sb.clone()
-            st = lmg.solve(skx, sky, sb, su, 400.0, 400.0, method=m, net=net.h, eps=1e-10, window=40)
+            st = lmg.solve(skx, sky, sb, su, 400.0, 400.0, method=m, net=h, eps=1e-10, window=40)
             row[name] = {"iterations": st["iterations"], "seconds": st["seconds"], "fallbacks": st["fallbacks"]}
         small.append(row)
 
@@ -958,6 +972,7 @@ def bench_learned(args, world, rank, local, pg):
     st_e2e = e2e_solve()
     e2e_s = max_over_ranks(pg, time.perf_counter() - te, local)
     net.close()
+    net_mg.close()
 
     line = {
         "metric": "time to 1e-10 residual (learned FCG)", "value": t_learned, "unit": "s", "n_gpus": world,
@@ -982,6 +997,13 @@ def bench_learned(args, world, rank, local, pg):
                           "rel_l2_vs_fp64_pcg_solution": err_mg, "time_ratio_vs_plain": t_mg / t_plain,
                           "note": "native FP32 aggregation V-cycle (2+2 damped-Jacobi sweeps) per FCG iteration,"
                                   " hierarchy setup inside the timed solve"},
+        "learned_mg_fcg": {"seconds": t_lmg, "iterations": learned_mg[0]["iterations"],
+                           "fallbacks": learned_mg[0]["fallbacks"],
+                           "final_residual_ratio": learned_mg[0]["final_residual"] / learned_mg[0]["initial_residual"],
+                           "rel_l2_vs_fp64_pcg_solution": err_lmg, "time_ratio_vs_plain": t_lmg / t_plain,
+                           "time_ratio_vs_multigrid_alone": t_lmg / t_mg, "training_seconds": train_mg_s,
+                           "final_loss_per_round": [float(np.mean(h[-50:])) for h in hists_mg],
+                           "note": "M(r) = V-cycle(r) + the network's correction, trained on e - V-cycle(r)"},
         "training": {"seconds": train_s, "final_loss_per_round": [float(np.mean(h[-50:])) for h in hists]},
         "small_scale_gain_64x64_rx400": small,
         "roofline": {"bound": "hbm", "achieved": conv_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
