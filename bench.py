@@ -948,7 +948,6 @@ def bench_learned(args, world, rank, local, pg):
             row[name] = {"iterations": st["iterations"], "seconds": st["seconds"], "fallbacks": st["fallbacks"]}
         small.append(row)
 
-    # e2e: host arrays in (pinned), one learned solve through the C-ABI, solution out
     # e2e: Kx, Ky, u0 in from pinned host memory, one solve through the C-ABI,
     # the solution out to pinned host memory (buffers allocated before timing;
     # one untimed call first, as the timed solves above had)
