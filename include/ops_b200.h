@@ -330,9 +330,13 @@ typedef struct ops_b200_trid_system {
 } ops_b200_trid_system;
 
 /* Solves all lines along `solvedim` of `nsys` system sets, of any shapes, in
- * one persistent launch (elem_size 8 = double, 4 = float) on `stream`
- * (cudaStream_t, NULL = default stream). Lines along x up to 512 points and
- * along y/z up to 256 points are supported. */
+ * one launch (elem_size 8 = double, 4 = float) on `stream` (cudaStream_t,
+ * NULL = default stream). Lines along x (contiguous) run the partition
+ * method in shared memory, up to 512 points; lines along y/z (strided,
+ * neighbouring lines contiguous) run Thomas per line, any length, with a
+ * c'/d' scratch array of 2 x (unknowns) elements that the library keeps and
+ * grows. The work lists and that scratch are shared by all calls: calls on
+ * different streams must not overlap. */
 int ops_b200_trid_batch(int elem_size, int solvedim, int nsys, const ops_b200_trid_system *systems, void *stream);
 
 /* ---- allocation-free sweep ----------------------------------------------
