@@ -327,22 +327,23 @@ __global__ void __launch_bounds__(kTileThreads, kCtasPerSm) trid_tile_kernel(con
 // row-major over the system's lines (coalesced too) and the backward pass
 // reads them back: 72 bytes per FP64 unknown (80 for _Inc) against the
 // tile kernel's 40, but no staging, no barriers and several rows of loads in
-// flight per thread, which is what the strided sweeps lacked. The
-// rows in flight are 4 in FP64 and 8 in FP32 (one 32-byte sector of each
-// line per array; measured best for the 256^3 sweeps). The
-// arithmetic is the textbook Thomas elimination:
+// flight per thread, which is what the strided sweeps lacked. Rows in
+// flight: 8 (one 32-byte sector of each line per array in FP32, two in
+// FP64), or 4 in FP64 when the lines fill the GPU (more than 1024 a SM): a
+// grid of few lines leaves the registers free and gains from the deeper
+// pipeline (256^3 FP64 y sweep 0.239 -> 0.219 ms), while the 64-block batch
+// (about 0.5 M lines) lost 7-20 % with it. The arithmetic is the textbook
+// Thomas elimination:
 //   c'_0 = c_0 / b_0, d'_0 = d_0 / b_0; for i >= 1, r = 1 / (b_i - a_i c'_{i-1}),
 //   c'_i = c_i r, d'_i = (d_i - a_i d'_{i-1}) r; x_{n-1} = d'_{n-1},
 //   x_i = d'_i - c'_i x_{i+1}.
 constexpr int kLineThreads = 128;
-template <class T>
-constexpr int line_unroll() { return sizeof(T) == 4 ? 8 : 4; }
+constexpr long long kLinesDeep = 148LL * 1024;  // at most this many lines: 8 rows in flight in FP64
 
-template <class T>
+template <class T, int kLineUnroll>
 __global__ void __launch_bounds__(kLineThreads) trid_line_kernel(const Sys *__restrict__ sys, int nsys,
                                                                  long long total, T *__restrict__ scr_c,
                                                                  T *__restrict__ scr_d) {
-  constexpr int kLineUnroll = line_unroll<T>();
   for (long long g = (long long)blockIdx.x * kLineThreads + threadIdx.x; g < total;
        g += (long long)gridDim.x * kLineThreads) {
     int lo = 0, hi = nsys - 1;  // last system whose first line is <= g
@@ -477,7 +478,10 @@ bool launch_lines(std::vector<Sys> systems, cudaStream_t stream, long long *kern
   OPSB_CUDA(cudaMemcpyAsync(B.sys, live.data(), live.size() * sizeof(Sys), cudaMemcpyHostToDevice, stream));
   T *sc = static_cast<T *>(B.scr), *sd = sc + unknowns;
   const int grid = (int)std::min<long long>((lines + kLineThreads - 1) / kLineThreads, 148LL * 16);
-  trid_line_kernel<T><<<grid, kLineThreads, 0, stream>>>(B.sys, (int)live.size(), lines, sc, sd);
+  if (sizeof(T) == 4 || lines <= kLinesDeep)
+    trid_line_kernel<T, 8><<<grid, kLineThreads, 0, stream>>>(B.sys, (int)live.size(), lines, sc, sd);
+  else
+    trid_line_kernel<T, 4><<<grid, kLineThreads, 0, stream>>>(B.sys, (int)live.size(), lines, sc, sd);
   OPSB_CUDA(cudaGetLastError());
   if (kernels) (*kernels)++;
   return true;
