@@ -68,3 +68,24 @@ def test_single_process_api_calls_without_gpu(capsys):
     p.set_cuda_opts(1, 2, 3)
     p.set_cuda_sync(0)
     assert (p.strategy, p.jacobi, p.batch_size, p.cuda_opts, p.cuda_sync) == (3, (1e-10, 1e-12, 5), 64, (1, 2, 3), 0)
+
+
+def test_heat_solve_arguments_are_checked_before_any_device_work():
+    """Unknown methods, bad shapes and bad tolerances are refused with
+    OPS_B200_ERR_ARG before the library touches a GPU (the field pointers
+    below are never dereferenced)."""
+    import ctypes as C
+
+    from ops_b200 import lib
+    from ops_b200._lib import HeatStats, HeatSystem
+    L = lib()
+    fake = C.c_void_p(4096)
+    sysd = HeatSystem(64, 64, 66, fake, fake, fake, fake, 1.0, 1.0)
+    st = HeatStats()
+    assert L.ops_b200_heat_solve(C.byref(sysd), 7, -1, 1e-10, 100, 0, None, C.byref(st), None) == -1
+    assert b"method" in L.ops_b200_last_error()
+    assert L.ops_b200_heat_solve(C.byref(sysd), 5, -1, 0.0, 100, 0, None, C.byref(st), None) == -1
+    bad = HeatSystem(64, 64, 65, fake, fake, fake, fake, 1.0, 1.0)      # pitch < nx + 2
+    assert L.ops_b200_heat_solve(C.byref(bad), 5, -1, 1e-10, 100, 0, None, C.byref(st), None) == -1
+    assert L.ops_b200_heat_mg_apply(C.byref(bad), fake, fake, None, None) == -1
+    assert b"shape" in L.ops_b200_last_error()
