@@ -3,8 +3,11 @@
 //
 // Each functor restates one reference kernel with the same operation order
 // (apps/c/CloverLeaf/*_kernel.h, cited per functor); with --fmad=false the
-// cell updates round exactly like the reference's x86-64 CPU build. Loop
-// names are "cloverleaf/<reference kernel name>".
+// cell updates round exactly like the reference's x86-64 CPU build.
+// Divisions whose numerator is often exactly zero (velocities, fluxes and
+// viscosity of quiescent regions) go through qdiv, which returns the same
+// IEEE quotient without the division for a zero numerator. Loop names are
+// "cloverleaf/<reference kernel name>".
 #include <cstddef>
 
 #include "clover_common.h"
@@ -247,15 +250,17 @@ struct viscosity_kernel {
     double ugrad = (xvel0(1, 0) + xvel0(1, 1)) - (xvel0(0, 0) + xvel0(0, 1));
     double vgrad = (yvel0(0, 1) + yvel0(1, 1)) - (yvel0(0, 0) + yvel0(1, 0));
     double div = (celldx(0, 0)) * (ugrad) + (celldy(0, 0)) * (vgrad);
-    double strain2 = 0.5 * (xvel0(0, 1) + xvel0(1, 1) - xvel0(0, 0) - xvel0(1, 0)) / (celldy(0, 0)) +
-                     0.5 * (yvel0(1, 0) + yvel0(1, 1) - yvel0(0, 0) - yvel0(0, 1)) / (celldx(0, 0));
-    double pgradx = (pressure(1, 0) - pressure(-1, 0)) / (celldx(0, 0) + celldx(1, 0));
-    double pgrady = (pressure(0, 1) - pressure(0, -1)) / (celldy(0, 0) + celldy(0, 1));
+    // qdiv: the same quotients; exactly zero numerators (uniform regions)
+    // take the product path
+    double strain2 = qdiv(0.5 * (xvel0(0, 1) + xvel0(1, 1) - xvel0(0, 0) - xvel0(1, 0)), (celldy(0, 0))) +
+                     qdiv(0.5 * (yvel0(1, 0) + yvel0(1, 1) - yvel0(0, 0) - yvel0(0, 1)), (celldx(0, 0)));
+    double pgradx = qdiv(pressure(1, 0) - pressure(-1, 0), celldx(0, 0) + celldx(1, 0));
+    double pgrady = qdiv(pressure(0, 1) - pressure(0, -1), celldy(0, 0) + celldy(0, 1));
     double pgradx2 = pgradx * pgradx;
     double pgrady2 = pgrady * pgrady;
-    double limiter = ((0.5 * (ugrad) / celldx(0, 0)) * pgradx2 + (0.5 * (vgrad) / celldy(0, 0)) * pgrady2 +
-                      strain2 * pgradx * pgrady) /
-                     op_max(pgradx2 + pgrady2, 1.0e-16);
+    double limiter = qdiv(qdiv(0.5 * (ugrad), celldx(0, 0)) * pgradx2 + qdiv(0.5 * (vgrad), celldy(0, 0)) * pgrady2 +
+                              strain2 * pgradx * pgrady,
+                          op_max(pgradx2 + pgrady2, 1.0e-16));
     if ((limiter > 0.0) || (div >= 0.0)) {
       viscosity(0, 0) = 0.0;
     } else {
@@ -280,7 +285,7 @@ struct calc_dt_kernel {  // :7
     double dsx = celldx(0, 0);
     double dsy = celldy(0, 0);
     double cc2 = soundspeed(0, 0) * soundspeed(0, 0);
-    cc2 = cc2 + 2.0 * viscosity(0, 0) / density0(0, 0);
+    cc2 = cc2 + qdiv(2.0 * viscosity(0, 0), density0(0, 0));
     cc2 = op_max(sqrt(cc2), cc.g_small);
     double dtct = cc.dtc_safe * op_min(dsx, dsy) / cc2;
     double div = 0.0;
@@ -292,7 +297,7 @@ struct calc_dt_kernel {  // :7
     dv2 = (yvel0(0, 1) + yvel0(1, 1)) * yarea(0, 1);
     div = div + dv2 - dv1;
     double dtvt = cc.dtv_safe * 2.0 * volume(0, 0) / op_max(op_max(fabs(dv1), fabs(dv2)), cc.g_small * volume(0, 0));
-    div = div / (2.0 * volume(0, 0));
+    div = qdiv(div, 2.0 * volume(0, 0));
     double dtdivt;
     if (div < -cc.g_small)
       dtdivt = cc.dtdiv_safe * (-1.0 / div);
@@ -348,7 +353,7 @@ struct PdV_kernel_predict {  // :7
     double total_flux = right_flux - left_flux + top_flux - bottom_flux;
     volume_change(0, 0) = (volume(0, 0)) / (volume(0, 0) + total_flux);
     double recip_volume = 1.0 / volume(0, 0);
-    double energy_change = (pressure(0, 0) / density0(0, 0) + viscosity(0, 0) / density0(0, 0)) * total_flux * recip_volume;
+    double energy_change = (pressure(0, 0) / density0(0, 0) + qdiv(viscosity(0, 0), density0(0, 0))) * total_flux * recip_volume;
     energy1(0, 0) = energy0(0, 0) - energy_change;
     density1(0, 0) = density0(0, 0) * volume_change(0, 0);
   }
@@ -368,7 +373,7 @@ struct PdV_kernel_nopredict {  // :45
     double total_flux = right_flux - left_flux + top_flux - bottom_flux;
     volume_change(0, 0) = (volume(0, 0)) / (volume(0, 0) + total_flux);
     double recip_volume = 1.0 / volume(0, 0);
-    double energy_change = (pressure(0, 0) / density0(0, 0) + viscosity(0, 0) / density0(0, 0)) * total_flux * recip_volume;
+    double energy_change = (pressure(0, 0) / density0(0, 0) + qdiv(viscosity(0, 0), density0(0, 0))) * total_flux * recip_volume;
     energy1(0, 0) = energy0(0, 0) - energy_change;
     density1(0, 0) = density0(0, 0) * volume_change(0, 0);
   }
@@ -452,7 +457,7 @@ __device__ __forceinline__ void advec_cell_flux(double vol_flux, const View &pre
   } else {
     upwind = 0; donor = 0; downwind = -1; dif = upwind;
   }
-  double sigmat = fabs(vol_flux) / pre_vol(donor);
+  double sigmat = qdiv(fabs(vol_flux), pre_vol(donor));
   double sigma3 = (1.0 + sigmat) * (vertexd(0) / vertexd(dif));
   double sigma4 = 2.0 - sigmat;
   double sigmav = sigmat;
@@ -465,7 +470,7 @@ __device__ __forceinline__ void advec_cell_flux(double vol_flux, const View &pre
   else
     limiter = 0.0;
   mass_flux = (vol_flux) * (density1(donor) + limiter);
-  double sigmam = fabs(mass_flux) / (density1(donor) * pre_vol(donor));
+  double sigmam = qdiv(fabs(mass_flux), density1(donor) * pre_vol(donor));
   diffuw = energy1(donor) - energy1(upwind);
   diffdw = energy1(downwind) - energy1(donor);
   if ((diffuw * diffdw) > 0.0)
@@ -624,7 +629,7 @@ __device__ __forceinline__ double advec_mom_flux(double node_flux, const View &n
   } else {
     upwind = -1; donor = 0; downwind = 1; dif = upwind;
   }
-  double sigma = fabs(node_flux) / node_mass_pre(donor);
+  double sigma = qdiv(fabs(node_flux), node_mass_pre(donor));
   double width = celld(0);
   double vdiffuw = vel1(donor) - vel1(upwind);
   double vdiffdw = vel1(downwind) - vel1(donor);
@@ -658,13 +663,13 @@ struct advec_mom_kernel1_y_nonvector {  // :242
 struct advec_mom_kernel2_x {  // :284
   CL_LOOP(advec_mom_kernel2_x);
   __device__ void operator()(D &vel1, const D &node_mass_post, const D &node_mass_pre, const D &mom_flux) const {
-    vel1(0, 0) = (vel1(0, 0) * node_mass_pre(0, 0) + mom_flux(-1, 0) - mom_flux(0, 0)) / node_mass_post(0, 0);
+    vel1(0, 0) = qdiv(vel1(0, 0) * node_mass_pre(0, 0) + mom_flux(-1, 0) - mom_flux(0, 0), node_mass_post(0, 0));
   }
 };
 struct advec_mom_kernel2_y {  // :293
   CL_LOOP(advec_mom_kernel2_y);
   __device__ void operator()(D &vel1, const D &node_mass_post, const D &node_mass_pre, const D &mom_flux) const {
-    vel1(0, 0) = (vel1(0, 0) * node_mass_pre(0, 0) + mom_flux(0, -1) - mom_flux(0, 0)) / node_mass_post(0, 0);
+    vel1(0, 0) = qdiv(vel1(0, 0) * node_mass_pre(0, 0) + mom_flux(0, -1) - mom_flux(0, 0), node_mass_post(0, 0));
   }
 };
 

@@ -5,8 +5,10 @@
 // (apps/c/CloverLeaf_3D/*_kernel.h, cited per functor); with --fmad=false the
 // cell updates round exactly like the reference's x86-64 CPU build. Kernels
 // that differ only in the axis they work along are one template over the
-// axis, which keeps every expression as the reference writes it. Loop names
-// are "cloverleaf3d/<reference kernel name>".
+// axis, which keeps every expression as the reference writes it. Divisions
+// whose numerator is often exactly zero go through qdiv (same IEEE quotient,
+// no division for a zero numerator). Loop names are
+// "cloverleaf3d/<reference kernel name>".
 #include <cstddef>
 
 #include "clover3d_common.h"
@@ -384,21 +386,23 @@ struct viscosity_kernel {
     double wgradz2 = zvel0(0, 0, 1) + zvel0(1, 0, 1) + zvel0(0, 1, 1) + zvel0(1, 1, 1);
     div = xarea(0, 0, 0) * (ugradx2 - ugradx1) + yarea(0, 0, 0) * (vgrady2 - vgrady1) +
           zarea(0, 0, 0) * (wgradz2 - wgradz1);
-    double xx = 0.25 * (ugradx2 - ugradx1) / (celldx(0, 0, 0));
-    double yy = 0.25 * (vgrady2 - vgrady1) / (celldy(0, 0, 0));
-    double zz = 0.25 * (wgradz2 - wgradz1) / (celldz(0, 0, 0));
-    double xy = 0.25 * (ugrady2 - ugrady1) / (celldy(0, 0, 0)) + 0.25 * (vgradx2 - vgradx1) / (celldx(0, 0, 0));
-    double xz = 0.25 * (ugradz2 - ugradz1) / (celldz(0, 0, 0)) + 0.25 * (wgradx2 - wgradx1) / (celldx(0, 0, 0));
-    double yz = 0.25 * (vgradz2 - vgradz1) / (celldz(0, 0, 0)) + 0.25 * (wgrady2 - wgrady1) / (celldy(0, 0, 0));
-    pgradx = (pressure(1, 0, 0) - pressure(-1, 0, 0)) / (celldx(0, 0, 0) + celldx(1, 0, 0));
-    pgrady = (pressure(0, 1, 0) - pressure(0, -1, 0)) / (celldy(0, 0, 0) + celldy(0, 1, 0));
-    pgradz = (pressure(0, 0, 1) - pressure(0, 0, -1)) / (celldz(0, 0, 0) + celldz(0, 0, 1));
+    // qdiv: the same quotients; exactly zero numerators (uniform regions)
+    // take the product path
+    double xx = qdiv(0.25 * (ugradx2 - ugradx1), (celldx(0, 0, 0)));
+    double yy = qdiv(0.25 * (vgrady2 - vgrady1), (celldy(0, 0, 0)));
+    double zz = qdiv(0.25 * (wgradz2 - wgradz1), (celldz(0, 0, 0)));
+    double xy = qdiv(0.25 * (ugrady2 - ugrady1), (celldy(0, 0, 0))) + qdiv(0.25 * (vgradx2 - vgradx1), (celldx(0, 0, 0)));
+    double xz = qdiv(0.25 * (ugradz2 - ugradz1), (celldz(0, 0, 0))) + qdiv(0.25 * (wgradx2 - wgradx1), (celldx(0, 0, 0)));
+    double yz = qdiv(0.25 * (vgradz2 - vgradz1), (celldz(0, 0, 0))) + qdiv(0.25 * (wgrady2 - wgrady1), (celldy(0, 0, 0)));
+    pgradx = qdiv(pressure(1, 0, 0) - pressure(-1, 0, 0), celldx(0, 0, 0) + celldx(1, 0, 0));
+    pgrady = qdiv(pressure(0, 1, 0) - pressure(0, -1, 0), celldy(0, 0, 0) + celldy(0, 1, 0));
+    pgradz = qdiv(pressure(0, 0, 1) - pressure(0, 0, -1), celldz(0, 0, 0) + celldz(0, 0, 1));
     pgradx2 = pgradx * pgradx;
     pgrady2 = pgrady * pgrady;
     pgradz2 = pgradz * pgradz;
-    limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady + xz * pgradx * pgradz +
-               yz * pgrady * pgradz) /
-              op_max(pgradx2 + pgrady2 + pgradz2, 1.0e-16);
+    limiter = qdiv(xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady + xz * pgradx * pgradz +
+                       yz * pgrady * pgradz,
+                   op_max(pgradx2 + pgrady2 + pgradz2, 1.0e-16));
     if ((limiter > 0.0) || (div >= 0.0)) {
       viscosity(0, 0, 0) = 0.0;
     } else {
@@ -427,7 +431,7 @@ struct calc_dt_kernel {  // :7
     ds = op_min(op_min(celldx(0, 0, 0), celldy(0, 0, 0)), celldz(0, 0, 0));
     ds = 1.0 / (ds * ds);
     cc = soundspeed(0, 0, 0) * soundspeed(0, 0, 0);
-    cc = cc + 2.0 * viscosity(0, 0, 0) / density0(0, 0, 0);
+    cc = cc + qdiv(2.0 * viscosity(0, 0, 0), density0(0, 0, 0));
     dtct = ds * cc;
     dtct = c3.dtc_safe * 1.0 / op_max(sqrt(dtct), c3.g_small);
     du1 = (xvel0(0, 0, 0) + xvel0(0, 1, 0) + xvel0(0, 0, 1) + xvel0(0, 1, 1)) * xarea(0, 0, 0);
@@ -529,7 +533,7 @@ struct PdV_kernel_predict {
     volume_change(0, 0, 0) = (volume(0, 0, 0)) / (volume(0, 0, 0) + total_flux);
     recip_volume = 1.0 / volume(0, 0, 0);
     energy_change =
-        (pressure(0, 0, 0) / density0(0, 0, 0) + viscosity(0, 0, 0) / density0(0, 0, 0)) * total_flux * recip_volume;
+        (pressure(0, 0, 0) / density0(0, 0, 0) + qdiv(viscosity(0, 0, 0), density0(0, 0, 0))) * total_flux * recip_volume;
     energy1(0, 0, 0) = energy0(0, 0, 0) - energy_change;
     density1(0, 0, 0) = density0(0, 0, 0) * volume_change(0, 0, 0);
   }
@@ -566,7 +570,7 @@ struct PdV_kernel_nopredict {
     volume_change(0, 0, 0) = (volume(0, 0, 0)) / (volume(0, 0, 0) + total_flux);
     recip_volume = 1.0 / volume(0, 0, 0);
     energy_change =
-        (pressure(0, 0, 0) / density0(0, 0, 0) + viscosity(0, 0, 0) / density0(0, 0, 0)) * total_flux * recip_volume;
+        (pressure(0, 0, 0) / density0(0, 0, 0) + qdiv(viscosity(0, 0, 0), density0(0, 0, 0))) * total_flux * recip_volume;
     energy1(0, 0, 0) = energy0(0, 0, 0) - energy_change;
     density1(0, 0, 0) = density0(0, 0, 0) * volume_change(0, 0, 0);
   }
@@ -734,7 +738,7 @@ __device__ __forceinline__ void advec_cell_flux(const D &vol_flux, const D &pre_
     downwind = -1;
     dif = upwind;
   }
-  sigmat = fabs(vol_flux(0, 0, 0)) / ax<AX>(pre_vol, donor);
+  sigmat = qdiv(fabs(vol_flux(0, 0, 0)), ax<AX>(pre_vol, donor));
   sigma3 = (1.0 + sigmat) * (vertexd(0, 0, 0) / ax<AX>(vertexd, dif));
   sigma4 = 2.0 - sigmat;
   sigmav = sigmat;
@@ -746,7 +750,7 @@ __device__ __forceinline__ void advec_cell_flux(const D &vol_flux, const D &pre_
   else
     limiter = 0.0;
   mass_flux(0, 0, 0) = (vol_flux(0, 0, 0)) * (ax<AX>(density1, donor) + limiter);
-  sigmam = fabs(mass_flux(0, 0, 0)) / (ax<AX>(density1, donor) * ax<AX>(pre_vol, donor));
+  sigmam = qdiv(fabs(mass_flux(0, 0, 0)), ax<AX>(density1, donor) * ax<AX>(pre_vol, donor));
   diffuw = ax<AX>(energy1, donor) - ax<AX>(energy1, upwind);
   diffdw = ax<AX>(energy1, downwind) - ax<AX>(energy1, donor);
   if ((diffuw * diffdw) > 0.0)
@@ -927,7 +931,7 @@ __device__ __forceinline__ void advec_mom_flux(const D &node_flux, const D &node
     downwind = 1;
     dif = upwind;
   }
-  sigma = fabs(node_flux(0, 0, 0)) / ax<AX>(node_mass_pre, donor);
+  sigma = qdiv(fabs(node_flux(0, 0, 0)), ax<AX>(node_mass_pre, donor));
   width = celld(0, 0, 0);
   vdiffuw = ax<AX>(vel1, donor) - ax<AX>(vel1, upwind);
   vdiffdw = ax<AX>(vel1, downwind) - ax<AX>(vel1, donor);
@@ -959,8 +963,8 @@ ADVEC_MOM1(advec_mom_kernel1_z_nonvector, 2)
 template <int AX>
 struct advec_mom_vel {
   __device__ void operator()(D &vel1, const D &node_mass_post, const D &node_mass_pre, const D &mom_flux) const {
-    vel1(0, 0, 0) = (vel1(0, 0, 0) * node_mass_pre(0, 0, 0) + ax<AX>(mom_flux, -1) - mom_flux(0, 0, 0)) /
-                    node_mass_post(0, 0, 0);
+    vel1(0, 0, 0) = qdiv(vel1(0, 0, 0) * node_mass_pre(0, 0, 0) + ax<AX>(mom_flux, -1) - mom_flux(0, 0, 0),
+                         node_mass_post(0, 0, 0));
   }
 };
 struct advec_mom_kernel2_x : advec_mom_vel<0> { C3_LOOP(advec_mom_kernel2_x); };

