@@ -244,7 +244,6 @@ UH_PAIR(update_halo_kernel4_minus_2_b, 0, -2, 1, FIELD_VOL_FLUX_Y, FIELD_MASS_FL
 // ---- viscosity_kernel.h:5 ----------------------------------------------------
 struct viscosity_kernel {
   CL_LOOP(viscosity_kernel);
-  static constexpr int min_blocks = 6;
   __device__ void operator()(const D &xvel0, const D &yvel0, const D &celldx, const D &celldy, const D &pressure,
                              const D &density0, D &viscosity) const {
     double ugrad = (xvel0(1, 0) + xvel0(1, 1)) - (xvel0(0, 0) + xvel0(0, 1));
@@ -341,7 +340,6 @@ struct calc_dt_kernel_print {  // :74
 // ---- PdV_kernel.h ------------------------------------------------------------
 struct PdV_kernel_predict {  // :7
   CL_LOOP(PdV_kernel_predict);
-  static constexpr int min_blocks = 6;
   __device__ void operator()(const D &xarea, const D &xvel0, const D &yarea, const D &yvel0, D &volume_change,
                              const D &volume, const D &pressure, const D &density0, D &density1,
                              const D &viscosity, const D &energy0, D &energy1) const {
