@@ -6,8 +6,9 @@
 // cell updates round exactly like the reference's x86-64 CPU build.
 // Divisions whose numerator is often exactly zero (velocities, fluxes and
 // viscosity of quiescent regions) go through qdiv, which returns the same
-// IEEE quotient without the division for a zero numerator. Loop names are
-// "cloverleaf/<reference kernel name>".
+// IEEE quotient without the division for a zero numerator, and the
+// advection limiter's cell-width ratio through qratio (exactly 1 for equal
+// widths). Loop names are "cloverleaf/<reference kernel name>".
 #include <cstddef>
 
 #include "clover_common.h"
@@ -456,7 +457,7 @@ __device__ __forceinline__ void advec_cell_flux(double vol_flux, const View &pre
     upwind = 0; donor = 0; downwind = -1; dif = upwind;
   }
   double sigmat = qdiv(fabs(vol_flux), pre_vol(donor));
-  double sigma3 = (1.0 + sigmat) * (vertexd(0) / vertexd(dif));
+  double sigma3 = (1.0 + sigmat) * qratio(vertexd(0), vertexd(dif));
   double sigma4 = 2.0 - sigmat;
   double sigmav = sigmat;
   double diffuw = density1(donor) - density1(upwind);

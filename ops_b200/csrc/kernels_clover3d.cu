@@ -7,7 +7,8 @@
 // that differ only in the axis they work along are one template over the
 // axis, which keeps every expression as the reference writes it. Divisions
 // whose numerator is often exactly zero go through qdiv (same IEEE quotient,
-// no division for a zero numerator). Loop names are
+// no division for a zero numerator), the advection limiter's cell-width
+// ratio through qratio (exactly 1 for equal widths). Loop names are
 // "cloverleaf3d/<reference kernel name>".
 #include <cstddef>
 
@@ -739,7 +740,7 @@ __device__ __forceinline__ void advec_cell_flux(const D &vol_flux, const D &pre_
     dif = upwind;
   }
   sigmat = qdiv(fabs(vol_flux(0, 0, 0)), ax<AX>(pre_vol, donor));
-  sigma3 = (1.0 + sigmat) * (vertexd(0, 0, 0) / ax<AX>(vertexd, dif));
+  sigma3 = (1.0 + sigmat) * qratio(vertexd(0, 0, 0), ax<AX>(vertexd, dif));
   sigma4 = 2.0 - sigmat;
   sigmav = sigmat;
   diffuw = ax<AX>(density1, donor) - ax<AX>(density1, upwind);

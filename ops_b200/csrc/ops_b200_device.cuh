@@ -49,6 +49,13 @@ __device__ __forceinline__ double qdiv(double a, double b) {
   if (a == 0.0 && b != 0.0 && isfinite(b)) return a * b;
   return a / b;
 }
+// a / b, with the same IEEE result for every input: equal finite nonzero
+// operands give exactly 1 without the division (the cell-width ratios of a
+// uniform mesh).
+__device__ __forceinline__ double qratio(double a, double b) {
+  if (a == b && b != 0.0 && isfinite(b)) return 1.0;
+  return a / b;
+}
 
 // 2D accessor: p points at the current point; (i, j) is a stencil offset.
 // As in the reference's ACC<T> (ops/c/include/ops_lib_core.h:1525-1556) an
