@@ -122,30 +122,33 @@ void Runtime::init(int device, int diags) {
   inited_ = true;
 }
 
-static void require(bool cond, int code, const std::string &msg) {
-  if (!cond) throw Error(code, msg);
-}
+// A checked condition; the message (often built from strings) is evaluated
+// only when the check fails, so the checks cost nothing on the loop path.
+#define OPSB_REQUIRE(cond, code, msg)              \
+  do {                                             \
+    if (!(cond)) throw Error((code), (msg));       \
+  } while (0)
 
 Dat &Runtime::dat(int i) {
-  require(i >= 0 && i < (int)dats_.size() && dats_[i], E_ARG, "invalid dat handle " + std::to_string(i));
+  OPSB_REQUIRE(i >= 0 && i < (int)dats_.size() && dats_[i], E_ARG, "invalid dat handle " + std::to_string(i));
   return *dats_[i];
 }
 Stencil &Runtime::stencil(int i) {
-  require(i >= 0 && i < (int)stencils_.size(), E_ARG, "invalid stencil handle " + std::to_string(i));
+  OPSB_REQUIRE(i >= 0 && i < (int)stencils_.size(), E_ARG, "invalid stencil handle " + std::to_string(i));
   return stencils_[i];
 }
 Reduction &Runtime::reduction(int i) {
-  require(i >= 0 && i < (int)reductions_.size(), E_ARG, "invalid reduction handle " + std::to_string(i));
+  OPSB_REQUIRE(i >= 0 && i < (int)reductions_.size(), E_ARG, "invalid reduction handle " + std::to_string(i));
   return reductions_[i];
 }
 Block &Runtime::block(int i) {
-  require(i >= 0 && i < (int)blocks_.size(), E_ARG, "invalid block handle " + std::to_string(i));
+  OPSB_REQUIRE(i >= 0 && i < (int)blocks_.size(), E_ARG, "invalid block handle " + std::to_string(i));
   return blocks_[i];
 }
 
 int Runtime::decl_block(int dims, const char *name) {
-  require(inited_, E_STATE, "ops_decl_block before ops_init");
-  require(dims >= 1 && dims <= 3, E_UNSUPPORTED, "blocks of 1 to 3 dimensions are supported");
+  OPSB_REQUIRE(inited_, E_STATE, "ops_decl_block before ops_init");
+  OPSB_REQUIRE(dims >= 1 && dims <= 3, E_UNSUPPORTED, "blocks of 1 to 3 dimensions are supported");
   Block b;
   b.index = (int)blocks_.size();
   b.dims = dims;
@@ -165,11 +168,11 @@ static int type_size_of(const char *type) {
 
 int Runtime::decl_dat(int blk, int dim, const int *size, const int *base, const int *d_m, const int *d_p,
                       const void *data, int type_size, const char *type, const char *name) {
-  require(inited_, E_STATE, "ops_decl_dat before ops_init");
+  OPSB_REQUIRE(inited_, E_STATE, "ops_decl_dat before ops_init");
   Block &b = block(blk);
-  require(dim >= 1, E_ARG, "dat dim must be >= 1");
+  OPSB_REQUIRE(dim >= 1, E_ARG, "dat dim must be >= 1");
   int ts = type_size > 0 ? type_size : type_size_of(type);
-  require(ts > 0, E_ARG, std::string("unknown dat type ") + (type ? type : "(null)"));
+  OPSB_REQUIRE(ts > 0, E_ARG, std::string("unknown dat type ") + (type ? type : "(null)"));
   auto d = std::make_unique<Dat>();
   d->index = (int)dats_.size();
   d->block = blk;
@@ -180,8 +183,8 @@ int Runtime::decl_dat(int blk, int dim, const int *size, const int *base, const 
   d->name = name ? name : "";
   for (int i = 0; i < 3; i++) {
     if (i < b.dims) {
-      require(d_m[i] <= 0 && d_p[i] >= 0, E_ARG, "halo depths must satisfy d_m <= 0 <= d_p");
-      require(size[i] >= 0, E_ARG, "negative dat size");
+      OPSB_REQUIRE(d_m[i] <= 0 && d_p[i] >= 0, E_ARG, "halo depths must satisfy d_m <= 0 <= d_p");
+      OPSB_REQUIRE(size[i] >= 0, E_ARG, "negative dat size");
       d->base[i] = base ? base[i] : 0;
       d->d_m[i] = d_m[i];
       d->d_p[i] = d_p[i];
@@ -215,8 +218,8 @@ int Runtime::decl_dat(int blk, int dim, const int *size, const int *base, const 
 }
 
 int Runtime::decl_stencil(int dims, int points, const int *offs, const int *stride, const char *name) {
-  require(inited_, E_STATE, "ops_decl_stencil before ops_init");
-  require(dims >= 1 && dims <= 3 && points >= 1, E_ARG, "bad stencil shape");
+  OPSB_REQUIRE(inited_, E_STATE, "ops_decl_stencil before ops_init");
+  OPSB_REQUIRE(dims >= 1 && dims <= 3 && points >= 1, E_ARG, "bad stencil shape");
   Stencil s;
   s.index = (int)stencils_.size();
   s.dims = dims;
@@ -230,9 +233,9 @@ int Runtime::decl_stencil(int dims, int points, const int *offs, const int *stri
 
 int Runtime::decl_mgrid_stencil(int dims, int points, const int *offs, const int *mgrid_stride, int type,
                                 const char *name) {
-  require(type == 1 || type == 2, E_ARG, "multigrid stencil type must be 1 (prolong) or 2 (restrict)");
-  require(mgrid_stride != nullptr, E_ARG, "multigrid stencils need a stride");
-  for (int i = 0; i < dims && i < 3; i++) require(mgrid_stride[i] >= 1, E_ARG, "multigrid stride must be >= 1");
+  OPSB_REQUIRE(type == 1 || type == 2, E_ARG, "multigrid stencil type must be 1 (prolong) or 2 (restrict)");
+  OPSB_REQUIRE(mgrid_stride != nullptr, E_ARG, "multigrid stencils need a stride");
+  for (int i = 0; i < dims && i < 3; i++) OPSB_REQUIRE(mgrid_stride[i] >= 1, E_ARG, "multigrid stride must be >= 1");
   int h = decl_stencil(dims, points, offs, nullptr, name);
   Stencil &st = stencils_[h];
   st.type = type;
@@ -241,18 +244,18 @@ int Runtime::decl_mgrid_stencil(int dims, int points, const int *offs, const int
 }
 
 int Runtime::decl_reduction(int size, const char *type, const char *name) {
-  require(inited_, E_STATE, "ops_decl_reduction_handle before ops_init");
-  require(size > 0, E_ARG, "reduction size must be positive");
+  OPSB_REQUIRE(inited_, E_STATE, "ops_decl_reduction_handle before ops_init");
+  OPSB_REQUIRE(size > 0, E_ARG, "reduction size must be positive");
   Reduction r;
   r.index = (int)reductions_.size();
   r.size = size;
   r.type = type ? type : "double";
   r.elem = type_size_of(r.type.c_str());
-  require(r.elem > 0, E_ARG, "unknown reduction type " + r.type);
+  OPSB_REQUIRE(r.elem > 0, E_ARG, "unknown reduction type " + r.type);
   r.name = name ? name : "";
   auto span = [](int bytes) { return (size_t)((std::max(bytes, 64) + 63) / 64 * 64); };
   size_t off = reductions_.empty() ? 0 : (size_t)(reductions_.back().slot_d - red_arena_) + span(reductions_.back().size);
-  require(off + span(size) <= kRedArenaBytes, E_UNSUPPORTED, "reduction handles exceed the 64 KiB arena");
+  OPSB_REQUIRE(off + span(size) <= kRedArenaBytes, E_UNSUPPORTED, "reduction handles exceed the 64 KiB arena");
   r.slot_d = red_arena_ + off;
   OPSB_CUDA(cudaMemsetAsync(r.slot_d, 0, span(size), stream_));
   red_dirty_ = true;
@@ -261,7 +264,7 @@ int Runtime::decl_reduction(int size, const char *type, const char *name) {
 }
 
 void Runtime::decl_const(const char *name, int dim, const char *type, const void *data) {
-  require(inited_, E_STATE, "ops_decl_const before ops_init");
+  OPSB_REQUIRE(inited_, E_STATE, "ops_decl_const before ops_init");
   execute();  // ops_update_const flushes the queue first (ops_lazy.cpp semantics)
   // "<app>/<name>" updates that app's slot only; a bare name updates every
   // app's slot of that name.
@@ -276,7 +279,7 @@ void Runtime::decl_const(const char *name, int dim, const char *type, const void
     size_t seen = 0;
     for (auto it = range.first; it != range.second; ++it) {
       if (!scope.empty() && it->second.scope != scope) continue;
-      require(seen == 0 || seen == it->second.bytes, E_ARG,
+      OPSB_REQUIRE(seen == 0 || seen == it->second.bytes, E_ARG,
               "constant '" + key + "' has different layouts in several apps: qualify it as <app>/" + key);
       seen = it->second.bytes;
     }
@@ -298,13 +301,13 @@ void Runtime::decl_const(const char *name, int dim, const char *type, const void
 // ---------------------------------------------------------------------------
 void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim, const int *range,
                        const Arg *args, int nargs) {
-  require(inited_, E_STATE, "ops_par_loop before ops_init");
-  require(loop != nullptr, E_NOTFOUND, "unknown loop kernel");
+  OPSB_REQUIRE(inited_, E_STATE, "ops_par_loop before ops_init");
+  OPSB_REQUIRE(loop != nullptr, E_NOTFOUND, "unknown loop kernel");
   Block &b = block(blk);
-  require(dim == b.dims, E_ARG, "ops_par_loop dim does not match the block");
-  require(nargs == loop->nparams, E_ARG,
+  OPSB_REQUIRE(dim == b.dims, E_ARG, "ops_par_loop dim does not match the block");
+  OPSB_REQUIRE(nargs == loop->nparams, E_ARG,
           "loop " + loop->kernel + " takes " + std::to_string(loop->nparams) + " args, got " + std::to_string(nargs));
-  require(nargs <= OPSB_MAX_ARGS, E_ARG, "too many loop args");
+  OPSB_REQUIRE(nargs <= OPSB_MAX_ARGS, E_ARG, "too many loop args");
   Desc d;
   d.loop = loop;
   d.name = name ? name : loop->kernel;
@@ -325,30 +328,30 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
       case ARG_DAT: {
         Dat &dt = dat(a.dat);
         stencil(a.stencil);
-        require(p.cls == 'A', E_ARG, "loop " + loop->kernel + ": arg " + std::to_string(i) + " is a dat but the kernel expects a pointer");
-        require(p.elem == dt.type_size, E_ARG, "loop " + loop->kernel + ": dat " + dt.name + " element size mismatch");
-        require(dt.dim == 1, E_UNSUPPORTED, "dat " + dt.name + ": multi-component dats are not supported by loop kernels");
-        require(dt.plane < (1LL << 31), E_UNSUPPORTED, "dat " + dt.name + " has a plane of 2^31 elements or more");
-        require(dt.block == blk, E_ARG, "dat " + dt.name + " is declared on another block");
-        require(dt.locked == 0, E_STATE, "dat " + dt.name + " is used in a loop while its raw pointer is held (ops_lib_core.cpp:2321)");
-        require(stencils_[a.stencil].type == 0 || loop->mgrid_ok, E_UNSUPPORTED,
+        OPSB_REQUIRE(p.cls == 'A', E_ARG, "loop " + loop->kernel + ": arg " + std::to_string(i) + " is a dat but the kernel expects a pointer");
+        OPSB_REQUIRE(p.elem == dt.type_size, E_ARG, "loop " + loop->kernel + ": dat " + dt.name + " element size mismatch");
+        OPSB_REQUIRE(dt.dim == 1, E_UNSUPPORTED, "dat " + dt.name + ": multi-component dats are not supported by loop kernels");
+        OPSB_REQUIRE(dt.plane < (1LL << 31), E_UNSUPPORTED, "dat " + dt.name + " has a plane of 2^31 elements or more");
+        OPSB_REQUIRE(dt.block == blk, E_ARG, "dat " + dt.name + " is declared on another block");
+        OPSB_REQUIRE(dt.locked == 0, E_STATE, "dat " + dt.name + " is used in a loop while its raw pointer is held (ops_lib_core.cpp:2321)");
+        OPSB_REQUIRE(stencils_[a.stencil].type == 0 || loop->mgrid_ok, E_UNSUPPORTED,
                 "loop " + loop->kernel + " is not built for restrict/prolong stencils (mgrid)");
         check_in_allocation(d, a, dt);
         if (a.acc != ACC_READ) dt.host.clear();
         break;
       }
       case ARG_GBL:
-        require(p.cls == 'c' || p.cls == 'p', E_ARG, "loop " + loop->kernel + ": arg " + std::to_string(i) + " is a global but the kernel expects an accessor");
-        require(a.gbl.size() <= 4096, E_ARG, "global argument larger than 4 KiB");
+        OPSB_REQUIRE(p.cls == 'c' || p.cls == 'p', E_ARG, "loop " + loop->kernel + ": arg " + std::to_string(i) + " is a global but the kernel expects an accessor");
+        OPSB_REQUIRE(a.gbl.size() <= 4096, E_ARG, "global argument larger than 4 KiB");
         break;
       case ARG_REDUCE: {
         Reduction &r = reduction(a.red);
-        require(p.cls == 'R', E_ARG, "loop " + loop->kernel + ": reduction arg must bind to a RED<> parameter");
-        require(a.dim <= p.ndim, E_ARG, "reduction " + r.name + " wider than the kernel's accumulator");
-        require(p.elem == r.elem, E_ARG, "reduction " + r.name + " type does not match the kernel parameter");
-        require(a.dim <= OPSB_MAX_RED_DIM && a.dim * r.elem <= r.size, E_ARG, "reduction " + r.name + " too wide");
-        require(nred < OPSB_MAX_REDUCE_ARGS, E_ARG, "too many reductions in one loop");
-        require(a.acc == ACC_INC || a.acc == ACC_MIN || a.acc == ACC_MAX, E_ARG, "reduction access must be INC, MIN or MAX");
+        OPSB_REQUIRE(p.cls == 'R', E_ARG, "loop " + loop->kernel + ": reduction arg must bind to a RED<> parameter");
+        OPSB_REQUIRE(a.dim <= p.ndim, E_ARG, "reduction " + r.name + " wider than the kernel's accumulator");
+        OPSB_REQUIRE(p.elem == r.elem, E_ARG, "reduction " + r.name + " type does not match the kernel parameter");
+        OPSB_REQUIRE(a.dim <= OPSB_MAX_RED_DIM && a.dim * r.elem <= r.size, E_ARG, "reduction " + r.name + " too wide");
+        OPSB_REQUIRE(nred < OPSB_MAX_REDUCE_ARGS, E_ARG, "too many reductions in one loop");
+        OPSB_REQUIRE(a.acc == ACC_INC || a.acc == ACC_MIN || a.acc == ACC_MAX, E_ARG, "reduction access must be INC, MIN or MAX");
         // ops_arg_reduce_core (ops/c/src/core/ops_lib_core.cpp:856): the first use after a result restarts.
         d.red_first[i] = r.initialized ? 0 : 1;
         r.initialized = 1;
@@ -358,7 +361,7 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         break;
       }
       case ARG_IDX:
-        require(p.cls == 'I', E_ARG, "ops_arg_idx must bind to an IDX parameter");
+        OPSB_REQUIRE(p.cls == 'I', E_ARG, "ops_arg_idx must bind to an IDX parameter");
         break;
       default:
         throw Error(E_ARG, "unknown arg kind");
@@ -408,7 +411,7 @@ void Runtime::check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) co
       lo = hi = 0;
     }
     const long long first = (long long)dt.base[k] + dt.d_m[k], last = first + dt.size[k] - 1;
-    require(lo >= first && hi <= last, E_ARG,
+    OPSB_REQUIRE(lo >= first && hi <= last, E_ARG,
             "loop " + d.loop->kernel + ": dat " + dt.name + " accessed at [" + std::to_string(lo) + ", " +
                 std::to_string(hi) + "] in dimension " + std::to_string(k) + ", allocated [" +
                 std::to_string(first) + ", " + std::to_string(last) + "]");
@@ -688,7 +691,7 @@ void Runtime::run_queue(std::vector<Desc> &q) {
       const Arg &a = d.args[i];
       if (a.kind != ARG_GBL) continue;
       size_t off = (gbl_used_ + 15) & ~(size_t)15;
-      require(off + a.gbl.size() <= gbl_cap_, E_UNSUPPORTED, "global argument arena exhausted in one flush");
+      OPSB_REQUIRE(off + a.gbl.size() <= gbl_cap_, E_UNSUPPORTED, "global argument arena exhausted in one flush");
       memcpy(gbl_host_.data() + off, a.gbl.data(), a.gbl.size());
       d.gbl_off[i] = off;
       gbl_used_ = off + a.gbl.size();
@@ -764,10 +767,10 @@ void Runtime::reduction_result(int handle, void *out) {
 void Runtime::dat_set_data(int di, const void *host, size_t bytes) {
   execute();
   Dat &d = dat(di);
-  require(d.locked == 0, E_STATE, "ops_dat_set_data on a dat whose raw pointer is held");
+  OPSB_REQUIRE(d.locked == 0, E_STATE, "ops_dat_set_data on a dat whose raw pointer is held");
   size_t row = (size_t)d.size[0] * d.elem_size;
   size_t rows = (size_t)d.size[1] * d.size[2];
-  require(bytes == row * rows, E_ARG, "ops_dat_set_data: buffer size does not match the dat extent");
+  OPSB_REQUIRE(bytes == row * rows, E_ARG, "ops_dat_set_data: buffer size does not match the dat extent");
   OPSB_CUDA(cudaMemcpy2DAsync(d.data_d + (size_t)d.pad_front * d.elem_size, (size_t)d.pitch * d.elem_size, host, row,
                               row, rows, cudaMemcpyHostToDevice, stream_));
   OPSB_CUDA(cudaStreamSynchronize(stream_));
@@ -779,7 +782,7 @@ void Runtime::dat_fetch_data(int di, void *host, size_t bytes) {
   Dat &d = dat(di);
   size_t row = (size_t)d.size[0] * d.elem_size;
   size_t rows = (size_t)d.size[1] * d.size[2];
-  require(bytes == row * rows, E_ARG, "ops_dat_fetch_data: buffer size does not match the dat extent");
+  OPSB_REQUIRE(bytes == row * rows, E_ARG, "ops_dat_fetch_data: buffer size does not match the dat extent");
   OPSB_CUDA(cudaMemcpy2DAsync(host, row, d.data_d + (size_t)d.pad_front * d.elem_size, (size_t)d.pitch * d.elem_size,
                               row, rows, cudaMemcpyDeviceToHost, stream_));
   OPSB_CUDA(cudaStreamSynchronize(stream_));
@@ -798,7 +801,7 @@ void Runtime::dat_get_extents(int di, int *disp, int *size) {
 char *Runtime::dat_get_raw_pointer(int di, int memspace, int *stride_elems) {
   execute();
   Dat &d = dat(di);
-  require(d.locked == 0, E_STATE, "raw pointer already held for dat " + d.name);
+  OPSB_REQUIRE(d.locked == 0, E_STATE, "raw pointer already held for dat " + d.name);
   if (stride_elems) {
     stride_elems[0] = (int)d.pitch;
     stride_elems[1] = d.size[1];
@@ -818,7 +821,7 @@ char *Runtime::dat_get_raw_pointer(int di, int memspace, int *stride_elems) {
 
 void Runtime::dat_release_raw_data(int di, int acc) {
   Dat &d = dat(di);
-  require(d.locked != 0, E_STATE, "ops_dat_release_raw_data without a matching ops_dat_get_raw_pointer");
+  OPSB_REQUIRE(d.locked != 0, E_STATE, "ops_dat_release_raw_data without a matching ops_dat_get_raw_pointer");
   if (d.locked == 1 && acc != ACC_READ) {
     OPSB_CUDA(cudaMemcpyAsync(d.data_d, d.host.data(), d.bytes, cudaMemcpyHostToDevice, stream_));
     OPSB_CUDA(cudaStreamSynchronize(stream_));
@@ -848,7 +851,7 @@ void Runtime::dat_swap(int a, int b) {
   execute();
   Dat &x = dat(a);
   Dat &y = dat(b);
-  require(x.bytes == y.bytes && x.pitch == y.pitch && x.origin == y.origin && x.elem_size == y.elem_size, E_ARG,
+  OPSB_REQUIRE(x.bytes == y.bytes && x.pitch == y.pitch && x.origin == y.origin && x.elem_size == y.elem_size, E_ARG,
           "dat_swap needs two dats of identical layout");
   std::swap(x.data_d, y.data_d);
   x.host.clear();
