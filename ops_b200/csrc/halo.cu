@@ -71,23 +71,25 @@ __global__ void k_halo(const HaloDev *__restrict__ hs, int nh, long long total) 
 
 bool is_float_type(const std::string &t) { return t == "double" || t == "float"; }
 
-void require(bool cond, int code, const std::string &msg) {
-  if (!cond) throw Error(code, msg);
-}
+// A checked condition whose message is built only when the check fails.
+#define HALO_REQUIRE(cond, code, msg)        \
+  do {                                       \
+    if (!(cond)) throw Error((code), (msg)); \
+  } while (0)
 
 }  // namespace
 
 int Runtime::decl_halo(int from, int to, const int *iter, const int *from_base, const int *to_base,
                        const int *from_dir, const int *to_dir) {
-  require(inited_, E_STATE, "ops_decl_halo before ops_init");
-  require(iter && from_base && to_base && from_dir && to_dir, E_ARG, "ops_decl_halo: null array");
+  HALO_REQUIRE(inited_, E_STATE, "ops_decl_halo before ops_init");
+  HALO_REQUIRE(iter && from_base && to_base && from_dir && to_dir, E_ARG, "ops_decl_halo: null array");
   Dat &f = dat(from);
   Dat &t = dat(to);
   const int dims = blocks_[f.block].dims;
-  require(blocks_[t.block].dims == dims, E_ARG, "ops_decl_halo: the two dats' blocks differ in dimension");
-  require(f.dim == t.dim, E_ARG, "ops_decl_halo: the two dats differ in components per point");
+  HALO_REQUIRE(blocks_[t.block].dims == dims, E_ARG, "ops_decl_halo: the two dats' blocks differ in dimension");
+  HALO_REQUIRE(f.dim == t.dim, E_ARG, "ops_decl_halo: the two dats differ in components per point");
   if (f.type != t.type || f.type_size != t.type_size)
-    require(is_float_type(f.type) && is_float_type(t.type), E_UNSUPPORTED,
+    HALO_REQUIRE(is_float_type(f.type) && is_float_type(t.type), E_UNSUPPORTED,
             "ops_decl_halo: a mixed exchange is supported between float and double only");
   Halo h;
   h.from = from;
@@ -99,7 +101,7 @@ int Runtime::decl_halo(int from, int to, const int *iter, const int *from_base, 
     h.tbase[i] = real ? to_base[i] : 0;
     h.fdir[i] = real ? from_dir[i] : i + 1;
     h.tdir[i] = real ? to_dir[i] : i + 1;
-    require(h.iter[i] >= 0, E_ARG, "ops_decl_halo: negative iteration size");
+    HALO_REQUIRE(h.iter[i] >= 0, E_ARG, "ops_decl_halo: negative iteration size");
   }
   // directions: a permutation of +-1..dims for each side
   for (int side = 0; side < 2; side++) {
@@ -107,7 +109,7 @@ int Runtime::decl_halo(int from, int to, const int *iter, const int *from_base, 
     int seen = 0;
     for (int i = 0; i < dims; i++) {
       const int a = std::abs(dir[i]);
-      require(a >= 1 && a <= dims && !(seen & (1 << a)), E_ARG, "ops_decl_halo: directions must permute +-1..dims");
+      HALO_REQUIRE(a >= 1 && a <= dims && !(seen & (1 << a)), E_ARG, "ops_decl_halo: directions must permute +-1..dims");
       seen |= 1 << a;
     }
   }
@@ -120,7 +122,7 @@ int Runtime::decl_halo(int from, int to, const int *iter, const int *from_base, 
       const int n = h.iter[std::abs(dir[i]) - 1];
       if (n == 0) continue;
       const int lo = d.base[i] + d.d_m[i], hi = lo + d.size[i];
-      require(base[i] >= lo && base[i] + n <= hi, E_ARG,
+      HALO_REQUIRE(base[i] >= lo && base[i] + n <= hi, E_ARG,
               "ops_decl_halo: the box on dat " + d.name + " leaves its allocation in dimension " + std::to_string(i));
     }
   }
@@ -129,11 +131,11 @@ int Runtime::decl_halo(int from, int to, const int *iter, const int *from_base, 
 }
 
 int Runtime::decl_halo_group(int n, const int *halos) {
-  require(inited_, E_STATE, "ops_decl_halo_group before ops_init");
-  require(n >= 0 && (n == 0 || halos), E_ARG, "ops_decl_halo_group: bad list");
+  HALO_REQUIRE(inited_, E_STATE, "ops_decl_halo_group before ops_init");
+  HALO_REQUIRE(n >= 0 && (n == 0 || halos), E_ARG, "ops_decl_halo_group: bad list");
   std::vector<int> g;
   for (int i = 0; i < n; i++) {
-    require(halos[i] >= 0 && halos[i] < (int)halos_.size(), E_ARG, "ops_decl_halo_group: unknown halo");
+    HALO_REQUIRE(halos[i] >= 0 && halos[i] < (int)halos_.size(), E_ARG, "ops_decl_halo_group: unknown halo");
     g.push_back(halos[i]);
   }
   halo_groups_.push_back(g);
@@ -141,7 +143,7 @@ int Runtime::decl_halo_group(int n, const int *halos) {
 }
 
 void Runtime::halo_transfer(int group) {
-  require(group >= 0 && group < (int)halo_groups_.size(), E_ARG, "ops_halo_transfer: unknown group");
+  HALO_REQUIRE(group >= 0 && group < (int)halo_groups_.size(), E_ARG, "ops_halo_transfer: unknown group");
   const std::vector<int> &g = halo_groups_[group];
   if (g.empty()) return;
   execute();  // loops queued before the transfer see the old halos, loops after it the new ones
@@ -150,7 +152,7 @@ void Runtime::halo_transfer(int group) {
     const Halo &h = halos_[hi];
     const Dat &f = dat(h.from);
     const Dat &t = dat(h.to);
-    require(f.locked == 0 && t.locked == 0, E_STATE, "ops_halo_transfer on a dat whose raw pointer is held");
+    HALO_REQUIRE(f.locked == 0 && t.locked == 0, E_STATE, "ops_halo_transfer on a dat whose raw pointer is held");
     HaloDev d;
     memset(&d, 0, sizeof(d));
     d.src = f.origin_ptr();
