@@ -59,9 +59,9 @@ struct Clover {
     memset(&field, 0, sizeof(field));
   }
 
+  PrefixedLoops loops{"cloverleaf/"};
   void loop(const char *k, const char *name, const int *range, std::initializer_list<Arg> a) {
-    std::string full = std::string("cloverleaf/") + k;
-    par_loop_named(full.c_str(), name, clover_grid, 2, range, a);
+    r.par_loop(loops.get(k), name, clover_grid, 2, range, a.begin(), (int)a.size());
   }
   Arg dat(int d, int s, int acc) { return arg_dat(d, 1, s, acc); }
   Arg dat_opt(int d, int s, int acc, int flag) { return arg_dat_opt(d, 1, s, acc, flag); }

@@ -69,9 +69,9 @@ struct Clover3D {
     memset(&field, 0, sizeof(field));
   }
 
+  PrefixedLoops loops{"cloverleaf3d/"};
   void loop(const char *k, const char *name, const int *range, std::initializer_list<Arg> a) {
-    std::string full = std::string("cloverleaf3d/") + k;
-    par_loop_named(full.c_str(), name, clover_grid, 3, range, a);
+    r.par_loop(loops.get(k), name, clover_grid, 3, range, a.begin(), (int)a.size());
   }
   void loop(const char *k, const int *range, std::initializer_list<Arg> a) { loop(k, k, range, a); }
   Arg dat(int d, int s, int acc) { return arg_dat(d, 1, s, acc); }
@@ -657,8 +657,7 @@ struct Clover3D {
       std::vector<Arg> a = {dat(work_array6, S000, ACC_WRITE), dat(work_array7, S000, ACC_WRITE),
                             dat(volume, S000, ACC_READ)};
       a.insert(a.end(), fluxes.begin(), fluxes.end());
-      std::string full = std::string("cloverleaf3d/") + k;
-      par_loop_named(full.c_str(), k, clover_grid, 3, rangexyz, a);
+      r.par_loop(loops.get(k), k, clover_grid, 3, rangexyz, a.data(), (int)a.size());
     };
     if (sweep_number == 1 && dir == 1)
       pre("advec_mom_kernel_x1", {dat(vol_flux_x, S_P100, ACC_READ), dat(vol_flux_y, S_0P10, ACC_READ),

@@ -72,9 +72,9 @@ struct Tea {
       if (e) cudaEventDestroy(e);
   }
 
+  PrefixedLoops loops{"tealeaf/"};
   void loop(const char *k, const int *range, std::initializer_list<Arg> a) {
-    std::string full = std::string("tealeaf/") + k;
-    par_loop_named(full.c_str(), k, tea_grid, 2, range, a);
+    r.par_loop(loops.get(k), k, tea_grid, 2, range, a.begin(), (int)a.size());
   }
   Arg dat(int d, int s, int acc) { return arg_dat(d, 1, s, acc); }
   int stencil(int points, std::initializer_list<int> offs, const char *name) {

@@ -383,6 +383,29 @@ inline void par_loop_named(const char *kernel, const char *name, int block, int 
   Runtime::get().par_loop(li, name, block, dim, range, args.data(), (int)args.size());
 }
 
+// Loop kernels of one app looked up once: "<prefix><name>" resolved on the
+// first call for a name and kept (keyed by the name's hash, confirmed by
+// comparing the text), so the app drivers' per-loop path builds no strings.
+class PrefixedLoops {
+ public:
+  explicit PrefixedLoops(const char *prefix) : prefix_(prefix) {}
+  const LoopInfo *get(const char *name) {
+    uint64_t h = 0xCBF29CE484222325ULL;
+    for (const char *c = name; *c; c++) h = (h ^ (unsigned char)*c) * 0x100000001B3ULL;
+    auto it = cache_.find(h);
+    if (it != cache_.end() && it->second.first == name) return it->second.second;
+    const std::string full = prefix_ + name;
+    const LoopInfo *li = Runtime::find_loop(full);
+    if (!li) throw Error(E_NOTFOUND, "no registered loop kernel named " + full);
+    cache_[h] = {std::string(name), li};
+    return li;
+  }
+
+ private:
+  std::string prefix_;
+  std::unordered_map<uint64_t, std::pair<std::string, const LoopInfo *>> cache_;
+};
+
 // ops_par_loop(kernel, name, block, dim, range, args...) for a functor K.
 template <class K>
 void par_loop(const char *name, int block, int dim, const int *range, std::initializer_list<Arg> args) {
