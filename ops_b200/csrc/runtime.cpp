@@ -86,6 +86,7 @@ Runtime::~Runtime() {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   for (auto &d : dats_)
     if (d && d->data_d) cudaFree(d->data_d);
+  for (auto &kv : spare_) cudaFree(kv.second);
   if (red_arena_) cudaFree(red_arena_);
   if (gbl_dev_) cudaFree(gbl_dev_);
   if (red_scratch_) cudaFree(red_scratch_);
@@ -205,7 +206,7 @@ int Runtime::decl_dat(int blk, int dim, const int *size, const int *base, const 
   d->origin = d->pad_front + (long long)(-d->base[0] - d->d_m[0]) + (long long)(-d->base[1] - d->d_m[1]) * d->pitch +
               (long long)(-d->base[2] - d->d_m[2]) * d->plane;
   d->bytes = (size_t)d->plane * d->size[2] * e;
-  OPSB_CUDA(cudaMalloc(&d->data_d, d->bytes > 0 ? d->bytes : 256));
+  d->data_d = alloc_dat_storage(d->bytes);
   OPSB_CUDA(cudaMemsetAsync(d->data_d, 0, d->bytes, stream_));
   int idx = d->index;
   dats_.push_back(std::move(d));
@@ -837,7 +838,7 @@ void Runtime::release_to(const Mark &m) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   graphs_.clear();
   while (dats_.size() > m.dats) {
-    if (dats_.back() && dats_.back()->data_d) cudaFree(dats_.back()->data_d);
+    if (dats_.back() && dats_.back()->data_d) recycle_dat_storage(dats_.back()->data_d, dats_.back()->bytes);
     dats_.pop_back();
   }
   while (reductions_.size() > m.reductions) {
@@ -845,6 +846,31 @@ void Runtime::release_to(const Mark &m) {
   }
   stencils_.resize(std::min(stencils_.size(), m.stencils));
   blocks_.resize(std::min(blocks_.size(), m.blocks));
+}
+
+char *Runtime::alloc_dat_storage(size_t bytes) {
+  const size_t n = bytes > 0 ? bytes : 256;
+  auto it = spare_.find(n);
+  if (it != spare_.end()) {
+    char *p = it->second;
+    spare_.erase(it);
+    spare_bytes_ -= n;
+    return p;
+  }
+  char *p = nullptr;
+  OPSB_CUDA(cudaMalloc(&p, n));
+  return p;
+}
+
+// Called with the stream idle (release_to synchronizes first).
+void Runtime::recycle_dat_storage(char *p, size_t bytes) {
+  const size_t n = bytes > 0 ? bytes : 256;
+  if (spare_bytes_ + n > kSpareCap) {
+    cudaFree(p);
+    return;
+  }
+  spare_.emplace(n, p);
+  spare_bytes_ += n;
 }
 
 void Runtime::dat_swap(int a, int b) {

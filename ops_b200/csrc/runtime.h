@@ -247,6 +247,14 @@ class Runtime {
   cudaStream_t stream_ = nullptr;
   std::vector<Block> blocks_;
   std::vector<std::unique_ptr<Dat>> dats_;
+  // Dat storage given back by release_to (an app driver's teardown), kept
+  // by size for the next dats of the same size instead of cudaFree /
+  // cudaMalloc of gigabytes per app call; at most kSpareCap bytes are kept.
+  static constexpr size_t kSpareCap = (size_t)64 << 30;
+  std::multimap<size_t, char *> spare_;
+  size_t spare_bytes_ = 0;
+  char *alloc_dat_storage(size_t bytes);
+  void recycle_dat_storage(char *p, size_t bytes);
   struct Halo {
     int from = -1, to = -1;
     int iter[3], fbase[3], tbase[3], fdir[3], tdir[3];
