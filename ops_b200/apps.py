@@ -11,14 +11,19 @@ def _ptr(a):
     return None if a is None else a.ctypes.data
 
 
-def laplace2d(field, iters, warmup=0, return_errors=True):
+def laplace2d(field, iters, warmup=0, return_errors=True, out=None):
     """Laplace Jacobi (apps/c/laplace2d_tutorial/step7/laplace2d.cpp:113-124).
 
     field: (jmax+2, imax+2) float64 full extent (ring = boundary values).
+    out: optional C-contiguous float64 array of the same shape that receives
+    the final field (e.g. pinned host memory); a new array otherwise.
     Returns (final_field, errors_per_iteration, device_seconds)."""
     field = np.ascontiguousarray(field, dtype=np.float64)
     jmax, imax = field.shape[0] - 2, field.shape[1] - 2
-    out = np.empty_like(field)
+    if out is None:
+        out = np.empty_like(field)
+    elif out.shape != field.shape or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+        raise ValueError("out must be a C-contiguous float64 array shaped like field")
     errs = np.empty(max(warmup + iters, 1), dtype=np.float64) if return_errors else None
     secs = ctypes.c_double(0.0)
     check(lib().ops_b200_app_laplace2d(imax, jmax, warmup, iters, _ptr(field), _ptr(out), _ptr(errs),
