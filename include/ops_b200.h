@@ -167,6 +167,13 @@ int ops_b200_counters(long long *kernels, long long *graphs, long long *loops);
  * counterpart; disabled with the "fusion" option). */
 int ops_b200_loops_skipped(long long *skipped);
 int ops_b200_reset_counters(void);
+/* Dat storage that the app drivers give back when they return is kept for
+ * the next dats of the same size (no cudaFree/cudaMalloc of gigabytes per
+ * call). This frees the kept blocks now (they are also freed and the
+ * allocation retried when a dat allocation runs out of device memory) and
+ * stores the bytes given back in *freed (may be NULL). No reference
+ * counterpart. */
+int ops_b200_release_spare_storage(long long *freed);
 
 /* Per-kernel device timing: while enabled, every launch is bracketed by CUDA
  * events on the runtime stream (graph replay is bypassed). Query by kernel
@@ -315,6 +322,29 @@ int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summaries, int m
  * one GPU. Queued loops are flushed first. */
 int ops_b200_tridMultiDimBatch(int ndim, int solvedim, const int *range, int a, int b, int c, int d);
 int ops_b200_tridMultiDimBatch_Inc(int ndim, int solvedim, const int *range, int a, int b, int c, int d, int u);
+
+/* ops_tridsolver_params (ops/c/include/ops_tridiag.h:45-72): the strategy
+ * and tuning values of Tridsolver's multi-process solves, held in a plain
+ * struct instead of the reference's class. _init stands for both
+ * constructors (strategy -1 = the reference's default, GATHER_SCATTER = 0;
+ * JACOBI 2, PCR 3, LATENCY_HIDING_INTERLEAVED 4, LATENCY_HIDING_TWO_STEP 5);
+ * the setters mirror set_jacobi_params, set_batch_size, set_cuda_opts and
+ * set_cuda_sync and only record their values: as in the reference's
+ * single-process backends (ops/c/src/tridiag/ops_tridiag.cpp:48-76), nothing
+ * on one GPU reads them. Invalid values are OPS_B200_ERR_ARG. */
+typedef struct ops_b200_tridsolver_params {
+  int block, strategy;
+  double jacobi_rtol, jacobi_atol;
+  int jacobi_maxiter, batch_size;
+  int cuda_opts[3];
+  int cuda_sync;
+} ops_b200_tridsolver_params;
+int ops_b200_tridsolver_params_init(ops_b200_tridsolver_params *p, int block, int strategy);
+int ops_b200_tridsolver_params_set_jacobi_params(ops_b200_tridsolver_params *p, double rtol, double atol,
+                                                 int maxiter);
+int ops_b200_tridsolver_params_set_batch_size(ops_b200_tridsolver_params *p, int batch_size);
+int ops_b200_tridsolver_params_set_cuda_opts(ops_b200_tridsolver_params *p, int opt_x, int opt_y, int opt_z);
+int ops_b200_tridsolver_params_set_cuda_sync(ops_b200_tridsolver_params *p, int sync);
 
 /* One strided system set, as Tridsolver's trid{D,S}mtsvStridedBatch[Inc]
  * takes it (call sites ops/c/src/tridiag/ops_tridiag.cpp:126,140,219,236):

@@ -37,6 +37,12 @@ class TridSystem(ctypes.Structure):
                 ("pads", ctypes.c_int * 3)]
 
 
+class TridsolverParams(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int), ("strategy", ctypes.c_int), ("jacobi_rtol", ctypes.c_double),
+                ("jacobi_atol", ctypes.c_double), ("jacobi_maxiter", ctypes.c_int), ("batch_size", ctypes.c_int),
+                ("cuda_opts", ctypes.c_int * 3), ("cuda_sync", ctypes.c_int)]
+
+
 class KernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 96), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double),
                 ("alg_bytes", ctypes.c_double)]
@@ -160,6 +166,12 @@ def _declare(L):
         "ops_b200_set_option": ([cp, i], i),
         "ops_b200_counters": ([P, P, P], i),
         "ops_b200_reset_counters": ([], i),
+        "ops_b200_release_spare_storage": ([P], i),
+        "ops_b200_tridsolver_params_init": ([P, i, i], i),
+        "ops_b200_tridsolver_params_set_jacobi_params": ([P, d, d, i], i),
+        "ops_b200_tridsolver_params_set_batch_size": ([P, i], i),
+        "ops_b200_tridsolver_params_set_cuda_opts": ([P, i, i, i], i),
+        "ops_b200_tridsolver_params_set_cuda_sync": ([P, i], i),
         "ops_b200_set_kernel_timing": ([i], i),
         "ops_b200_kernel_time": ([cp, P, P], i),
         "ops_b200_clear_kernel_timing": ([], i),

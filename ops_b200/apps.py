@@ -24,6 +24,8 @@ def laplace2d(field, iters, warmup=0, return_errors=True, out=None):
         out = np.empty_like(field)
     elif out.shape != field.shape or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
         raise ValueError("out must be a C-contiguous float64 array shaped like field")
+    elif not out.flags["WRITEABLE"]:
+        raise ValueError("out must be writeable (the final field is written into it)")
     errs = np.empty(max(warmup + iters, 1), dtype=np.float64) if return_errors else None
     secs = ctypes.c_double(0.0)
     check(lib().ops_b200_app_laplace2d(imax, jmax, warmup, iters, _ptr(field), _ptr(out), _ptr(errs),

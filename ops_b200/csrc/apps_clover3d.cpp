@@ -844,12 +844,12 @@ extern "C" int ops_b200_app_cloverleaf3d(const ops_b200_clover3d_deck *deck, int
       throw Error(E_ARG, "x_cells, y_cells and z_cells must be >= 2");
     Runtime &r = Runtime::get();
     if (!r.initialized()) r.init(0, 0);
-    Runtime::Mark mk = r.mark();
+    ReleaseScope scope(r);
+    const Runtime::Mark &mk = scope.mark();
     clover3d::Clover3D c(r);
     c.setup(*deck);
-    cudaEvent_t e0, e1;
-    OPSB_CUDA(cudaEventCreate(&e0));
-    OPSB_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     bool started = false;
     if (warmup_steps == 0) {
       r.execute();
@@ -869,11 +869,7 @@ extern "C" int ops_b200_app_cloverleaf3d(const ops_b200_clover3d_deck *deck, int
     OPSB_CUDA(cudaEventRecord(e1, r.stream()));
     if (!started) OPSB_CUDA(cudaEventRecord(e0, r.stream()));
     OPSB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    OPSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (device_seconds) *device_seconds = ms * 1e-3;
+    if (device_seconds) *device_seconds = ev.ms() * 1e-3;
     int n = (int)(c.summaries.size() / 8);
     if (n_summaries) *n_summaries = n;
     if (summaries) memcpy(summaries, c.summaries.data(), sizeof(double) * 8 * std::min(n, max_summaries));
@@ -889,7 +885,7 @@ extern "C" int ops_b200_app_cloverleaf3d(const ops_b200_clover3d_deck *deck, int
         fclose(f);
       }
     }
-    r.release_to(mk);
+    scope.release();
     return 0;
   });
 }

@@ -27,7 +27,7 @@ extern "C" int ops_b200_app_laplace2d(int imax, int jmax, int warmup, int iters,
     if (imax <= 0 || jmax <= 0 || iters < 0 || warmup < 0 || !field_in) throw Error(E_ARG, "bad Laplace arguments");
     Runtime &r = Runtime::get();
     if (!r.initialized()) r.init(0, 0);
-    Runtime::Mark mk = r.mark();
+    ReleaseScope scope(r);
     int block = r.decl_block(2, "my_grid");
     int size[] = {imax, jmax}, base[] = {0, 0}, d_m[] = {-1, -1}, d_p[] = {1, 1};
     int dA = r.decl_dat(block, 1, size, base, d_m, d_p, field_in, 8, "double", "A");
@@ -40,9 +40,8 @@ extern "C" int ops_b200_app_laplace2d(int imax, int jmax, int warmup, int iters,
     r.decl_const("imax", 1, "int", &imax);
     r.decl_const("jmax", 1, "int", &jmax);
 
-    cudaEvent_t e0, e1;
-    OPSB_CUDA(cudaEventCreate(&e0));
-    OPSB_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     int interior[] = {0, imax, 0, jmax};
     double error = 1.0;
     for (int it = 0; it < warmup + iters; it++) {
@@ -59,13 +58,9 @@ extern "C" int ops_b200_app_laplace2d(int imax, int jmax, int warmup, int iters,
     r.execute();
     OPSB_CUDA(cudaEventRecord(e1, r.stream()));
     OPSB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    OPSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (device_seconds) *device_seconds = ms * 1e-3;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (device_seconds) *device_seconds = ev.ms() * 1e-3;
     if (field_out) r.dat_fetch_data(dA, field_out, (size_t)(imax + 2) * (jmax + 2) * sizeof(double));
-    r.release_to(mk);
+    scope.release();
     return 0;
   });
 }

@@ -899,12 +899,12 @@ extern "C" int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summa
     if (deck->x_cells < 2 || deck->y_cells < 2) throw Error(E_ARG, "x_cells and y_cells must be >= 2");
     Runtime &r = Runtime::get();
     if (!r.initialized()) r.init(0, 0);
-    Runtime::Mark mk = r.mark();
+    ReleaseScope scope(r);
+    const Runtime::Mark &mk = scope.mark();
     tea::Tea t(r);
     t.setup(*deck);
-    cudaEvent_t e0, e1;
-    OPSB_CUDA(cudaEventCreate(&e0));
-    OPSB_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     r.execute();
     OPSB_CUDA(cudaEventRecord(e0, r.stream()));
     while (!t.cycle()) {
@@ -912,11 +912,7 @@ extern "C" int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summa
     r.execute();
     OPSB_CUDA(cudaEventRecord(e1, r.stream()));
     OPSB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    OPSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (device_seconds) *device_seconds = ms * 1e-3;
+    if (device_seconds) *device_seconds = ev.ms() * 1e-3;
     int n = (int)(t.summaries.size() / 6), ns = (int)(t.solves.size() / OPS_B200_TEA_SOLVE_COLS);
     if (n_summaries) *n_summaries = n;
     if (n_solves) *n_solves = ns;
@@ -935,7 +931,7 @@ extern "C" int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summa
         fclose(f);
       }
     }
-    r.release_to(mk);
+    scope.release();
     return 0;
   });
 }

@@ -254,6 +254,63 @@ int ops_b200_counters(long long *kernels, long long *graphs, long long *loops) {
   });
 }
 
+int ops_b200_release_spare_storage(long long *freed) {
+  return guarded([&] {
+    long long n = (long long)rt().release_spare_storage();
+    if (freed) *freed = n;
+    return 0;
+  });
+}
+
+int ops_b200_tridsolver_params_init(ops_b200_tridsolver_params *p, int block, int strategy) {
+  return guarded([&] {
+    if (!p) throw opsb::Error(opsb::E_ARG, "ops_tridsolver_params: NULL params");
+    if (strategy < -1 || strategy > 5) throw opsb::Error(opsb::E_ARG, "ops_tridsolver_params: unknown strategy");
+    std::memset(p, 0, sizeof(*p));
+    p->block = block;
+    p->strategy = strategy < 0 ? 0 : strategy;
+    return 0;
+  });
+}
+
+int ops_b200_tridsolver_params_set_jacobi_params(ops_b200_tridsolver_params *p, double rtol, double atol,
+                                                 int maxiter) {
+  return guarded([&] {
+    if (!p || !(rtol >= 0.0) || !(atol >= 0.0) || maxiter < 0)
+      throw opsb::Error(opsb::E_ARG, "set_jacobi_params: tolerances and maxiter must be non-negative");
+    p->jacobi_rtol = rtol;
+    p->jacobi_atol = atol;
+    p->jacobi_maxiter = maxiter;
+    return 0;
+  });
+}
+
+int ops_b200_tridsolver_params_set_batch_size(ops_b200_tridsolver_params *p, int batch_size) {
+  return guarded([&] {
+    if (!p || batch_size < 0) throw opsb::Error(opsb::E_ARG, "set_batch_size: batch size must be non-negative");
+    p->batch_size = batch_size;
+    return 0;
+  });
+}
+
+int ops_b200_tridsolver_params_set_cuda_opts(ops_b200_tridsolver_params *p, int opt_x, int opt_y, int opt_z) {
+  return guarded([&] {
+    if (!p) throw opsb::Error(opsb::E_ARG, "set_cuda_opts: NULL params");
+    p->cuda_opts[0] = opt_x;
+    p->cuda_opts[1] = opt_y;
+    p->cuda_opts[2] = opt_z;
+    return 0;
+  });
+}
+
+int ops_b200_tridsolver_params_set_cuda_sync(ops_b200_tridsolver_params *p, int sync) {
+  return guarded([&] {
+    if (!p) throw opsb::Error(opsb::E_ARG, "set_cuda_sync: NULL params");
+    p->cuda_sync = sync;
+    return 0;
+  });
+}
+
 int ops_b200_reset_counters(void) {
   return guarded([&] {
     rt().reset_counters();

@@ -24,6 +24,7 @@
 //     call before any stream capture that should contain a sweep.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -41,8 +42,11 @@ constexpr int kBX = 128, kBY = 2;
 static __device__ __align__(256) double g_noalloc_scratch[kMaxBlocks + 1];
 
 // Device addresses of the scratch, one per device (host code cannot use the
-// symbol itself: on the host it names a shadow, not device memory).
-double *g_scratch_ptr[kMaxDevices] = {nullptr};
+// symbol itself: on the host it names a shadow, not device memory). Read
+// without the lock on every call, so each slot is atomic: the first call on
+// a device publishes the address with release order after looking it up,
+// later calls (any thread) read it with acquire order.
+std::atomic<double *> g_scratch_ptr[kMaxDevices];
 std::mutex g_setup_mutex;
 thread_local char g_err[256] = "no error";
 
@@ -113,17 +117,18 @@ extern "C" int ops_b200_laplace_sweep_noalloc(int imax, int jmax, const double *
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(OPS_B200_ERR_CUDA, "laplace_sweep_noalloc: no current CUDA device");
-  double *scratch = g_scratch_ptr[dev];
+  double *scratch = g_scratch_ptr[dev].load(std::memory_order_acquire);
   if (!scratch) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    scratch = g_scratch_ptr[dev].load(std::memory_order_relaxed);
+    if (!scratch) {
       void *p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p)
         return fail(OPS_B200_ERR_CUDA, "laplace_sweep_noalloc: cudaGetSymbolAddress failed for the scratch array");
-      g_scratch_ptr[dev] = static_cast<double *>(p);
+      scratch = static_cast<double *>(p);
+      g_scratch_ptr[dev].store(scratch, std::memory_order_release);
     }
-    scratch = g_scratch_ptr[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // The counter must start at zero; a previous call re-arms it, this makes

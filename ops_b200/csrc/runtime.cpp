@@ -848,6 +848,10 @@ void Runtime::release_to(const Mark &m) {
   blocks_.resize(std::min(blocks_.size(), m.blocks));
 }
 
+// Storage for a new dat: a kept block of exactly this size if there is one,
+// else a new allocation. When the device is out of memory the kept blocks
+// (which no other allocator in the process can use) are freed and the
+// allocation is tried once more.
 char *Runtime::alloc_dat_storage(size_t bytes) {
   const size_t n = bytes > 0 ? bytes : 256;
   auto it = spare_.find(n);
@@ -858,8 +862,34 @@ char *Runtime::alloc_dat_storage(size_t bytes) {
     return p;
   }
   char *p = nullptr;
-  OPSB_CUDA(cudaMalloc(&p, n));
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e == cudaErrorMemoryAllocation && !spare_.empty()) {
+    cudaGetLastError();  // clear the (non-sticky) allocation error
+    release_spare_storage();
+    p = nullptr;
+    e = cudaMalloc(&p, n);
+  }
+  cuda_check(e, "cudaMalloc of dat storage");
   return p;
+}
+
+size_t Runtime::release_spare_storage() {
+  if (spare_.empty()) return 0;
+  if (stream_) OPSB_CUDA(cudaStreamSynchronize(stream_));
+  size_t freed = 0;
+  for (auto &kv : spare_) {
+    cudaFree(kv.second);
+    freed += kv.first;
+  }
+  spare_.clear();
+  spare_bytes_ = 0;
+  return freed;
+}
+
+void Runtime::discard_queue() {
+  queue_.clear();
+  qrec_.clear();
+  dat_ver_.clear();
 }
 
 // Called with the stream idle (release_to synchronizes first).

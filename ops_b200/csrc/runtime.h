@@ -231,6 +231,13 @@ class Runtime {
   struct Mark { size_t blocks, dats, stencils, reductions; };
   Mark mark() const { return {blocks_.size(), dats_.size(), stencils_.size(), reductions_.size()}; }
   void release_to(const Mark &m);
+  // Drops the queued loops without running them (an app driver's error
+  // path, before it releases its declarations).
+  void discard_queue();
+  // Frees the dat storage kept for reuse (see alloc_dat_storage); returns
+  // the bytes given back.
+  size_t release_spare_storage();
+  size_t spare_storage_bytes() const { return spare_bytes_; }
 
   ~Runtime();
 
@@ -313,6 +320,58 @@ class Runtime {
   bool redundant(const Desc &d, LoopRecord &rec);
   void check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) const;
   long long kernels_launched_ = 0, graphs_launched_ = 0, loops_enqueued_ = 0;
+};
+
+// Releases an app call's declarations (blocks, dats, stencils, reductions
+// made after construction) when the scope ends, on the error paths too: a
+// driver that throws gives its dat storage back instead of holding it until
+// ops_b200_exit. On an error path the queued loops are dropped first, and a
+// failure while releasing (a CUDA error that poisoned the context, say) is
+// swallowed so that the original error reaches the caller.
+class ReleaseScope {
+ public:
+  explicit ReleaseScope(Runtime &r) : r_(r), m_(r.mark()) {}
+  ReleaseScope(const ReleaseScope &) = delete;
+  ReleaseScope &operator=(const ReleaseScope &) = delete;
+  ~ReleaseScope() {
+    if (done_) return;
+    try {
+      r_.discard_queue();
+      r_.release_to(m_);
+    } catch (...) {
+    }
+  }
+  // The normal path: release now, errors propagate.
+  void release() {
+    done_ = true;
+    r_.release_to(m_);
+  }
+  const Runtime::Mark &mark() const { return m_; }
+
+ private:
+  Runtime &r_;
+  Runtime::Mark m_;
+  bool done_ = false;
+};
+
+// Two CUDA events (start, end of a timed region) destroyed with the scope.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  EventPair() {
+    OPSB_CUDA(cudaEventCreate(&a));
+    OPSB_CUDA(cudaEventCreate(&b));
+  }
+  EventPair(const EventPair &) = delete;
+  EventPair &operator=(const EventPair &) = delete;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+  float ms() const {
+    float t = 0.f;
+    OPSB_CUDA(cudaEventElapsedTime(&t, a, b));
+    return t;
+  }
 };
 
 // ---------------------------------------------------------------------------

@@ -427,26 +427,35 @@ def ops_print_dat_to_txtfile(dat, file_name):
 
 class ops_tridsolver_params:
     """ops_tridsolver_params (ops/c/include/ops_tridiag.h:45-72): strategy and
-    tuning of Tridsolver's multi-process solves. The reference's
-    single-process backends ignore every setter (ops_tridiag.cpp:48-76); so
-    does this one. The values given are kept for callers that read them
-    back (None until set)."""
+    tuning of Tridsolver's multi-process solves, held by the C-ABI struct
+    ops_b200_tridsolver_params. The reference's single-process backends
+    ignore every setter (ops_tridiag.cpp:48-76); so does this one. The values
+    given are kept for callers that read them back (None until set)."""
     GATHER_SCATTER, ALLGATHER, JACOBI, PCR, LATENCY_HIDING_INTERLEAVED, LATENCY_HIDING_TWO_STEP = range(6)
 
     def __init__(self, block, strategy=None):
+        from ._lib import TridsolverParams
+        self._p = TridsolverParams()
+        handle = block if isinstance(block, int) else getattr(block, "index", -1)
+        check(lib().ops_b200_tridsolver_params_init(ctypes.byref(self._p), int(handle),
+                                                     -1 if strategy is None else int(strategy)))
         self.block, self.strategy = block, strategy
         self.jacobi = self.batch_size = self.cuda_opts = self.cuda_sync = None
 
     def set_jacobi_params(self, rtol, atol, maxiter):
+        check(lib().ops_b200_tridsolver_params_set_jacobi_params(ctypes.byref(self._p), rtol, atol, maxiter))
         self.jacobi = (rtol, atol, maxiter)
 
     def set_batch_size(self, batch_size):
+        check(lib().ops_b200_tridsolver_params_set_batch_size(ctypes.byref(self._p), batch_size))
         self.batch_size = batch_size
 
     def set_cuda_opts(self, opt_x, opt_y, opt_z):
+        check(lib().ops_b200_tridsolver_params_set_cuda_opts(ctypes.byref(self._p), opt_x, opt_y, opt_z))
         self.cuda_opts = (opt_x, opt_y, opt_z)
 
     def set_cuda_sync(self, sync):
+        check(lib().ops_b200_tridsolver_params_set_cuda_sync(ctypes.byref(self._p), sync))
         self.cuda_sync = sync
 
 

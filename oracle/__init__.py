@@ -41,9 +41,11 @@ def build():
     return LIB
 
 
-def build_reference(ref_root="/root/reference"):
-    """Build the reference OpenMP apps into oracle/_ref (needs the reference tree)."""
-    if not os.path.isdir(os.path.join(ref_root, "ops", "c", "src")):
+def build_reference(ref_root=None):
+    """Build the reference OpenMP apps into oracle/_ref (needs the reference
+    tree: `ref_root`, else the OPS_REFERENCE_ROOT environment variable)."""
+    ref_root = ref_root or os.environ.get("OPS_REFERENCE_ROOT")
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "ops", "c", "src")):
         return False
     subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), ref_root], check=True,
                    stdout=subprocess.DEVNULL)

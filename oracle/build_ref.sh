@@ -13,9 +13,9 @@
 #      `<app>_openmp` target does (makefiles/Makefile.c_app:218-224), plus the
 #      oracle hook object (full-precision printing, optional field dumps).
 #
-# usage: oracle/build_ref.sh [reference_root]     (default /root/reference)
+# usage: oracle/build_ref.sh [reference_root]   (default: $OPS_REFERENCE_ROOT)
 set -euo pipefail
-REF=${1:-${OPS_REFERENCE_ROOT:-/root/reference}}
+REF=${1:-${OPS_REFERENCE_ROOT:-}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 # /usr/bin/g++ carries the OpenMP spec file; another g++ earlier on PATH may not

@@ -290,3 +290,77 @@ def halo():
 
 if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "halo":
     halo()
+
+
+# ---------------------------------------------------------------------------
+# Full-size configurations: the headline decks at their stated sizes. The
+# fixtures hold every per-step scalar the reference prints (dt, field
+# summaries, max|delta|, iteration counts) and a SHA-256 digest of each final
+# field (the reference's host layout without its x padding, which is also the
+# layout of ops_b200's dumps), so a GPU test checks the full-size fields bit
+# for bit without carrying gigabytes of fixtures.
+#
+#     python tests/golden/make_golden.py fullsize
+# ---------------------------------------------------------------------------
+FULL_CLOVER = ("fullsize_clover_3840_s200", 3840, 200, 2)
+FULL_TEA = ("fullsize_tea_4096_pcg", 4096, 4)
+FULL_LAPLACE = ("fullsize_laplace_4096_it1000", 4096, 1000, 1)
+
+
+def sha256(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def fullsize_clover(threads):
+    from ops_b200 import apps, seeded
+    name, n, steps, seed = FULL_CLOVER
+    deck = apps.clover_deck(x_cells=n, y_cells=n, xmin=0.0, ymin=0.0, xmax=10.0, ymax=10.0, initial_timestep=0.04,
+                            timestep_rise=1.5, max_timestep=0.04, end_step=steps, summary_frequency=1,
+                            states=seeded.clover_config2_states(n, n, seed))
+    text = apps.clover_deck_text(deck)
+    summ, dts, dumps = run_reference_clover(text, dump=True, threads=threads, timeout=7200)
+    digests = {k: sha256(v) for k, v in dumps.items()}
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, deck=text, summaries=summ, dts=dts, field_names=np.array(sorted(digests)),
+                        field_sha256=np.array([digests[k] for k in sorted(digests)]),
+                        field_shapes=np.array([dumps[k].shape for k in sorted(digests)]))
+    print("wrote", path, summ.shape, len(dts))
+
+
+def fullsize_tea(threads):
+    from ops_b200 import apps
+    name, n, seed = FULL_TEA
+    kw = dict(x_cells=n, y_cells=n, xmin=0.0, ymin=0.0, xmax=10.0, ymax=10.0, initial_timestep=0.004, end_step=1,
+              summary_frequency=1, max_iters=200000, eps=1e-10, solver=1, preconditioner=1,
+              states=("seeded", n, n, seed))
+    kw["states"] = tea_states(kw["states"])
+    text = apps.tea_deck_text(apps.tea_deck(**kw))
+    summ, iters, errs, _, _ = run_reference_tea(text, dump=False, threads=threads, timeout=7200)
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, deck=text, summaries=summ, iters=iters, errors=errs)
+    print("wrote", path, summ, iters, errs)
+
+
+def fullsize_laplace(threads):
+    exe = oracle.reference_binary("laplace2d_seeded")
+    if exe is None:
+        raise SystemExit("oracle/_ref/bin/laplace2d_seeded missing: run oracle/build_ref.sh")
+    name, n, iters, seed = FULL_LAPLACE
+    with tempfile.TemporaryDirectory() as td:
+        dump = os.path.join(td, "A.bin")
+        r = subprocess.run([exe, str(n), str(n), str(iters), str(seed), dump], cwd=td, capture_output=True,
+                           text=True, check=True, timeout=7200, env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        errs = [float(l.split()[3]) for l in r.stdout.splitlines() if l.startswith("iter ")]
+        field = np.fromfile(dump, dtype=np.float64).reshape(n + 2, n + 2)
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, errors=np.array(errs), field_sha256=sha256(field), field_sum=float(field.sum()),
+                        imax=n, jmax=n, iters=iters, seed=seed)
+    print("wrote", path, len(errs))
+
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "fullsize":
+    nthreads = os.cpu_count() or 1
+    which = sys.argv[2:] or ["laplace", "clover", "tea"]
+    for w in which:
+        {"laplace": fullsize_laplace, "clover": fullsize_clover, "tea": fullsize_tea}[w](nthreads)

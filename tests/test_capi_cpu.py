@@ -4,6 +4,8 @@ import glob
 import os
 import re
 
+import pytest
+
 import ops_b200.build as build
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -68,6 +70,15 @@ def test_single_process_api_calls_without_gpu(capsys):
     p.set_cuda_opts(1, 2, 3)
     p.set_cuda_sync(0)
     assert (p.strategy, p.jacobi, p.batch_size, p.cuda_opts, p.cuda_sync) == (3, (1e-10, 1e-12, 5), 64, (1, 2, 3), 0)
+    # the C-ABI struct holds the same values
+    c = p._p
+    assert (c.strategy, c.jacobi_rtol, c.jacobi_atol, c.jacobi_maxiter, c.batch_size, list(c.cuda_opts),
+            c.cuda_sync) == (3, 1e-10, 1e-12, 5, 64, [1, 2, 3], 0)
+    assert O.ops_tridsolver_params(None)._p.strategy == O.ops_tridsolver_params.GATHER_SCATTER
+    with pytest.raises(O.OpsError):
+        O.ops_tridsolver_params(None, 9)
+    with pytest.raises(O.OpsError):
+        p.set_batch_size(-1)
 
 
 def test_heat_solve_arguments_are_checked_before_any_device_work():

@@ -29,7 +29,12 @@ def _bind():
     return f, L
 
 
-@pytest.mark.parametrize("imax,jmax,seed", [(300, 211, 3), (4096, 64, 4), (1, 1, 5)])
+# (300, 5000): the grid's y extent is clamped (790 blocks of 2 rows), so the
+# kernel's y loop makes several passes; (65536, 40): the widest allowed
+# rows, 512 blocks across, where the block budget of the shared scratch
+# bounds the grid's y extent.
+@pytest.mark.parametrize("imax,jmax,seed", [(300, 211, 3), (4096, 64, 4), (1, 1, 5), (300, 5000, 6),
+                                            (65536, 40, 7)])
 def test_noalloc_sweep_matches_allocating_entry_point(imax, jmax, seed):
     import torch
     sweep, L = _bind()
