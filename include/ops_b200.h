@@ -157,7 +157,10 @@ int ops_b200_dat_get_raw_pointer(int dat, int memspace, void **ptr, int *stride)
 int ops_b200_dat_release_raw_data(int dat, int acc);
 
 /* Runtime options: "graphs" (CUDA-graph replay of repeated flushes, default
- * 1) and "fusion" (copy elision and chain kernels, default 1). */
+ * 1), "fusion" (copy elision and chain kernels, default 1) and "tiling"
+ * (loop-chain fusion: runs of queued 2D loops executed as one kernel over
+ * shared-memory tiles, default 1, needs "fusion"; the counterpart of the
+ * reference's lazy tiling, ops/c/src/core/ops_lazy.cpp:380-1173). */
 int ops_b200_set_option(const char *name, int value);
 /* Counters since the last reset: kernels launched by this library, CUDA
  * graphs launched, loops queued. */
@@ -167,6 +170,11 @@ int ops_b200_counters(long long *kernels, long long *graphs, long long *loops);
  * counterpart; disabled with the "fusion" option). */
 int ops_b200_loops_skipped(long long *skipped);
 int ops_b200_reset_counters(void);
+/* Loop-chain fusion since the last counter reset: fused kernels launched,
+ * loops they replaced, and the compulsory HBM bytes of the fused kernels
+ * (each dat's points read and written once per chain) against those of the
+ * replaced loops run one by one. No reference counterpart. */
+int ops_b200_fusion_stats(long long *chains, long long *loops, double *fused_bytes, double *loop_bytes);
 /* Dat storage that the app drivers give back when they return is kept for
  * the next dats of the same size (no cudaFree/cudaMalloc of gigabytes per
  * call). This frees the kept blocks now (they are also freed and the

@@ -167,6 +167,7 @@ def _declare(L):
         "ops_b200_counters": ([P, P, P], i),
         "ops_b200_reset_counters": ([], i),
         "ops_b200_release_spare_storage": ([P], i),
+        "ops_b200_fusion_stats": ([P, P, P, P], i),
         "ops_b200_tridsolver_params_init": ([P, i, i], i),
         "ops_b200_tridsolver_params_set_jacobi_params": ([P, d, d, i], i),
         "ops_b200_tridsolver_params_set_batch_size": ([P, i], i),

@@ -239,6 +239,7 @@ int ops_b200_set_option(const char *name, int value) {
     std::string n = name ? name : "";
     if (n == "graphs") rt().set_graphs(value);
     else if (n == "fusion") rt().set_fusion(value);
+    else if (n == "tiling") rt().set_tiling(value);
     else throw opsb::Error(opsb::E_ARG, "unknown option " + n);
     return 0;
   });
@@ -250,6 +251,17 @@ int ops_b200_counters(long long *kernels, long long *graphs, long long *loops) {
     if (kernels) *kernels = r.kernels_launched();
     if (graphs) *graphs = r.graphs_launched();
     if (loops) *loops = r.loops_enqueued();
+    return 0;
+  });
+}
+
+int ops_b200_fusion_stats(long long *chains, long long *loops, double *fused_bytes, double *loop_bytes) {
+  return guarded([&] {
+    const opsb::Runtime::FusionStats &s = rt().fusion_stats();
+    if (chains) *chains = s.chains;
+    if (loops) *loops = s.loops;
+    if (fused_bytes) *fused_bytes = s.bytes;
+    if (loop_bytes) *loop_bytes = s.loop_bytes;
     return 0;
   });
 }
@@ -314,6 +326,7 @@ int ops_b200_tridsolver_params_set_cuda_sync(ops_b200_tridsolver_params *p, int 
 int ops_b200_reset_counters(void) {
   return guarded([&] {
     rt().reset_counters();
+    rt().reset_fusion_stats();
     return 0;
   });
 }

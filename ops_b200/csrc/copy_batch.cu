@@ -161,11 +161,6 @@ CopyStrip *device_strips(const std::vector<CopyStrip> &b, bool may_upload) {
   return d;
 }
 
-bool capturing(cudaStream_t s) {
-  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-  OPSB_CUDA(cudaStreamIsCapturing(s, &st));
-  return st != cudaStreamCaptureStatusNone;
-}
 
 int match_copy_run(const std::vector<Desc> &q, size_t i) {
   size_t j = i;
@@ -174,28 +169,35 @@ int match_copy_run(const std::vector<Desc> &q, size_t i) {
   if (n < 2) return 0;
   Planned pl;
   if (!plan(q, i, n, pl)) return 0;
-  // While a graph is being captured nothing may be uploaded; the strips of
-  // this structure were uploaded when it ran uncaptured the first time.
-  if (capturing(Runtime::get().stream()))
-    for (const auto &b : pl.batches)
-      if (!device_strips(b, false)) return 0;
   return n;
 }
 
-void launch_copy_run(const std::vector<Desc> &q, size_t i, int n, cudaStream_t s) {
+// Planned before any capture: the strips are uploaded now (once per
+// distinct strip list) and the launches keep their device addresses.
+PlanItem prepare_copy_run(const std::vector<Desc> &q, size_t i, int n) {
   Planned pl;
   if (!plan(q, i, n, pl)) throw Error(E_STATE, "copy batch: plan failed after a match");
-  const bool cap = capturing(s);
+  struct Launch { CopyStrip *d; int n; long long total; int blocks; };
+  std::vector<Launch> ls;
   for (const auto &b : pl.batches) {
     if (b.empty()) continue;
-    CopyStrip *d = device_strips(b, !cap);
-    if (!d) throw Error(E_STATE, "copy batch: strips missing during capture");
+    CopyStrip *d = device_strips(b, true);
     long long total = b.back().first + (long long)b.back().nx * b.back().ny * b.back().nz;
     int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
-    copy_batch_kernel<<<blocks, 256, 0, s>>>(d, (int)b.size(), total);
-    OPSB_CUDA(cudaGetLastError());
-    Runtime::get().count_kernels(1);
+    ls.push_back({d, (int)b.size(), total, blocks});
   }
+  PlanItem it;
+  it.name = "runtime/copy_batch";
+  it.kernels = (long long)ls.size();
+  it.bytes = 16.0 * (double)pl.cells;
+  if (!ls.empty())
+    it.run = [ls](cudaStream_t s) {
+      for (const Launch &l : ls) {
+        copy_batch_kernel<<<l.blocks, 256, 0, s>>>(l.d, l.n, l.total);
+        OPSB_CUDA(cudaGetLastError());
+      }
+    };
+  return it;
 }
 
 struct CopyChainReg {
@@ -203,7 +205,7 @@ struct CopyChainReg {
     ChainRule r;
     r.name = "runtime/copy_batch";
     r.match = match_copy_run;
-    r.launch = launch_copy_run;
+    r.prepare = prepare_copy_run;
     Runtime::register_chain(r);
   }
 };

@@ -75,7 +75,7 @@ bool zero_point_stencil(const Stencil &s) {
 }
 }  // namespace
 
-void Runtime::launch_swap_outside(const Desc &d, cudaStream_t s) {
+PlanItem Runtime::prepare_swap_outside(const Desc &d) {
   const Dat &A = *dats_[d.args[0].dat];
   const Dat &B = *dats_[d.args[1].dat];
   SwapParams p;
@@ -124,12 +124,17 @@ void Runtime::launch_swap_outside(const Desc &d, cudaStream_t s) {
     for (int k = 0; k < 3; k++) n *= (p.box[i].hi[k] - p.box[i].lo[k]);
     p.prefix[i + 1] = p.prefix[i] + n;
   }
-  if (nb == 0) return;
+  PlanItem it;
+  it.name = d.loop->kernel;
+  if (nb == 0) return it;
   long long total = p.prefix[nb];
   int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 8);
-  swap_outside_kernel<<<blocks, 256, 0, s>>>(p);
-  OPSB_CUDA(cudaGetLastError());
-  kernels_launched_++;
+  it.kernels = 1;
+  it.run = [p, blocks](cudaStream_t s) {
+    swap_outside_kernel<<<blocks, 256, 0, s>>>(p);
+    OPSB_CUDA(cudaGetLastError());
+  };
+  return it;
 }
 
 void Runtime::elide_copies(std::vector<Desc> &q) {

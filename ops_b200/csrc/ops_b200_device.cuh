@@ -61,16 +61,26 @@ __device__ __forceinline__ double qratio(double a, double b) {
 // As in the reference's ACC<T> (ops/c/include/ops_lib_core.h:1525-1556) an
 // offset is i + j * (row pitch) whatever the stencil's stride: a dat that is
 // one point wide along a dimension is only ever offset along the other.
+// `coherent` selects how a read-only view loads: 0 through the non-coherent
+// read-only path (data no thread writes during the kernel: every argument of
+// a single loop kernel, where the flag is the constant 0 and the test folds
+// away), 1 with ordinary loads through a generic address (fused chain
+// kernels, whose views may point into shared-memory tiles or at data other
+// phases of the same kernel write).
 template <class T>
 struct ACC2 {
   using value_type = T;
   T *p;
   int sy;
+  int coherent;
   ACC2() = default;
-  __device__ __forceinline__ ACC2(T *p_, int sy_) : p(p_), sy(sy_) {}
+  __device__ __forceinline__ ACC2(T *p_, int sy_) : p(p_), sy(sy_), coherent(0) {}
+  __device__ __forceinline__ ACC2(T *p_, int sy_, int coh) : p(p_), sy(sy_), coherent(coh) {}
   __device__ __forceinline__ T &operator()(int i, int j) { return p[i + j * sy]; }
-  // Read-only view (the kernel's const ACC<T>& arguments): non-coherent loads.
-  __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (i + j * sy)); }
+  // Read-only view (the kernel's const ACC<T>& arguments).
+  __device__ __forceinline__ T operator()(int i, int j) const {
+    return coherent ? p[i + j * sy] : __ldg(p + (i + j * sy));
+  }
 };
 
 // 3D accessor.

@@ -84,6 +84,9 @@ Runtime::~Runtime() {
   for (auto e : event_pool_) cudaEventDestroy(e);
   for (auto &kv : graphs_)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  release_fusion_state();
+  for (auto &kv : shadow_)
+    if (kv.second) cudaFree(kv.second);
   for (auto &d : dats_)
     if (d && d->data_d) cudaFree(d->data_d);
   for (auto &kv : spare_) cudaFree(kv.second);
@@ -120,6 +123,8 @@ void Runtime::init(int device, int diags) {
   if (g) graphs_on_ = atoi(g);
   const char *f = getenv("OPS_B200_FUSION");
   if (f) fusion_on_ = atoi(f);
+  const char *t = getenv("OPS_B200_TILING");
+  if (t) tiling_on_ = atoi(t);
   inited_ = true;
 }
 
@@ -550,6 +555,11 @@ uint64_t Runtime::queue_key(const std::vector<Desc> &q) const {
       if (a.kind == ARG_REDUCE) h = mix64(h, ((uint64_t)a.red << 1) | (uint64_t)d.red_first[i]);
       if (a.kind == ARG_GBL) h = mix64(h, (uint64_t)d.gbl_off[i] ^ ((uint64_t)a.gbl.size() << 40));
     }
+    // A fused chain resolves a boundary copy loop's field flags when it is
+    // planned: the flag values are part of the structure.
+    if (const CopyLoopSpec *sp = find_copy_loop(d.loop))
+      if (sp->flags_arg >= 0 && sp->flags_arg < (int)d.args.size())
+        for (char c : d.args[sp->flags_arg].gbl) h = mix64(h, (uint64_t)(unsigned char)c);
   }
   return h;
 }
@@ -622,31 +632,66 @@ void Runtime::collect_timing() {
   pending_.clear();
 }
 
-void Runtime::launch_items(std::vector<Desc> &q) {
+// Every item of a flush, in queue order, with its launch resolved now: fused
+// chains (fusion.cpp), then runtime-internal items, chain rules (batched
+// boundary copies) and single loops. Storage moves made by a fused chain
+// are visible to the items planned after it only.
+void Runtime::plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::vector<int> &renamed,
+                         bool &tuning) {
+  out.clear();
+  renamed.clear();
+  tuning = false;
+  std::vector<FusedItem> fused;
+  plan_fusion(q, fused);
   auto &chains = registry().chains;
+  size_t fi = 0;
   size_t i = 0;
   while (i < q.size()) {
+    if (fi < fused.size() && fused[fi].first == i) {
+      FusedItem &f = fused[fi++];
+      build_fused(q, f);
+      renamed.insert(renamed.end(), f.renamed.begin(), f.renamed.end());
+      tuning = tuning || f.tuning;
+      PlanItem it;
+      it.name = f.name;
+      it.bytes = f.bytes;
+      it.kernels = 1;
+      it.fused_loops = (long long)f.n;
+      it.loop_bytes = f.loop_bytes;
+      auto launch = f.launch;
+      const fuse::FPlan *dplan = f.dplan;
+      const int grid = f.grid;
+      const size_t smem = (size_t)f.smem;
+      cudaEvent_t e0 = f.ev0, e1 = f.ev1;
+      it.run = [launch, dplan, grid, smem, e0, e1](cudaStream_t s) {
+        if (e0) OPSB_CUDA(cudaEventRecord(e0, s));
+        launch(dplan, grid, smem, s);
+        OPSB_CUDA(cudaGetLastError());
+        if (e1) OPSB_CUDA(cudaEventRecord(e1, s));
+      };
+      out.push_back(std::move(it));
+      i += f.n;
+      continue;
+    }
+    const size_t limit = fi < fused.size() ? fused[fi].first : q.size();
     if (q[i].loop->internal) {
-      timed_launch_begin(q[i].loop->kernel);
-      launch_swap_outside(q[i], stream_);
-      timed_launch_end();
+      out.push_back(prepare_swap_outside(q[i]));
       i++;
       continue;
     }
     if (fusion_on_) {
-      bool fused = false;
+      bool done = false;
       for (auto &rule : chains) {
         int n = rule.match(q, i);
+        n = (int)std::min<size_t>((size_t)std::max(n, 0), limit - i);
         if (n > 0) {
-          timed_launch_begin(rule.name);
-          rule.launch(q, i, n, stream_);
-          timed_launch_end();
+          out.push_back(rule.prepare(q, i, n));
           i += n;
-          fused = true;
+          done = true;
           break;
         }
       }
-      if (fused) continue;
+      if (done) continue;
     }
     const Desc &d = q[i];
     LoopParams lp;
@@ -657,15 +702,52 @@ void Runtime::launch_items(std::vector<Desc> &q) {
     launch_shape(d.range, d.dim, nred > 0, g, b);
     long long nx = (long long)d.range[1] - d.range[0];
     long long nr = (long long)(d.range[3] - d.range[2]) * (d.range[5] - d.range[4]);
+    PlanItem it;
+    it.name = d.loop->kernel;
     if ((nx > 0 && nr > 0) || nred > 0) {
-      timed_launch_begin(d.loop->kernel, timing_on_ ? alg_bytes(d) : 0.0);
-      d.loop->launch(lp, g, b, stream_);
-      OPSB_CUDA(cudaGetLastError());
-      timed_launch_end();
-      kernels_launched_++;
+      it.bytes = timing_on_ ? alg_bytes(d) : 0.0;
+      it.kernels = 1;
+      auto launch = d.loop->launch;
+      it.run = [lp, g, b, launch](cudaStream_t s) {
+        launch(lp, g, b, s);
+        OPSB_CUDA(cudaGetLastError());
+      };
     }
+    out.push_back(std::move(it));
     i++;
   }
+}
+
+void Runtime::launch_plan(std::vector<PlanItem> &items) {
+  for (PlanItem &it : items) {
+    if (!it.run) continue;
+    timed_launch_begin(it.name, it.bytes);
+    it.run(stream_);
+    timed_launch_end();
+    kernels_launched_ += it.kernels;
+    if (it.fused_loops > 0) {
+      fstats_.chains++;
+      fstats_.loops += it.fused_loops;
+      fstats_.bytes += it.bytes;
+      fstats_.loop_bytes += it.loop_bytes;
+    }
+  }
+}
+
+// A captured flush replayed: the dats its fused chains renamed move again.
+void Runtime::apply_renames(const std::vector<int> &renamed) {
+  for (int di : renamed) {
+    Dat &d = *dats_[di];
+    std::swap(d.data_d, shadow_.at(di));
+    d.host.clear();
+  }
+}
+
+void Runtime::add_fusion_stats(const FusionStats &s) {
+  fstats_.chains += s.chains;
+  fstats_.loops += s.loops;
+  fstats_.bytes += s.bytes;
+  fstats_.loop_bytes += s.loop_bytes;
 }
 
 void Runtime::run_queue(std::vector<Desc> &q) {
@@ -701,42 +783,59 @@ void Runtime::run_queue(std::vector<Desc> &q) {
   if (gbl_used_ > 0)
     OPSB_CUDA(cudaMemcpyAsync(gbl_dev_, gbl_host_.data(), gbl_used_, cudaMemcpyHostToDevice, stream_));
 
-  if (!graphs_on_ || timing_on_ || q.size() < 2) {
-    launch_items(q);
+  const bool use_graphs = graphs_on_ && !timing_on_ && q.size() >= 2;
+  GraphEntry *ge = nullptr;
+  if (use_graphs) {
+    ge = &graphs_[queue_key(q)];
+    if (ge->exec) {
+      OPSB_CUDA(cudaGraphLaunch(ge->exec, stream_));
+      graphs_launched_++;
+      kernels_launched_ += ge->kernels;
+      apply_renames(ge->renamed);
+      add_fusion_stats(ge->fstats);
+      return;
+    }
+  }
+  std::vector<PlanItem> items;
+  std::vector<int> renamed;
+  bool tuning = false;
+  plan_items(q, items, renamed, tuning);
+  if (!use_graphs || tuning) {
+    launch_plan(items);
     return;
   }
-  uint64_t key = queue_key(q);
-  GraphEntry &ge = graphs_[key];
-  ge.seen++;
-  if (ge.exec) {
-    OPSB_CUDA(cudaGraphLaunch(ge.exec, stream_));
-    graphs_launched_++;
-    kernels_launched_ += ge.kernels;
-    return;
-  }
-  if (ge.seen < 2) {
-    launch_items(q);
+  ge->seen++;
+  if (ge->seen < 2) {
+    launch_plan(items);
     return;
   }
   // Second sighting of this queue structure: capture it once, replay from now on.
   cudaGraph_t graph = nullptr;
-  long long before = kernels_launched_;
+  const long long before = kernels_launched_;
+  const FusionStats fs0 = fstats_;
   OPSB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
   try {
-    launch_items(q);
+    launch_plan(items);
   } catch (...) {
     cudaStreamEndCapture(stream_, &graph);
     if (graph) cudaGraphDestroy(graph);
     throw;
   }
   OPSB_CUDA(cudaStreamEndCapture(stream_, &graph));
-  ge.kernels = kernels_launched_ - before;
+  ge->kernels = kernels_launched_ - before;
   kernels_launched_ = before;
-  OPSB_CUDA(cudaGraphInstantiate(&ge.exec, graph, 0));
+  ge->renamed = renamed;
+  ge->fstats.chains = fstats_.chains - fs0.chains;
+  ge->fstats.loops = fstats_.loops - fs0.loops;
+  ge->fstats.bytes = fstats_.bytes - fs0.bytes;
+  ge->fstats.loop_bytes = fstats_.loop_bytes - fs0.loop_bytes;
+  fstats_ = fs0;
+  OPSB_CUDA(cudaGraphInstantiate(&ge->exec, graph, 0));
   cudaGraphDestroy(graph);
-  OPSB_CUDA(cudaGraphLaunch(ge.exec, stream_));
+  OPSB_CUDA(cudaGraphLaunch(ge->exec, stream_));
   graphs_launched_++;
-  kernels_launched_ += ge.kernels;
+  kernels_launched_ += ge->kernels;
+  add_fusion_stats(ge->fstats);
 }
 
 void Runtime::execute() {
@@ -838,9 +937,16 @@ void Runtime::release_to(const Mark &m) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   graphs_.clear();
   while (dats_.size() > m.dats) {
+    const int di = (int)dats_.size() - 1;
     if (dats_.back() && dats_.back()->data_d) recycle_dat_storage(dats_.back()->data_d, dats_.back()->bytes);
+    auto sh = shadow_.find(di);
+    if (sh != shadow_.end()) {
+      if (sh->second) recycle_dat_storage(sh->second, dats_.back()->bytes);
+      shadow_.erase(sh);
+    }
     dats_.pop_back();
   }
+  release_fusion_state();
   while (reductions_.size() > m.reductions) {
     reductions_.pop_back();
   }

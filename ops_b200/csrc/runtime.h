@@ -30,6 +30,11 @@
 #include "ops_b200_device.cuh"
 
 namespace opsb {
+namespace fuse {
+struct FPlan;
+}
+class FusionPlanner;
+struct FusionState;
 
 // Error codes of the C-ABI (include/ops_b200.h).
 enum ErrCode { E_OK = 0, E_ARG = -1, E_CUDA = -2, E_STATE = -3, E_NOTFOUND = -4, E_TIMEOUT = -5, E_UNSUPPORTED = -6 };
@@ -113,13 +118,43 @@ struct Desc {
   uint64_t hash = 0;
 };
 
-// A fused replacement for a run of queued loops. `match` inspects the queue
-// from position i and returns how many descriptors it covers (0 = no match);
-// `launch` enqueues the replacement work on the stream.
+// A launch prepared when a flush is planned: the device work of one queued
+// loop, or of a run of loops that a chain rule or the fuser replaces, with
+// every storage address it uses resolved at planning time (a fused chain can
+// move a dat's storage; the loops after it see the new storage, the loops
+// before it the old). Planning happens before any graph capture, so `run`
+// only launches.
+struct PlanItem {
+  std::string name;           // timing name (loop kernel, rule or fused group)
+  double bytes = 0.0;         // compulsory bytes (per-kernel timing)
+  long long kernels = 0;      // kernels `run` launches
+  long long fused_loops = 0;  // fused chain: loops it covers
+  double loop_bytes = 0.0;    // fused chain: the covered loops' own compulsory bytes
+  std::function<void(cudaStream_t)> run;
+};
+
+// A replacement for a run of queued loops. `match` inspects the queue from
+// position i and returns how many descriptors it covers (0 = no match);
+// `prepare` resolves the replacement's launches at planning time.
 struct ChainRule {
   std::string name;
   std::function<int(const std::vector<Desc> &, size_t)> match;
-  std::function<void(const std::vector<Desc> &, size_t, int, cudaStream_t)> launch;
+  std::function<PlanItem(const std::vector<Desc> &, size_t, int)> prepare;
+};
+
+// A run of queued loops that the fuser (fusion.cpp) executes as one kernel.
+struct FusedItem {
+  size_t first = 0, n = 0;
+  std::string name;
+  double bytes = 0.0, loop_bytes = 0.0;  // compulsory bytes fused / as separate loops
+  bool tuning = false;                   // this execution times a candidate tile shape
+  uint64_t key = 0;
+  int shape = 0, grid = 0, smem = 0;
+  std::vector<int> renamed;              // dats moved to their shadow storage by this chain
+  void (*launch)(const fuse::FPlan *, int, size_t, cudaStream_t) = nullptr;
+  fuse::FPlan *dplan = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::shared_ptr<void> analysis;        // the planner's analysis until the plan is built
 };
 
 struct LoopStats {
@@ -216,6 +251,7 @@ class Runtime {
   double alg_bytes(const Desc &d) const;
   void timed_launch_end();
   void set_fusion(int on) { fusion_on_ = on; }
+  void set_tiling(int on) { tiling_on_ = on; }
   long long loops_skipped() const { return loops_skipped_; }
   int fusion_enabled() const { return fusion_on_; }
   int diags() const { return diags_; }
@@ -241,12 +277,27 @@ class Runtime {
 
   ~Runtime();
 
+  // Loop-chain fusion statistics since the last reset: fused kernels
+  // launched, loops they covered, and their compulsory bytes fused and as
+  // separate loops.
+  struct FusionStats { long long chains = 0, loops = 0; double bytes = 0.0, loop_bytes = 0.0; };
+  const FusionStats &fusion_stats() const { return fstats_; }
+  void reset_fusion_stats() { fstats_ = FusionStats(); }
+
  private:
+  friend class FusionPlanner;
   Runtime() = default;
   void run_queue(std::vector<Desc> &q);
   void elide_copies(std::vector<Desc> &q);
-  void launch_swap_outside(const Desc &d, cudaStream_t s);
-  void launch_items(std::vector<Desc> &q);
+  PlanItem prepare_swap_outside(const Desc &d);
+  void plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::vector<int> &renamed, bool &tuning);
+  void launch_plan(std::vector<PlanItem> &items);
+  void plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &items);
+  void build_fused(const std::vector<Desc> &q, FusedItem &item);
+  FusionState &fusion_state();
+  void release_fusion_state();
+  void apply_renames(const std::vector<int> &renamed);
+  void add_fusion_stats(const FusionStats &s);
   uint64_t queue_key(const std::vector<Desc> &q) const;
 
   bool inited_ = false;
@@ -293,7 +344,14 @@ class Runtime {
     int seen = 0;
     cudaGraphExec_t exec = nullptr;
     long long kernels = 0;
+    std::vector<int> renamed;  // storage moves the captured flush makes (replayed on the host)
+    FusionStats fstats;        // fusion statistics of one replay
   };
+  // Fused chains write renamed dats into a shadow allocation of the same
+  // size, which then becomes the dat's storage (the old one the shadow).
+  std::unordered_map<int, char *> shadow_;
+  FusionState *fusion_state_ = nullptr;  // owned; created and freed in fusion.cpp
+  FusionStats fstats_;
   std::unordered_map<uint64_t, GraphEntry> graphs_;
   int graphs_on_ = 1;
   int timing_on_ = 0;
@@ -305,6 +363,7 @@ class Runtime {
   double cur_bytes_ = 0.0;
   cudaEvent_t cur_ev_ = nullptr;
   int fusion_on_ = 1;
+  int tiling_on_ = 0;  // loop-chain fusion into tiled kernels (needs fusion_on_)
   // Redundant-loop elimination within one flush: per queued loop, the
   // version of each dat arg (read: as observed, written: as produced);
   // dat versions count the writes of the queued loops and restart at every

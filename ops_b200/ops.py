@@ -268,6 +268,14 @@ def counters():
     return {"kernels": k.value, "graphs": g.value, "loops": l.value}
 
 
+def fusion_stats():
+    """Loop-chain fusion since the last counter reset: fused kernels launched,
+    loops they replaced, and the compulsory bytes fused vs as separate loops."""
+    c, n, fb, lb = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+    check(lib().ops_b200_fusion_stats(ctypes.byref(c), ctypes.byref(n), ctypes.byref(fb), ctypes.byref(lb)))
+    return {"chains": c.value, "loops": n.value, "fused_bytes": fb.value, "loop_bytes": lb.value}
+
+
 def set_kernel_timing(on):
     check(lib().ops_b200_set_kernel_timing(int(on)))
 
@@ -460,6 +468,7 @@ class ops_tridsolver_params:
 
 
 __all__ = [n for n in dir() if n.startswith("ops_")] + ["OpsError", "set_option", "counters", "reset_counters",
+                                                          "fusion_stats",
                                                           "set_kernel_timing", "kernel_time", "clear_kernel_timing",
                                                           "trid_batch", "OPS_READ", "OPS_WRITE", "OPS_RW", "OPS_INC",
                                                           "OPS_MIN", "OPS_MAX", "OPS_HOST", "OPS_DEVICE"]
