@@ -22,7 +22,13 @@ namespace fuse {
 struct TileCtx {
   const FPlan *P;
   double *sm;
-  double *scratch;   // write sink for masked points (shared, 32 doubles, centre at +16)
+  // Write sink for masked points: this thread's own kScratch doubles, one
+  // cell per argument (at +16 + its index in the loop, so that stencil
+  // offsets of up to 16 stay inside). Per thread and per argument, because
+  // kernels read back what they wrote through arguments declared
+  // write-only (CloverLeaf's accelerate_kernel reads stepbymass after
+  // setting it; advec_cell_kernel4 reads pre_mass, post_mass and advec_vol).
+  double *scratch;
   double *racc;      // per-thread reduction accumulators
   int cx0, cy0, cx1, cy1;
 };
@@ -38,7 +44,7 @@ struct FSlot<ACC2<T>> {
       T *p = reinterpret_cast<T *>(c.sm + b.off + (x - (c.cx0 - b.hx0)) + (y - (c.cy0 - b.hy0)) * b.pitch);
       acc = ACC2<T>(p, b.pitch, 1);
     } else if (a.mode == M_RW && a.masked && !core) {
-      acc = ACC2<T>(reinterpret_cast<T *>(c.scratch + 16), 0, 1);
+      acc = ACC2<T>(reinterpret_cast<T *>(c.scratch + 16 + a.slot), 0, 1);
     } else {
       acc = ACC2<T>(reinterpret_cast<T *>(a.ptr) + (x * a.sx + y * a.sy), a.ay, a.mode == M_RW ? 1 : 0);
     }
@@ -162,7 +168,7 @@ __device__ inline void copy_phase(const TileCtx &c, const FLoop &L, int rx0, int
 template <class G>
 __global__ void __launch_bounds__(kThreads, 2) fused_chain_kernel(const FPlan *__restrict__ P) {
   extern __shared__ double sm_all[];
-  __shared__ double scratch[32];
+  double scratch[kScratch];
   __shared__ double red_smem[32];
   __shared__ int last;
   double racc[kMaxRed];

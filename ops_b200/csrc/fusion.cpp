@@ -124,6 +124,11 @@ struct LoopInfoF {
   std::vector<int> cp_args;  // copy loop: argument indices whose flag is set
 };
 
+bool trace_on() {
+  static const bool t = getenv("OPS_B200_FUSION_TRACE") != nullptr;
+  return t;
+}
+
 // Rejections that a longer chain cannot undo: the greedy growth stops there.
 bool final_rejection(const std::string &why) {
   return why == "halo depth above the limit" || why == "too many loops" || why == "too many arguments" ||
@@ -475,14 +480,20 @@ class FusionPlanner {
           case ARG_DAT: {
             const Dat &dt = *rt.dats_[a.dat];
             const Stencil &st = rt.stencils_[a.stencil];
-            const FieldInfo &f = A.fields.at(a.dat);
             F.ptr = dt.origin_ptr();
             F.sx = st.stride[0] ? 1 : 0;
             F.sy = st.stride[1] ? (int)dt.pitch : 0;
             F.ay = (int)dt.pitch;
+            auto fit = A.fields.find(a.dat);
+            if (fit == A.fields.end()) {  // a copy loop's field whose flag is off: never accessed
+              F.mode = M_RO;
+              break;
+            }
+            const FieldInfo &f = fit->second;
             F.mode = f.mode;
             if (f.mode == M_TILE) F.buf = buf_of.at(a.dat);
             F.masked = f.mode == M_RW && (a.acc == ACC_WRITE || a.acc == ACC_RW);
+            F.slot = (int)i;
             break;
           }
           case ARG_GBL:
@@ -730,15 +741,24 @@ void Runtime::plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &it
         i++;
         continue;
       }
+      // the chain from i that saves the most HBM traffic
       size_t best = 0;
+      double best_saved = 0.0;
       ChainAnalysis A;
       for (size_t j = i + 1; j <= q.size(); j++) {
         int gj;
         if (!fp.eligible(q[j - 1], &gj)) break;
-        if (fp.analyse(q, i, j - i, A))
-          best = j - i;
-        else if (final_rejection(A.why))
-          break;
+        if (fp.analyse(q, i, j - i, A)) {
+          const double saved = A.loop_bytes - A.fused_bytes;
+          if (saved > best_saved) {
+            best = j - i;
+            best_saved = saved;
+          }
+        } else {
+          if (trace_on() && A.why != "fewer than two compute loops")
+            fprintf(stderr, "  chain [%zu, %zu) rejected: %s\n", i, j, A.why.c_str());
+          if (final_rejection(A.why)) break;
+        }
       }
       if (best > 0) {
         b.push_back({i, best});
@@ -750,7 +770,7 @@ void Runtime::plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &it
     bit = S.bounds.emplace(qk, std::move(b)).first;
   }
   const bool tuning_on = !(getenv("OPS_B200_TUNE") && atoi(getenv("OPS_B200_TUNE")) == 0);
-  static const bool trace = getenv("OPS_B200_FUSION_TRACE") != nullptr;
+  const bool trace = trace_on();
   for (const auto &fb : bit->second) {
     auto A = std::make_shared<ChainAnalysis>();
     if (!fp.analyse(q, fb.first, fb.second, *A)) continue;  // the structure was analysed before

@@ -42,6 +42,7 @@ constexpr int kMaxBufs = 24;     // shared-memory tiles
 constexpr int kMaxRed = 8;       // reduction arguments over a chain
 constexpr int kMaxBoxes = 96;    // write-back boxes over all tiles
 constexpr int kThreads = 256;
+constexpr int kScratch = 16 + 24 + 16;  // per-thread masked-write cells (see TileCtx::scratch)
 // Guard cells (zeros) around the shared-memory tiles, so that a kernel
 // reading outside its declared stencil reads a wrong value (which the parity
 // tests see) instead of leaving the shared-memory window.
@@ -57,7 +58,7 @@ struct FArg {
   int buf;     // TILE: shared-memory tile
   int red;     // RED: chain reduction slot
   int masked;  // RW written by this loop: points outside the core write a scratch cell
-  int pad;
+  int slot;    // that scratch cell: the argument's index in its loop (arguments must not alias)
 };
 
 struct FLoop {
