@@ -320,12 +320,17 @@ def bench_clover(args, world, rank, local, pg):
     cells = N * N
     K, W = args.steps, args.warmup
 
+    # Untimed: the fused chains' tile shapes are tuned on their first
+    # executions (both sweep orders) and kept in the tuning cache file, which
+    # the timed call reads.
+    apps.cloverleaf(clover_deck(24, N))
     barrier(pg, local)
     O.reset_counters()
     with ClockSampler(local) as cs:
         summ, secs = apps.cloverleaf(clover_deck(W + K, N), warmup_steps=W)
     clocks = cs.summary()
     c = O.counters()
+    fs = O.fusion_stats()
     barrier(pg, local)
     secs = max_over_ranks(pg, secs, local)
 
@@ -378,6 +383,11 @@ def bench_clover(args, world, rank, local, pg):
                         " 5-value field summary back"},
         "gpu_launches": int(round(launches_per_step * K)),
         "clocks": clocks,
+        "fusion": {"chains_per_step": fs["chains"] / (W + K), "loops_fused_per_step": fs["loops"] / (W + K),
+                   "chain_alg_bytes_per_cell": fs["fused_bytes"] / (W + K) / cells,
+                   "same_loops_unfused_bytes_per_cell": fs["loop_bytes"] / (W + K) / cells,
+                   "note": "loop chains of the lazy queue run as one tiled kernel each; chain bytes = each dat's"
+                           " points read once and written once per chain (the step's other loops run unfused)"},
         "final_summary": {"vol": summ[-1, 2], "mass": summ[-1, 3], "ie": summ[-1, 4], "ke": summ[-1, 5],
                           "press": summ[-1, 6]},
     }

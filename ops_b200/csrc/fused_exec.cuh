@@ -35,19 +35,35 @@ struct TileCtx {
 
 template <class P> struct FSlot;
 
+// An accessor argument: where its point (x, y) lives is resolved once per
+// phase (a shared-memory tile, or the dat in HBM), so that a point costs
+// one multiply-add per argument.
 template <class T>
 struct FSlot<ACC2<T>> {
   ACC2<T> acc;
-  __device__ __forceinline__ ACC2<T> &at(const TileCtx &c, const FArg &a, int x, int y, bool core) {
+  T *base;       // address of logical (0, 0) in the bound storage (may lie outside it)
+  int sx, sy, ay, coh, masked;
+  T *sink;
+  __device__ __forceinline__ void init(const TileCtx &c, const FArg &a) {
     if (a.mode == M_TILE) {
       const FBuf &b = c.P->B[a.buf];
-      T *p = reinterpret_cast<T *>(c.sm + b.off + (x - (c.cx0 - b.hx0)) + (y - (c.cy0 - b.hy0)) * b.pitch);
-      acc = ACC2<T>(p, b.pitch, 1);
-    } else if (a.mode == M_RW && a.masked && !core) {
-      acc = ACC2<T>(reinterpret_cast<T *>(c.scratch + 16 + a.slot), 0, 1);
+      const long long o = (long long)b.off - (c.cx0 - b.hx0) - (long long)(c.cy0 - b.hy0) * b.pitch;
+      base = reinterpret_cast<T *>(c.sm) + o;
+      sx = 1;
+      sy = ay = b.pitch;
+      coh = 1;
     } else {
-      acc = ACC2<T>(reinterpret_cast<T *>(a.ptr) + (x * a.sx + y * a.sy), a.ay, a.mode == M_RW ? 1 : 0);
+      base = reinterpret_cast<T *>(a.ptr);
+      sx = a.sx;
+      sy = a.sy;
+      ay = a.ay;
+      coh = a.mode == M_RW;
     }
+    masked = a.mode == M_RW && a.masked;
+    sink = reinterpret_cast<T *>(c.scratch + 16 + a.slot);
+  }
+  __device__ __forceinline__ ACC2<T> &at(const TileCtx &, const FArg &, int x, int y, bool core) {
+    acc = (masked && !core) ? ACC2<T>(sink, 0, 1) : ACC2<T>(base + (x * sx + y * sy), ay, coh);
     return acc;
   }
   __device__ __forceinline__ void done(const TileCtx &, const FArg &, bool) {}
@@ -57,6 +73,7 @@ template <class T, int N>
 struct FSlot<RED<T, N>> {
   static_assert(N == 1, "fused chains take one-component reductions");
   RED<T, N> r;
+  __device__ __forceinline__ void init(const TileCtx &, const FArg &) {}
   __device__ __forceinline__ RED<T, N> &at(const TileCtx &c, const FArg &a, int, int, bool core) {
     r.v[0] = core ? (T)c.racc[a.red] : red_identity<T>(c.P->red[a.red].acc);
     return r;
@@ -69,6 +86,7 @@ struct FSlot<RED<T, N>> {
 template <>
 struct FSlot<IDX> {
   IDX i;
+  __device__ __forceinline__ void init(const TileCtx &, const FArg &) {}
   __device__ __forceinline__ IDX &at(const TileCtx &, const FArg &, int x, int y, bool) {
     i.v[0] = x;
     i.v[1] = y;
@@ -80,6 +98,7 @@ struct FSlot<IDX> {
 
 template <class T>
 struct FSlot<T *> {
+  __device__ __forceinline__ void init(const TileCtx &, const FArg &) {}
   __device__ __forceinline__ T *at(const TileCtx &, const FArg &a, int, int, bool) {
     return reinterpret_cast<T *>(a.ptr);
   }
@@ -93,6 +112,10 @@ struct FusedCall<K, void (C::*)(P...) const> {
   using Tup = SlotTuple<Seq, FSlot<std::decay_t<P>>...>;
 
   template <size_t... I>
+  __device__ static __forceinline__ void init_all(Tup &t, const TileCtx &c, const FArg *a, std::index_sequence<I...>) {
+    (get_leaf<I, FSlot<std::decay_t<P>>>(t).init(c, a[I]), ...);
+  }
+  template <size_t... I>
   __device__ static __forceinline__ void point(const K &k, Tup &t, const TileCtx &c, const FArg *a, int x, int y,
                                                bool core, std::index_sequence<I...>) {
     k(get_leaf<I, FSlot<std::decay_t<P>>>(t).at(c, a[I], x, y, core)...);
@@ -105,6 +128,7 @@ struct FusedCall<K, void (C::*)(P...) const> {
     const K k{};
     Tup t;
     const FArg *a = c.P->A + L.arg0;
+    init_all(t, c, a, Seq{});
     const int w = rx1 - rx0;
     const int n = w * (ry1 - ry0);
     for (int p = threadIdx.x; p < n; p += kThreads) {
@@ -118,9 +142,10 @@ struct FusedCall<K, void (C::*)(P...) const> {
 };
 
 // A compile-time list of loop functors; dispatch by index.
-template <class... K>
+template <int MinBlocks, class... K>
 struct Group {
   static constexpr int size = sizeof...(K);
+  static constexpr int min_blocks = MinBlocks;
   template <int I, class First, class... Rest>
   __device__ static __forceinline__ void run_at(int kid, const TileCtx &c, const FLoop &L, int rx0, int rx1,
                                                 int ry0, int ry1) {
@@ -165,8 +190,10 @@ __device__ inline void copy_phase(const TileCtx &c, const FLoop &L, int rx0, int
   }
 }
 
+// G::min_blocks: CTAs per SM the register allocation must allow (the
+// group's functors decide how many registers that leaves).
 template <class G>
-__global__ void __launch_bounds__(kThreads, 2) fused_chain_kernel(const FPlan *__restrict__ P) {
+__global__ void __launch_bounds__(kThreads, G::min_blocks) fused_chain_kernel(const FPlan *__restrict__ P) {
   extern __shared__ double sm_all[];
   double scratch[kScratch];
   __shared__ double red_smem[32];
@@ -204,13 +231,20 @@ __global__ void __launch_bounds__(kThreads, 2) fused_chain_kernel(const FPlan *_
       const int n = w * (y1 - y0);
       const double *src = reinterpret_cast<const double *>(B.src);
       double *dst = sm + B.off;
+      // asynchronous copies (cp.async, 8 bytes each): every tile's loads are
+      // in flight at once instead of one dependent load per thread at a time
       for (int p = threadIdx.x; p < n; p += kThreads) {
         const int yy = p / w;
         const int x = x0 + (p - yy * w);
         const int y = y0 + yy;
-        dst[(x - (c.cx0 - B.hx0)) + (y - (c.cy0 - B.hy0)) * B.pitch] = src[x + (long long)y * B.ay];
+        const unsigned int s_addr = (unsigned int)__cvta_generic_to_shared(
+            dst + (x - (c.cx0 - B.hx0)) + (y - (c.cy0 - B.hy0)) * B.pitch);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s_addr), "l"(src + x + (long long)y * B.ay)
+                     : "memory");
       }
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     for (int l = 0; l < P->nloops; l++) {
       const FLoop &L = P->L[l];
@@ -302,17 +336,18 @@ int group_occupancy(int smem) {
   return n;
 }
 
-template <class... K>
+template <int MinBlocks, class... K>
 struct GroupRegistrar {
   GroupRegistrar(const char *name) {
     static const char *const names[] = {K::kname...};
+    using G = Group<MinBlocks, K...>;
     GroupInfo g;
     g.name = name;
     g.nkernels = sizeof...(K);
     g.kernels = names;
-    g.launch = &launch_group<Group<K...>>;
-    g.set_smem = &group_set_smem<Group<K...>>;
-    g.occupancy = &group_occupancy<Group<K...>>;
+    g.launch = &launch_group<G>;
+    g.set_smem = &group_set_smem<G>;
+    g.occupancy = &group_occupancy<G>;
     register_group(g);
   }
 };

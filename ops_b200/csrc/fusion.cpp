@@ -94,11 +94,19 @@ bool exists_point(const B2 &R, const std::vector<B2> &in, bool in_all, const std
   return false;
 }
 
-constexpr int kMaxDepth = 6;              // deepest halo a chain may need
+constexpr int kMaxDepth = 3;              // deepest halo a chain may need (recompute grows with it)
 constexpr int kSmemBudget = 220 * 1024;   // dynamic shared memory per CTA
 struct Shape { int tx, ty; };
-const Shape kShapes[] = {{64, 8}, {128, 8}, {64, 16}, {32, 16}, {128, 4}};
+const Shape kShapes[] = {{64, 8}, {128, 8}, {64, 16}, {128, 16}, {32, 16}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+// Tuning candidates: a tile shape, with the read-only dats read from HBM in
+// the loops (even index) or staged into shared memory with the rest at the
+// start of each tile (odd index); the last candidate runs the chain's loops
+// one by one, unfused.
+constexpr int kNumCands = 2 * kNumShapes;
+constexpr int kUnfused = kNumCands;
+inline const Shape &cand_shape(int c) { return kShapes[c / 2]; }
+inline bool cand_stage_ro(int c) { return (c & 1) != 0; }
 
 struct DatAccess {
   int loop, arg, dat;
@@ -110,6 +118,7 @@ struct FieldInfo {
   int dat = -1;
   int mode = M_RO;
   bool staged = false, renamed = false;
+  bool stageable = false;  // RO, a 2D double dat: may be staged into a read-only tile
   int hx0 = 0, hx1 = 0, hy0 = 0, hy1 = 0;
   std::vector<B2> writes;  // ranges of the loops writing it
   B2 alloc{0, 0, 0, 0};
@@ -343,6 +352,7 @@ class FusionPlanner {
       }
       if (f.writes.empty()) {
         f.mode = M_RO;
+        f.stageable = !edge && rt.dats_[f.dat]->elem_size == 8;
       } else if (!raw && !hazard && !self_rw) {
         f.mode = M_RW;
       } else {
@@ -355,7 +365,7 @@ class FusionPlanner {
     // tile halos: every access's reach around the core
     for (const DatAccess &a : A.acc) {
       FieldInfo &f = A.fields[a.dat];
-      if (f.mode != M_TILE) continue;
+      if (f.mode != M_TILE && !f.stageable) continue;
       const LoopInfoF &L = A.loops[a.loop];
       f.hx0 = std::max(f.hx0, L.ex0 - a.st.x0);
       f.hx1 = std::max(f.hx1, L.ex1 + a.st.x1 - 1);
@@ -363,7 +373,7 @@ class FusionPlanner {
       f.hy1 = std::max(f.hy1, L.ey1 + a.st.y1 - 1);
     }
     int nbufs = 0;
-    for (auto &kv : A.fields) nbufs += kv.second.mode == M_TILE;
+    for (auto &kv : A.fields) nbufs += kv.second.mode == M_TILE || kv.second.stageable;
     if (nbufs > kMaxBufs) return reject(A, "too many tiles");
 
     // 4. bytes: the fused chain's compulsory traffic against the loops' own
@@ -386,11 +396,11 @@ class FusionPlanner {
   }
 
   // Shared memory of a chain at a tile shape, in doubles (guards included).
-  static int smem_doubles(const ChainAnalysis &A, int TX, int TY) {
+  static int smem_doubles(const ChainAnalysis &A, int TX, int TY, bool stage_ro) {
     long long s = 2 * kGuard;
     for (const auto &kv : A.fields) {
       const FieldInfo &f = kv.second;
-      if (f.mode != M_TILE) continue;
+      if (f.mode != M_TILE && !(stage_ro && f.stageable)) continue;
       s += (long long)(TX + f.hx0 + f.hx1) * (TY + f.hy0 + f.hy1);
     }
     return (int)std::min<long long>(s, 1LL << 30);
@@ -398,7 +408,7 @@ class FusionPlanner {
 
   // The device plan at a tile shape; renames are applied to the runtime's
   // dats (the chain writes the renamed dats into their shadow storage).
-  void build(const std::vector<Desc> &q, const ChainAnalysis &A, int TX, int TY, FPlan &P,
+  void build(const std::vector<Desc> &q, const ChainAnalysis &A, int TX, int TY, bool stage_ro, FPlan &P,
              std::vector<int> &renamed) {
     memset(&P, 0, sizeof(P));
     P.TX = TX;
@@ -416,7 +426,8 @@ class FusionPlanner {
     int off = 0, nwb = 0;
     for (const auto &kv : A.fields) {
       const FieldInfo &f = kv.second;
-      if (f.mode != M_TILE) continue;
+      const bool ro_tile = stage_ro && f.stageable;
+      if (f.mode != M_TILE && !ro_tile) continue;
       const int b = P.nbufs++;
       buf_of[f.dat] = b;
       FBuf &B = P.B[b];
@@ -428,8 +439,12 @@ class FusionPlanner {
       B.ay = (int)d.pitch;
       B.ax0 = f.alloc.x0; B.ax1 = f.alloc.x1; B.ay0 = f.alloc.y0; B.ay1 = f.alloc.y1;
       char *cur = d.origin_ptr();
-      B.src = f.staged ? cur : nullptr;
-      if (f.renamed) {
+      B.src = (f.staged || ro_tile) ? cur : nullptr;
+      if (ro_tile) {  // read-only: staged, never written back
+        B.dst = nullptr;
+        B.wb0 = nwb;
+        B.nwb = 0;
+      } else if (f.renamed) {
         char *&sh = rt.shadow_[f.dat];
         if (!sh) sh = rt.alloc_dat_storage(d.bytes);
         std::swap(d.data_d, sh);  // the dat now lives in the former shadow
@@ -491,7 +506,10 @@ class FusionPlanner {
             }
             const FieldInfo &f = fit->second;
             F.mode = f.mode;
-            if (f.mode == M_TILE) F.buf = buf_of.at(a.dat);
+            if (buf_of.count(a.dat)) {
+              F.mode = M_TILE;
+              F.buf = buf_of.at(a.dat);
+            }
             F.masked = f.mode == M_RW && (a.acc == ACC_WRITE || a.acc == ACC_RW);
             F.slot = (int)i;
             break;
@@ -516,17 +534,16 @@ class FusionPlanner {
       }
     }
     P.red_scratch = rt.red_scratch_;
-    validate(A, P);
+    validate(A, P, buf_of);
   }
 
   // Every shared-memory access the plan allows stays inside its tile: each
   // access's reach (the loop's halo depths grown by the stencil box) within
   // the tile's halo, write-back boxes within the allocation, the tiles within
   // the shared memory. Checked on the host for every plan built.
-  static void validate(const ChainAnalysis &A, const FPlan &P) {
+  static void validate(const ChainAnalysis &A, const FPlan &P, const std::map<int, int> &buf_of) {
     for (const DatAccess &a : A.acc) {
-      const FieldInfo &f = A.fields.at(a.dat);
-      if (f.mode != M_TILE) continue;
+      if (!buf_of.count(a.dat)) continue;
       const FLoop &L = P.L[a.loop];
       const FArg &F = P.A[L.arg0 + a.arg];
       if (F.mode != M_TILE || F.buf < 0 || F.buf >= P.nbufs) throw Error(E_STATE, "fusion plan: tile binding");
@@ -583,7 +600,7 @@ struct FusionState {
     int chosen = -1;
     int next = 0;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;  // shape, events
-    std::vector<double> ms = std::vector<double>(kNumShapes, 1e30);
+    std::vector<double> ms = std::vector<double>(kNumCands + 1, 1e30);
   };
   std::map<uint64_t, Tune> tune;
   bool loaded = false;
@@ -595,6 +612,13 @@ struct FusionState {
   std::map<uint64_t, std::vector<std::pair<size_t, size_t>>> bounds;
   std::map<std::pair<int, int>, int> occupancy;  // (group, smem bytes) -> CTAs per SM
   std::set<int> smem_set;
+
+  void drop_plans() {
+    for (auto &kv : plans)
+      if (kv.second.first) cudaFree(kv.second.first);
+    plans.clear();
+    bounds.clear();
+  }
 
   ~FusionState() {
     for (auto &kv : plans)
@@ -633,10 +657,12 @@ struct FusionState {
     while (std::getline(in, line)) {
       std::istringstream ls(line);
       std::string key;
-      int tx = 0, ty = 0;
+      int tx = 0, ty = 0, ro = 0;
       if (!(ls >> key >> tx >> ty)) continue;
+      if (!(ls >> ro)) ro = 0;
+      if (tx == 0 && ty == 0) tune[std::stoull(key, nullptr, 16)].chosen = kUnfused;
       for (int s = 0; s < kNumShapes; s++)
-        if (kShapes[s].tx == tx && kShapes[s].ty == ty) tune[std::stoull(key, nullptr, 16)].chosen = s;
+        if (kShapes[s].tx == tx && kShapes[s].ty == ty) tune[std::stoull(key, nullptr, 16)].chosen = 2 * s + (ro ? 1 : 0);
     }
   }
 
@@ -652,7 +678,8 @@ struct FusionState {
     std::ofstream out(path, std::ios::app);
     if (out) {
       char buf[64];
-      snprintf(buf, sizeof(buf), "%016llx %d %d\n", (unsigned long long)key, kShapes[s].tx, kShapes[s].ty);
+      snprintf(buf, sizeof(buf), "%016llx %d %d %d\n", (unsigned long long)key, s == kUnfused ? 0 : cand_shape(s).tx,
+               s == kUnfused ? 0 : cand_shape(s).ty, s == kUnfused ? 0 : (int)cand_stage_ro(s));
       out << buf;
     }
   }
@@ -685,6 +712,16 @@ struct FusionState {
         if (T.ms[s] < T.ms[best]) best = s;
       T.chosen = best;
       save(key, best);
+      if (trace_on()) {
+        fprintf(stderr, "tuned chain %016llx:", (unsigned long long)key);
+        for (int s : fits)
+          fprintf(stderr, " %s=%.4fms", s == kUnfused ? "unfused"
+                                                      : (std::to_string(cand_shape(s).tx) + "x" +
+                                                         std::to_string(cand_shape(s).ty) + (cand_stage_ro(s) ? "s" : ""))
+                                                            .c_str(),
+                  T.ms[s]);
+        fprintf(stderr, " -> %s\n", best == kUnfused ? "unfused" : "fused");
+      }
       return best;
     }
     *tuning = true;
@@ -705,6 +742,11 @@ struct FusionState {
 FusionState &Runtime::fusion_state() {
   if (!fusion_state_) fusion_state_ = new FusionState();
   return *fusion_state_;
+}
+// An app call's end: its plans (which hold its dats' addresses) go; the
+// tile-shape tuning state stays for the next calls of the same chains.
+void Runtime::release_fusion_plans() {
+  if (fusion_state_) fusion_state_->drop_plans();
 }
 void Runtime::release_fusion_state() {
   delete fusion_state_;
@@ -776,8 +818,8 @@ void Runtime::plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &it
     if (!fp.analyse(q, fb.first, fb.second, *A)) continue;  // the structure was analysed before
     const fuse::GroupInfo &G = fuse::groups()[A->group];
     std::vector<int> fits;
-    for (int s = 0; s < kNumShapes; s++) {
-      const int smem = FusionPlanner::smem_doubles(*A, kShapes[s].tx, kShapes[s].ty) * 8;
+    for (int s = 0; s < kNumCands; s++) {
+      const int smem = FusionPlanner::smem_doubles(*A, cand_shape(s).tx, cand_shape(s).ty, cand_stage_ro(s)) * 8;
       if (smem > kSmemBudget) continue;
       auto ok = S.occupancy.find({A->group, smem});
       if (ok == S.occupancy.end()) {
@@ -789,17 +831,28 @@ void Runtime::plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &it
       }
       if (ok->second > 0) fits.push_back(s);
     }
+    if (tuning_on && !fits.empty()) fits.push_back(kUnfused);
     bool tuning = false;
     const int s = S.shape_for(A->key, fits, tuning_on, &tuning);
-    if (s < 0) continue;
+    if (s < 0 || (s == kUnfused && !tuning)) continue;
     if (trace) FusionPlanner::trace(q, *A, *this);
     FusedItem it;
     it.first = A->first;
     it.n = A->n;
     it.tuning = tuning;
+    it.unfused = s == kUnfused;
     it.key = A->key;
     it.shape = s;
-    it.name = std::string("fused/") + G.name;
+    // timing name: the group and the chain's first and last compute kernels
+    std::string k0, k1;
+    for (size_t l = 0; l < A->n; l++)
+      if (!A->loops[l].copy) {
+        const std::string &kn = q[A->first + l].loop->kernel;
+        const std::string shortname = kn.substr(kn.find('/') + 1);
+        if (k0.empty()) k0 = shortname;
+        k1 = shortname;
+      }
+    it.name = std::string("fused/") + G.name + "[" + k0 + ".." + k1 + "]";
     it.bytes = A->fused_bytes;
     it.loop_bytes = A->loop_bytes;
     it.launch = G.launch;
@@ -813,10 +866,16 @@ void Runtime::plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &it
 // planned after it see the new storage and those before it the old.
 void Runtime::build_fused(const std::vector<Desc> &q, FusedItem &it) {
   FusionState &S = fusion_state();
+  if (it.shape == kUnfused) {  // timing the unfused loops: the planner brackets them with the events
+    it.ev0 = S.event();
+    it.ev1 = S.event();
+    S.tune[it.key].pending.push_back({it.shape, {it.ev0, it.ev1}});
+    return;
+  }
   FusionPlanner fp(*this);
   const ChainAnalysis &A = *std::static_pointer_cast<ChainAnalysis>(it.analysis);
   auto plan = std::make_unique<FPlan>();
-  fp.build(q, A, kShapes[it.shape].tx, kShapes[it.shape].ty, *plan, it.renamed);
+  fp.build(q, A, cand_shape(it.shape).tx, cand_shape(it.shape).ty, cand_stage_ro(it.shape), *plan, it.renamed);
   plan->red_counter = red_counters_ + (A.first % kNumCounters);
   it.smem = plan->smem_doubles * 8;
   const int occ = S.occupancy.at({A.group, it.smem});

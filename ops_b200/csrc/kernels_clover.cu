@@ -742,20 +742,24 @@ REG(advec_mom_kernel_post_pre_advec_x) REG(advec_mom_kernel_post_pre_advec_y)
 REG(advec_mom_kernel1_x_nonvector) REG(advec_mom_kernel1_y_nonvector) REG(advec_mom_kernel2_x) REG(advec_mom_kernel2_y)
 REG(reset_field_kernel1) REG(reset_field_kernel2) REG(field_summary_kernel)
 
-// The hydro cycle's loop kernels as one fusion group: the lazy queue's
-// planner (fusion.cpp) may run any chain of them, with the boundary copies
-// between them, as one tiled kernel.
-static fuse::GroupRegistrar<ideal_gas_kernel, viscosity_kernel, calc_dt_kernel, calc_dt_kernel_min,
+// The hydro cycle's loop kernels as two fusion groups: the lazy queue's
+// planner (fusion.cpp) may run any chain of one group's kernels, with the
+// boundary copies between them, as one tiled kernel. The timestep and
+// Lagrangian loops compile leaner than the advection loops, so they get a
+// group (and register budget) of their own.
+static fuse::GroupRegistrar<3, ideal_gas_kernel, viscosity_kernel, calc_dt_kernel, calc_dt_kernel_min,
                             PdV_kernel_predict, PdV_kernel_nopredict, revert_kernel, accelerate_kernel,
-                            flux_calc_kernelx, flux_calc_kernely, advec_cell_kernel1_xdir, advec_cell_kernel2_xdir,
-                            advec_cell_kernel3_xdir, advec_cell_kernel4_xdir, advec_cell_kernel1_ydir,
-                            advec_cell_kernel2_ydir, advec_cell_kernel3_ydir, advec_cell_kernel4_ydir,
-                            advec_mom_kernel_x1, advec_mom_kernel_y1, advec_mom_kernel_x2, advec_mom_kernel_y2,
+                            flux_calc_kernelx, flux_calc_kernely, reset_field_kernel1, reset_field_kernel2>
+    fused_lagrange("cloverleaf2d_lagrange");
+static fuse::GroupRegistrar<2, advec_cell_kernel1_xdir, advec_cell_kernel2_xdir, advec_cell_kernel3_xdir,
+                            advec_cell_kernel4_xdir, advec_cell_kernel1_ydir, advec_cell_kernel2_ydir,
+                            advec_cell_kernel3_ydir, advec_cell_kernel4_ydir, advec_mom_kernel_x1,
+                            advec_mom_kernel_y1, advec_mom_kernel_x2, advec_mom_kernel_y2,
                             advec_mom_kernel_mass_flux_x, advec_mom_kernel_mass_flux_y,
                             advec_mom_kernel_post_pre_advec_x, advec_mom_kernel_post_pre_advec_y,
                             advec_mom_kernel1_x_nonvector, advec_mom_kernel1_y_nonvector, advec_mom_kernel2_x,
-                            advec_mom_kernel2_y, reset_field_kernel1, reset_field_kernel2>
-    fused_group("cloverleaf2d");
+                            advec_mom_kernel2_y>
+    fused_advect("cloverleaf2d_advect");
 
 // Named constants (ops_decl_const in clover_leaf.cpp:147-160).
 struct ConstReg {

@@ -633,9 +633,9 @@ void Runtime::collect_timing() {
 }
 
 // Every item of a flush, in queue order, with its launch resolved now: fused
-// chains (fusion.cpp), then runtime-internal items, chain rules (batched
-// boundary copies) and single loops. Storage moves made by a fused chain
-// are visible to the items planned after it only.
+// chains (fusion.cpp) and, between them, runtime-internal items, chain rules
+// (batched boundary copies) and single loops. Storage moves made by a fused
+// chain are visible to the items planned after it only.
 void Runtime::plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::vector<int> &renamed,
                          bool &tuning) {
   out.clear();
@@ -643,13 +643,24 @@ void Runtime::plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::
   tuning = false;
   std::vector<FusedItem> fused;
   plan_fusion(q, fused);
-  auto &chains = registry().chains;
-  size_t fi = 0;
   size_t i = 0;
-  while (i < q.size()) {
-    if (fi < fused.size() && fused[fi].first == i) {
-      FusedItem &f = fused[fi++];
-      build_fused(q, f);
+  for (FusedItem &f : fused) {
+    plan_plain(q, i, f.first, out);
+    build_fused(q, f);
+    if (f.unfused) {
+      // the tuner times this chain's loops run one by one: events around them
+      tuning = true;
+      cudaEvent_t e0 = f.ev0, e1 = f.ev1;
+      PlanItem a;
+      a.name = "runtime/tune_begin";
+      a.run = [e0](cudaStream_t s) { OPSB_CUDA(cudaEventRecord(e0, s)); };
+      out.push_back(std::move(a));
+      plan_plain(q, f.first, f.first + f.n, out);
+      PlanItem b;
+      b.name = "runtime/tune_end";
+      b.run = [e1](cudaStream_t s) { OPSB_CUDA(cudaEventRecord(e1, s)); };
+      out.push_back(std::move(b));
+    } else {
       renamed.insert(renamed.end(), f.renamed.begin(), f.renamed.end());
       tuning = tuning || f.tuning;
       PlanItem it;
@@ -670,10 +681,17 @@ void Runtime::plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::
         if (e1) OPSB_CUDA(cudaEventRecord(e1, s));
       };
       out.push_back(std::move(it));
-      i += f.n;
-      continue;
     }
-    const size_t limit = fi < fused.size() ? fused[fi].first : q.size();
+    i = f.first + f.n;
+  }
+  plan_plain(q, i, q.size(), out);
+}
+
+// The items of q[from, to) that no fused chain covers.
+void Runtime::plan_plain(std::vector<Desc> &q, size_t from, size_t to, std::vector<PlanItem> &out) {
+  auto &chains = registry().chains;
+  size_t i = from;
+  while (i < to) {
     if (q[i].loop->internal) {
       out.push_back(prepare_swap_outside(q[i]));
       i++;
@@ -683,7 +701,7 @@ void Runtime::plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::
       bool done = false;
       for (auto &rule : chains) {
         int n = rule.match(q, i);
-        n = (int)std::min<size_t>((size_t)std::max(n, 0), limit - i);
+        n = (int)std::min<size_t>((size_t)std::max(n, 0), to - i);
         if (n > 0) {
           out.push_back(rule.prepare(q, i, n));
           i += n;
@@ -946,7 +964,7 @@ void Runtime::release_to(const Mark &m) {
     }
     dats_.pop_back();
   }
-  release_fusion_state();
+  release_fusion_plans();
   while (reductions_.size() > m.reductions) {
     reductions_.pop_back();
   }

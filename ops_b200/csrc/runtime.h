@@ -148,6 +148,7 @@ struct FusedItem {
   std::string name;
   double bytes = 0.0, loop_bytes = 0.0;  // compulsory bytes fused / as separate loops
   bool tuning = false;                   // this execution times a candidate tile shape
+  bool unfused = false;                  // the candidate is the loops run one by one
   uint64_t key = 0;
   int shape = 0, grid = 0, smem = 0;
   std::vector<int> renamed;              // dats moved to their shadow storage by this chain
@@ -292,10 +293,12 @@ class Runtime {
   PlanItem prepare_swap_outside(const Desc &d);
   void plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::vector<int> &renamed, bool &tuning);
   void launch_plan(std::vector<PlanItem> &items);
+  void plan_plain(std::vector<Desc> &q, size_t from, size_t to, std::vector<PlanItem> &out);
   void plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &items);
   void build_fused(const std::vector<Desc> &q, FusedItem &item);
   FusionState &fusion_state();
   void release_fusion_state();
+  void release_fusion_plans();
   void apply_renames(const std::vector<int> &renamed);
   void add_fusion_stats(const FusionStats &s);
   uint64_t queue_key(const std::vector<Desc> &q) const;
@@ -363,7 +366,7 @@ class Runtime {
   double cur_bytes_ = 0.0;
   cudaEvent_t cur_ev_ = nullptr;
   int fusion_on_ = 1;
-  int tiling_on_ = 0;  // loop-chain fusion into tiled kernels (needs fusion_on_)
+  int tiling_on_ = 1;  // loop-chain fusion into tiled kernels (needs fusion_on_)
   // Redundant-loop elimination within one flush: per queued loop, the
   // version of each dat arg (read: as observed, written: as produced);
   // dat versions count the writes of the queued loops and restart at every
