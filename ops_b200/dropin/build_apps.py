@@ -31,10 +31,22 @@ CLOVER_OPS = ("clover_leaf.cpp initialise_chunk.cpp generate.cpp ideal_gas.cpp u
               "reset_field.cpp").split()
 CLOVER_OTHER = "start.cpp time_step.cpp build_field.cpp read_input.cpp initialise.cpp advection.cpp".split()
 
-# name: (source directory in the reference tree, registry prefix, OPS files, other files)
+TEA_OPS = ("tea_leaf.cpp field_summary.cpp generate.cpp initialise_chunk.cpp start.cpp set_field.cpp tea_leaf_cg.cpp "
+           "tea_leaf_cheby.cpp tea_leaf_common.cpp tea_leaf_jacobi.cpp tea_leaf_ppcg.cpp update_halo.cpp").split()
+
+
+def _other_cpp(ref, srcrel, opsf):
+    """The application's remaining .cpp files (compiled as they are)."""
+    d = os.path.join(ref, srcrel)
+    return sorted(f for f in os.listdir(d) if f.endswith(".cpp") and f not in opsf)
+
+
+# name: (source directory in the reference tree, registry prefix, OPS files, other files or None = all others)
 APPS = {
     "laplace2d_step7": ("apps/c/laplace2d_tutorial/step7", "laplace2d", ["laplace2d.cpp"], []),
     "cloverleaf": ("apps/c/CloverLeaf", "cloverleaf_dropin", CLOVER_OPS, CLOVER_OTHER),
+    "cloverleaf3d": ("apps/c/CloverLeaf_3D", "cloverleaf3d_dropin", CLOVER_OPS, CLOVER_OTHER),
+    "tealeaf": ("apps/c/TeaLeaf", "tealeaf_dropin", TEA_OPS, None),
 }
 
 
@@ -63,6 +75,8 @@ def shim_object(ref):
 
 def build_app(ref, name):
     srcrel, prefix, opsf, other = APPS[name]
+    if other is None:
+        other = _other_cpp(ref, srcrel, opsf)
     src = os.path.join(ref, srcrel)
     inc = os.path.join(ref, "ops", "c", "include")
     wd = os.path.join(OUT, name)

@@ -24,6 +24,7 @@
 #include "ops_lib_core.h"
 #include "ops_instance.h"
 #include "ops_util.h"
+#include "ops_checkpointing.h"
 #include "ops_dropin.h"
 
 namespace {
@@ -171,6 +172,46 @@ namespace {
 alignas(OPS_instance) unsigned char g_instance_storage[sizeof(OPS_instance)];
 }
 OPS_instance *OPS_instance::getOPSInstance() { return reinterpret_cast<OPS_instance *>(g_instance_storage); }
+
+// Row and plane sizes the legacy kernel style addresses through
+// (OPS_ACC<n>(x, y) = x + xdim<n> * y, ops/c/include/ops_macros.h:2785-2870).
+// The device functors the sm100a target makes from such kernels use
+// accessors instead; these definitions only satisfy the host copies of the
+// kernel functions that an application's translated files still compile.
+extern "C" {
+int xdim0, xdim1, xdim2, xdim3, xdim4, xdim5, xdim6, xdim7, xdim8, xdim9, xdim10, xdim11, xdim12, xdim13, xdim14,
+    xdim15, xdim16, xdim17, xdim18, xdim19, xdim20, xdim21, xdim22, xdim23, xdim24, xdim25, xdim26, xdim27, xdim28,
+    xdim29, xdim30, xdim31, xdim32, xdim33, xdim34, xdim35, xdim36, xdim37, xdim38, xdim39, xdim40, xdim41, xdim42,
+    xdim43, xdim44, xdim45, xdim46, xdim47, xdim48, xdim49, xdim50, xdim51, xdim52, xdim53, xdim54, xdim55, xdim56,
+    xdim57, xdim58, xdim59, xdim60, xdim61, xdim62, xdim63, xdim64, xdim65, xdim66, xdim67, xdim68, xdim69, xdim70,
+    xdim71, xdim72, xdim73, xdim74, xdim75, xdim76, xdim77, xdim78, xdim79, xdim80, xdim81, xdim82, xdim83, xdim84,
+    xdim85, xdim86, xdim87, xdim88, xdim89, xdim90, xdim91, xdim92, xdim93, xdim94, xdim95, xdim96, xdim97, xdim98,
+    xdim99;
+int ydim0, ydim1, ydim2, ydim3, ydim4, ydim5, ydim6, ydim7, ydim8, ydim9, ydim10, ydim11, ydim12, ydim13, ydim14,
+    ydim15, ydim16, ydim17, ydim18, ydim19, ydim20, ydim21, ydim22, ydim23, ydim24, ydim25, ydim26, ydim27, ydim28,
+    ydim29, ydim30, ydim31, ydim32, ydim33, ydim34, ydim35, ydim36, ydim37, ydim38, ydim39, ydim40, ydim41, ydim42,
+    ydim43, ydim44, ydim45, ydim46, ydim47, ydim48, ydim49, ydim50, ydim51, ydim52, ydim53, ydim54, ydim55, ydim56,
+    ydim57, ydim58, ydim59, ydim60, ydim61, ydim62, ydim63, ydim64, ydim65, ydim66, ydim67, ydim68, ydim69, ydim70,
+    ydim71, ydim72, ydim73, ydim74, ydim75, ydim76, ydim77, ydim78, ydim79, ydim80, ydim81, ydim82, ydim83, ydim84,
+    ydim85, ydim86, ydim87, ydim88, ydim89, ydim90, ydim91, ydim92, ydim93, ydim94, ydim95, ydim96, ydim97, ydim98,
+    ydim99;
+int zdim0, zdim1, zdim2, zdim3, zdim4, zdim5, zdim6, zdim7, zdim8, zdim9, zdim10, zdim11, zdim12, zdim13, zdim14,
+    zdim15, zdim16, zdim17, zdim18, zdim19, zdim20, zdim21, zdim22, zdim23, zdim24, zdim25, zdim26, zdim27, zdim28,
+    zdim29, zdim30, zdim31, zdim32, zdim33, zdim34, zdim35, zdim36, zdim37, zdim38, zdim39, zdim40, zdim41, zdim42,
+    zdim43, zdim44, zdim45, zdim46, zdim47, zdim48, zdim49, zdim50, zdim51, zdim52, zdim53, zdim54, zdim55, zdim56,
+    zdim57, zdim58, zdim59, zdim60, zdim61, zdim62, zdim63, zdim64, zdim65, zdim66, zdim67, zdim68, zdim69, zdim70,
+    zdim71, zdim72, zdim73, zdim74, zdim75, zdim76, zdim77, zdim78, zdim79, zdim80, zdim81, zdim82, zdim83, zdim84,
+    zdim85, zdim86, zdim87, zdim88, zdim89, zdim90, zdim91, zdim92, zdim93, zdim94, zdim95, zdim96, zdim97, zdim98,
+    zdim99;
+int udim0, udim1, udim2, udim3, udim4, udim5, udim6, udim7, udim8, udim9, udim10, udim11, udim12, udim13, udim14,
+    udim15, udim16, udim17, udim18, udim19, udim20, udim21, udim22, udim23, udim24, udim25, udim26, udim27, udim28,
+    udim29, udim30, udim31, udim32, udim33, udim34, udim35, udim36, udim37, udim38, udim39, udim40, udim41, udim42,
+    udim43, udim44, udim45, udim46, udim47, udim48, udim49, udim50, udim51, udim52, udim53, udim54, udim55, udim56,
+    udim57, udim58, udim59, udim60, udim61, udim62, udim63, udim64, udim65, udim66, udim67, udim68, udim69, udim70,
+    udim71, udim72, udim73, udim74, udim75, udim76, udim77, udim78, udim79, udim80, udim81, udim82, udim83, udim84,
+    udim85, udim86, udim87, udim88, udim89, udim90, udim91, udim92, udim93, udim94, udim95, udim96, udim97, udim98,
+    udim99;
+}
 
 // GPU power sampling is not part of this backend (NVML is out of scope).
 void OPS_instance::reset_power_counters() {}
@@ -757,11 +798,36 @@ void ops_NaNcheck(ops_dat dat) {
     }
 }
 
-// Checkpointing is out of scope: the call reports that no checkpoint was
-// restored and the run starts from the beginning.
+// Checkpointing (ops/c/include/ops_checkpointing.h) is out of scope: no
+// checkpoint is ever restored or written, so every call reports that the run
+// proceeds normally from the beginning.
 bool ops_checkpointing_init(const char *filename, double interval, int options) {
   (void)filename;
   (void)interval;
   (void)options;
+  return false;
+}
+void ops_checkpointing_initphase_done() {}
+void ops_checkpointing_manual_datlist(int ndats, ops_dat *datlist) {
+  (void)ndats;
+  (void)datlist;
+}
+bool ops_checkpointing_fastfw(int nbytes, char *payload) {
+  (void)nbytes;
+  (void)payload;
+  return false;
+}
+bool ops_checkpointing_manual_datlist_fastfw(int ndats, ops_dat *datlist, int nbytes, char *payload) {
+  (void)ndats;
+  (void)datlist;
+  (void)nbytes;
+  (void)payload;
+  return false;
+}
+bool ops_checkpointing_manual_datlist_fastfw_trigger(int ndats, ops_dat *datlist, int nbytes, char *payload) {
+  (void)ndats;
+  (void)datlist;
+  (void)nbytes;
+  (void)payload;
   return false;
 }

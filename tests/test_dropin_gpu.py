@@ -11,6 +11,8 @@ target and linked against ops_b200/dropin/ops_dropin.cu and libops_b200.so
   the reference's own OpenMP build (tests/golden/clover_64x64_s30.npz): dt of
   every step exactly, the field summaries to 1e-12 relative, and every dumped
   field bit for bit.
+* apps/c/CloverLeaf_3D and apps/c/TeaLeaf (Jacobi, CG and PPCG decks): the
+  same bars against their goldens (below).
 """
 import os
 import subprocess
@@ -54,6 +56,51 @@ def test_cloverleaf_matches_reference_golden(tmp_path):
     np.testing.assert_allclose(summ[:, 1:], ref[:, 1:], rtol=1e-12, atol=0)
     assert np.array_equal(dts, g["dts"])
     for f in FIELDS:
+        ext = g["f_" + f]
+        got = np.fromfile(str(tmp_path / (f + ".bin"))).reshape(ext.shape)
+        assert np.array_equal(got, ext), f
+
+
+def _run_app(name, tmp_path, deck_file, deck_text):
+    (tmp_path / deck_file).write_text(deck_text)
+    env = dict(os.environ, OPS_B200_PRINT_FULL="1", OPS_B200_DUMP_DIR=str(tmp_path))
+    r = subprocess.run([_binary(name)], cwd=tmp_path, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    return r.stdout
+
+
+@pytest.mark.parametrize("case", ["tea_kat_jacobi", "tea_cg_jacdiag_64", "tea_ppcg_jacdiag_64"])
+def test_tealeaf_matches_reference_golden(tmp_path, case):
+    """apps/c/TeaLeaf unmodified: solver iteration counts exactly, field
+    summaries to 1e-12; the Jacobi deck's fields bit for bit (its sums are
+    per cell; CG and PPCG take dot products in another order)."""
+    g = np.load(os.path.join(GOLDEN, case + ".npz"))
+    stdout = _run_app("tealeaf", tmp_path, "tea.in", str(g["deck"]))
+    out = (tmp_path / "tea.out").read_text()
+    summ = np.array([[float(x) for x in l.split()[1:7]] for l in out.splitlines() if l.strip().startswith("step:")])
+    iters = np.array([int(l.split()[-1]) for l in stdout.splitlines() if l.strip().startswith("Iteration count")])
+    assert np.array_equal(iters, g["iters"])
+    np.testing.assert_allclose(summ, g["summaries"], rtol=1e-12, atol=0)
+    if case == "tea_kat_jacobi":
+        for f in ("u", "energy1", "density"):
+            ext = g["f_" + f]
+            got = np.fromfile(str(tmp_path / (f + ".bin"))).reshape(ext.shape)
+            assert np.array_equal(got, ext), f
+
+
+def test_cloverleaf3d_matches_reference_golden(tmp_path):
+    """apps/c/CloverLeaf_3D unmodified (3D accessors, edge dats in all three
+    directions): dt of every step exactly, summaries to 1e-12, the dumped
+    fields bit for bit."""
+    g = np.load(os.path.join(GOLDEN, "clover3d_24x20x16_s40.npz"))
+    stdout = _run_app("cloverleaf3d", tmp_path, "clover.in", str(g["deck"]))
+    out = (tmp_path / "clover.out").read_text()
+    summ = np.array([[float(x) for x in l.split()[1:9]] for l in out.splitlines() if l.strip().startswith("step:")])
+    dts = np.array([float(l.split()[7]) for l in stdout.splitlines() if l.strip().startswith("Step ")])
+    assert summ.shape == g["summaries"].shape
+    np.testing.assert_allclose(summ, g["summaries"], rtol=1e-12, atol=0)
+    assert np.array_equal(dts, g["dts"])
+    for f in ("density0", "energy0", "pressure", "xvel0", "yvel0", "zvel0"):
         ext = g["f_" + f]
         got = np.fromfile(str(tmp_path / (f + ".bin"))).reshape(ext.shape)
         assert np.array_equal(got, ext), f
