@@ -763,6 +763,30 @@ def tea_deck(steps, n=TEA_N, max_iters=200000, **kw):
                          preconditioner=1, states=seeded.tea_config4_states(n, n, 4), **kw)
 
 
+def cpu_reference_tea_converged(threads, n=TEA_N):
+    """The reference OpenMP TeaLeaf's Jacobi-PCG on the same deck run to its
+    own stopping test (eps 1e-10): (solve seconds, iterations). The solve time
+    is the wall-time difference to the same run capped at 2 iterations (its
+    set-up), plus those 2 iterations at the run's own mean rate."""
+    import oracle
+    from ops_b200 import apps
+    exe = oracle.reference_binary("tealeaf")
+    if exe is None:
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+    wall, iters = [], []
+    for m in (2, 200000):
+        with tempfile.TemporaryDirectory() as td:
+            with open(os.path.join(td, "tea.in"), "w") as f:
+                f.write(apps.tea_deck_text(tea_deck(1, n, max_iters=m)))
+            r = subprocess.run([exe], cwd=td, capture_output=True, text=True, env=env, timeout=1800, check=True)
+        wall.append([float(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Total Wall time")][-1])
+        iters.append([int(l.split()[-1]) for l in r.stdout.splitlines() if l.strip().startswith("Iteration count")][-1])
+    n_it = iters[1]
+    per_it = (wall[1] - wall[0]) / max(1, n_it - 2)
+    return (wall[1] - wall[0]) + 2 * per_it, n_it
+
+
 def cpu_reference_tea(iters, threads, n=TEA_N):
     """Seconds per CG iteration of the reference OpenMP TeaLeaf on the same
     deck: two runs capped at 2 and 2 + iters iterations, wall-time difference."""
@@ -882,15 +906,10 @@ def bench_tea(args, world, rank, local, pg):
 def reference_tea(args, world, rank):
     threads = os.cpu_count() or 1
     N = args.grid or TEA_N
-    base = cpu_reference_tea(args.cpu_tea_iters, threads, N)
+    base = cpu_reference_tea_converged(threads, N)
     if base is None:
         return {"impl": "reference", "unavailable": "oracle/_ref/bin/tealeaf was not built"}
-    per_it, wall = base
-    # FP64 Jacobi-PCG iterations to ||r|| < 1e-10 ||r0|| at 4096^2, measured by this
-    # repository's solver on the B200: the TeaLeaf deck (tea) and the
-    # cell-centre rasterised fields of the learned workload (learned)
-    iters = args.tea_ref_iters or {"tea": 1712, "learned": 1355, "mg": 1355}.get(args.workload, 1712)
-    v = per_it * iters
+    v, iters = base
     return {
         "impl": "reference",
         "metric": {"learned": "time to 1e-10 residual (learned FCG)",
@@ -904,9 +923,10 @@ def reference_tea(args, world, rank):
                                                                              f"tealeaf2d_cg_jacdiag_{N}x{N}"),
                    "grid": [N, N], "eps": 1e-10},
         "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference",
-                         "sample": f"reference OpenMP TeaLeaf, CG capped at 2 and {2 + args.cpu_tea_iters} iterations;"
-                                   f" seconds per iteration x {iters} iterations (the FP64 PCG"
-                                   f" count at this size)"},
+                         "sample": f"reference OpenMP TeaLeaf Jacobi-PCG run to its own stopping test"
+                                   f" (sqrt|r.z| < 1e-10 ||r0||, {iters} iterations), one timestep; solve"
+                                   f" time = wall time minus the same run capped at 2 iterations, plus 2"
+                                   f" iterations"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -1206,14 +1226,14 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clover")
     ap.add_argument("--cpu-iters", type=int, default=100)
-    ap.add_argument("--cpu-clover-steps", type=int, default=5)
+    ap.add_argument("--cpu-clover-steps", type=int, default=40,
+                    help="clover/clover3d: most steps the reference arm times (it times --steps, up to this)")
     ap.add_argument("--grid", type=int, default=None, help="clover grid edge (default 3840; smaller for profiling)")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64", help="adi workload precision")
     ap.add_argument("--adi-case", choices=["cube", "batch"], default="cube", help="adi: 256^3 block or 64 uneven blocks")
     ap.add_argument("--reliable-delta", type=float, default=0.1,
                     help="tea: FP32 residual decrease between FP64 reliable updates")
     ap.add_argument("--cpu-tea-iters", type=int, default=100, help="tea: CG iterations in the CPU sample")
-    ap.add_argument("--tea-ref-iters", type=int, default=0, help="tea: FP64 PCG iterations to solution (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:

@@ -461,6 +461,18 @@ void launch_exec(const LoopParams &lp, dim3 g, dim3 b, cudaStream_t s) {
   exec_loop<K><<<g, b, 0, s>>>(lp);
 }
 
+// A kernel may bring its own launch (a specialised executor for its access
+// pattern) as `static void launch(const LoopParams &, dim3, dim3,
+// cudaStream_t)`; the runtime's grid shape is passed along as a hint.
+template <class K, class = void>
+struct CustomLaunch {
+  static constexpr bool value = false;
+};
+template <class K>
+struct CustomLaunch<K, std::void_t<decltype(&K::launch)>> {
+  static constexpr bool value = true;
+};
+
 template <class K, class = void>
 struct CopyTrait { static constexpr int dst = -1, src = -1; };
 template <class K>
@@ -478,7 +490,10 @@ LoopInfo make_loop_info(const char *kernel) {
     if (li.params[i].cls == 'A') li.ndim = li.params[i].ndim;
   li.copy_dst = CopyTrait<K>::dst;
   li.copy_src = CopyTrait<K>::src;
-  li.launch = &launch_exec<K>;
+  if constexpr (CustomLaunch<K>::value)
+    li.launch = &K::launch;
+  else
+    li.launch = &launch_exec<K>;
   li.mgrid_ok = LoopMgridOk<K>::value ? 1 : 0;
   return li;
 }
