@@ -144,10 +144,14 @@ int ops_b200_reduction_result(int handle, void *out);
 
 /* ops_dat_set_data / ops_dat_fetch_data
  * (ops/c/src/core/ops_dummy_singlenode.cpp:737-808): the full extent
- * (halos included), x fastest; `bytes` must equal that extent. */
+ * (halos included), x fastest; `bytes` must equal that extent. On a block
+ * partitioned across ranks (ops_b200_partition) they cover the rank's owned
+ * part, the extents ops_b200_dat_get_extents reports. */
 int ops_b200_dat_set_data(int dat, const void *data, size_t bytes);
 int ops_b200_dat_fetch_data(int dat, void *data, size_t bytes);
-/* ops_dat_get_extents: disp/size of the full extent (dims entries each). */
+/* ops_dat_get_extents: disp/size of the full extent (dims entries each);
+ * on a partitioned block, of the rank's owned part, disp counted from the
+ * dat's first point (ops/c/src/mpi/ops_mpi_rt_support.cpp:2216-2225). */
 int ops_b200_dat_get_extents(int dat, int *disp, int *size);
 /* ops_dat_get_raw_pointer / ops_dat_release_raw_data
  * (ops/c/src/core/ops_dummy_singlenode.cpp:662-735). Returns a pointer to
@@ -157,10 +161,13 @@ int ops_b200_dat_get_raw_pointer(int dat, int memspace, void **ptr, int *stride)
 int ops_b200_dat_release_raw_data(int dat, int acc);
 
 /* Runtime options: "graphs" (CUDA-graph replay of repeated flushes, default
- * 1), "fusion" (copy elision and chain kernels, default 1) and "tiling"
+ * 1), "fusion" (copy elision and chain kernels, default 1), "tiling"
  * (loop-chain fusion: runs of queued 2D loops executed as one kernel over
  * shared-memory tiles, default 1, needs "fusion"; the counterpart of the
- * reference's lazy tiling, ops/c/src/core/ops_lazy.cpp:380-1173). */
+ * reference's lazy tiling, ops/c/src/core/ops_lazy.cpp:380-1173) and
+ * "lists" (consecutive independent loops of one kernel, e.g. over the
+ * blocks of a multi-block application, launched as one kernel over a work
+ * list of their uneven domains, default 1, needs "fusion"). */
 int ops_b200_set_option(const char *name, int value);
 /* Counters since the last reset: kernels launched by this library, CUDA
  * graphs launched, loops queued. */
@@ -183,6 +190,63 @@ int ops_b200_fusion_stats(long long *chains, long long *loops, double *fused_byt
  * counterpart. */
 int ops_b200_release_spare_storage(long long *freed);
 
+/* ---- Decomposition across processes (one process per GPU) ----------------
+ * The reference's MPI backend (ops/c/src/mpi/): ops_partition splits every
+ * block across the ranks (ops_mpi_partition.cpp:84-256, ops_decomp :257),
+ * loops run over their rank's part, ops_halo_exchanges brings in the
+ * neighbours' rows a stencil reads (ops_mpi_rt_support.cpp:836) and
+ * reductions combine across ranks (:1271-1307). Here each block of 2 or 3
+ * dimensions is split into slabs along its outermost dimension (y in 2D, z
+ * in 3D) by the reference's integer division of its extent; dats of extent
+ * 1 along it are replicated. Loop indices stay global. Reductions combine
+ * in rank order (reproducible sums). Every rank must make the same calls in
+ * the same order, as with MPI. */
+
+/* One transfer of a host-transport exchange: send_bytes from `send` to rank
+ * `peer`, and recv_bytes from `peer` into `recv` (host memory). */
+typedef struct ops_b200_msg {
+  int peer;
+  const void *send;
+  size_t send_bytes;
+  void *recv;
+  size_t recv_bytes;
+} ops_b200_msg;
+/* Host transport callbacks (return 0 on success): `exchange` completes all n
+ * transfers before it returns (a rank's sends and receives may pair with
+ * one another, so post them together); `allgather` stores every rank's
+ * `bytes` from `send` in rank order at `recv`. */
+typedef int (*ops_b200_exchange_fn)(void *ctx, const ops_b200_msg *msgs, int n);
+typedef int (*ops_b200_allgather_fn)(void *ctx, const void *send, size_t bytes, void *recv);
+/* The transport is set before ops_b200_partition (may precede ops_b200_init).
+ * Host: the runtime flushes its queue at an exchange and stages the rows
+ * through pinned memory (any transport: gloo, sockets, MPI). */
+int ops_b200_set_transport_host(int nranks, int rank, ops_b200_exchange_fn exchange, ops_b200_allgather_fn allgather,
+                                void *ctx);
+/* NCCL (after ops_b200_init, on the runtime's device): exchanges become
+ * ncclSend/ncclRecv on the runtime stream, queued and graph-captured with
+ * the loops. Rank 0 makes the 128-byte id, every rank passes it. */
+int ops_b200_nccl_unique_id(void *id128);
+int ops_b200_set_transport_nccl(const void *id128, int nranks, int rank);
+/* ops_partition (ops/c/include/ops_lib_core.h: ops_partition(const char*)):
+ * partitions the blocks declared since the last call; a no-op with one rank
+ * or no transport, as in the reference's single-process backends. */
+int ops_b200_partition(const char *routine);
+/* This process's rank and the number of ranks (1, 0 without a transport),
+ * and the halo exchanges made since ops_b200_init. */
+int ops_b200_rank_info(int *rank, int *nranks, long long *exchanges);
+/* A block's slab on this rank: split dimension (-1: not split), the block's
+ * extent along it, the owned interior [lo, hi) and the halo depth. */
+int ops_b200_block_slab(int block, int *split_dim, int *extent, int *lo, int *hi, int *halo);
+/* The slab arithmetic alone (no runtime, no GPU): rank `rank` of `nranks`
+ * owns [lo, hi) of `extent` (ops_partition_blocks' integer division), and a
+ * dat spanning [gstart, gend) along the split keeps [win_lo, win_hi) of which
+ * it owns [own_lo, own_hi), with `halo` rows of each neighbour. */
+int ops_b200_slab_window(int extent, int nranks, int rank, int halo, int gstart, int gend, int *lo, int *hi,
+                         int *own_lo, int *own_hi, int *win_lo, int *win_hi);
+/* Exercises the host transport without a GPU: each rank sends a pattern to
+ * its neighbours and gathers every rank's id; returns 0 when all arrived. */
+int ops_b200_transport_selftest(void);
+
 /* Per-kernel device timing: while enabled, every launch is bracketed by CUDA
  * events on the runtime stream (graph replay is bypassed). Query by kernel
  * name ("laplace2d/apply_stencil", a chain rule name, ...): launches and total
@@ -203,7 +267,11 @@ int ops_b200_kernel_stats(ops_b200_kernel_stat *out, int max);
 
 /* ---- apps ----------------------------------------------------------------
  * Reference app drivers restated in C++ on the runtime above; they issue the
- * same sequence of loops as the reference drivers.
+ * same sequence of loops as the reference drivers, ops_partition included
+ * at the reference's point. With a transport of several ranks set, every
+ * rank calls the driver with the same deck; outputs are then the rank's
+ * owned part (Laplace: its rows of field_out; dumps: owned part per dat)
+ * and reductions are global.
  *
  * Laplace Jacobi (apps/c/laplace2d_tutorial/step7/laplace2d.cpp:41-124):
  * `field_in` is A's full extent ((imax+2)*(jmax+2) doubles, x fastest, halo

@@ -95,6 +95,15 @@ class TeaDeck(ctypes.Structure):
                 ("ch_cg_epslim", ctypes.c_double), ("ppcg_inner_steps", ctypes.c_int)]
 
 
+class Msg(ctypes.Structure):
+    _fields_ = [("peer", ctypes.c_int), ("send", ctypes.c_void_p), ("send_bytes", ctypes.c_size_t),
+                ("recv", ctypes.c_void_p), ("recv_bytes", ctypes.c_size_t)]
+
+
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(Msg), ctypes.c_int)
+ALLGATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+
+
 class HeatSystem(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("pitch", ctypes.c_longlong),
                 ("Kx", ctypes.c_void_p), ("Ky", ctypes.c_void_p), ("u0", ctypes.c_void_p), ("u", ctypes.c_void_p),
@@ -168,6 +177,14 @@ def _declare(L):
         "ops_b200_reset_counters": ([], i),
         "ops_b200_release_spare_storage": ([P], i),
         "ops_b200_fusion_stats": ([P, P, P, P], i),
+        "ops_b200_set_transport_host": ([i, i, EXCHANGE_FN, ALLGATHER_FN, P], i),
+        "ops_b200_nccl_unique_id": ([P], i),
+        "ops_b200_set_transport_nccl": ([P, i, i], i),
+        "ops_b200_partition": ([cp], i),
+        "ops_b200_rank_info": ([P, P, P], i),
+        "ops_b200_block_slab": ([i, P, P, P, P, P], i),
+        "ops_b200_slab_window": ([i, i, i, i, i, i, P, P, P, P, P, P], i),
+        "ops_b200_transport_selftest": ([], i),
         "ops_b200_tridsolver_params_init": ([P, i, i], i),
         "ops_b200_tridsolver_params_set_jacobi_params": ([P, d, d, i], i),
         "ops_b200_tridsolver_params_set_batch_size": ([P, i], i),

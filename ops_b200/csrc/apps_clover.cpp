@@ -656,6 +656,7 @@ struct Clover {
     dtold = dtinit;
     dt = dtinit;
     build_field();
+    r.partition("2D_BLOCK_DECOMPSE");  // build_field.cpp:235
     initialise_chunk();
     generate();
     advect_x = 1;
@@ -733,7 +734,7 @@ extern "C" int ops_b200_app_cloverleaf(const ops_b200_clover_deck *deck, int war
     if (dump_dir) {
       for (int i = mk.dats; i < r.ndats(); i++) {
         Dat &d = r.dat(i);
-        std::vector<char> buf((size_t)d.size[0] * d.size[1] * d.size[2] * d.elem_size);
+        std::vector<char> buf(r.dat_data_bytes(i));  // the rank's owned part when partitioned
         r.dat_fetch_data(i, buf.data(), buf.size());
         std::string path = std::string(dump_dir) + "/" + d.name + ".bin";
         FILE *f = fopen(path.c_str(), "wb");

@@ -798,6 +798,7 @@ struct Clover3D {
     dtold = dtinit;
     dt = dtinit;
     build_field();
+    r.partition("3D_BLOCK_DECOMPOSE");  // build_field.cpp:318
     initialise_chunk();
     generate();
     advect_x = 1;
@@ -876,7 +877,7 @@ extern "C" int ops_b200_app_cloverleaf3d(const ops_b200_clover3d_deck *deck, int
     if (dump_dir) {
       for (int i = mk.dats; i < r.ndats(); i++) {
         Dat &d = r.dat(i);
-        std::vector<char> buf((size_t)d.size[0] * d.size[1] * d.size[2] * d.elem_size);
+        std::vector<char> buf(r.dat_data_bytes(i));  // the rank's owned part when partitioned
         r.dat_fetch_data(i, buf.data(), buf.size());
         std::string path = std::string(dump_dir) + "/" + d.name + ".bin";
         FILE *f = fopen(path.c_str(), "wb");

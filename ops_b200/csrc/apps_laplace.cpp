@@ -37,6 +37,7 @@ extern "C" int ops_b200_app_laplace2d(int imax, int jmax, int warmup, int iters,
     int s5pt[] = {0, 0, 1, 0, -1, 0, 0, 1, 0, -1};
     int s5 = r.decl_stencil(2, 5, s5pt, nullptr, "5pt");
     int h_err = r.decl_reduction(sizeof(double), "double", "error");
+    r.partition("");  // laplace2d.cpp:61
     r.decl_const("imax", 1, "int", &imax);
     r.decl_const("jmax", 1, "int", &jmax);
 
@@ -59,7 +60,13 @@ extern "C" int ops_b200_app_laplace2d(int imax, int jmax, int warmup, int iters,
     OPSB_CUDA(cudaEventRecord(e1, r.stream()));
     OPSB_CUDA(cudaEventSynchronize(e1));
     if (device_seconds) *device_seconds = ev.ms() * 1e-3;
-    if (field_out) r.dat_fetch_data(dA, field_out, (size_t)(imax + 2) * (jmax + 2) * sizeof(double));
+    if (field_out) {
+      // partitioned across ranks: this rank's owned rows, in place in the
+      // whole (imax + 2) x (jmax + 2) array
+      int disp[2], ext[2];
+      r.dat_get_extents(dA, disp, ext);
+      r.dat_fetch_data(dA, field_out + (size_t)disp[1] * (imax + 2), r.dat_data_bytes(dA));
+    }
     scope.release();
     return 0;
   });

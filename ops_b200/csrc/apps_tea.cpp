@@ -666,6 +666,9 @@ struct Tea {
   // The CG solve as the device-resident iteration of heat_pcg.cu: the same
   // coefficient set-up loops, then the solver on the dats' storage.
   void tea_leaf_fused(double rx, double ry) {
+    // the fused solver addresses the whole field on one GPU
+    if (r.partitioned() && r.nranks() > 1)
+      throw Error(E_UNSUPPORTED, "fused heat solves do not run on a block partitioned across ranks");
     r.execute();
     heat::Field2D f;
     f.nx = grid.x_cells;
@@ -848,6 +851,7 @@ struct Tea {
     step = 0;
     dt = dtinit;
     build_field();
+    r.partition("2D_BLOCK_DECOMPSE");  // build_field.cpp:252
     r.decl_const("tealeaf/field", 1, "field_type", &field);
     r.decl_const("tealeaf/grid", 1, "grid_type", &grid);
     r.decl_const("tealeaf/number_of_states", 1, "int", &number_of_states);
@@ -922,7 +926,7 @@ extern "C" int ops_b200_app_tealeaf(const ops_b200_tea_deck *deck, double *summa
     if (dump_dir) {
       for (int i = mk.dats; i < r.ndats(); i++) {
         Dat &d = r.dat(i);
-        std::vector<char> buf((size_t)d.size[0] * d.size[1] * d.size[2] * d.elem_size);
+        std::vector<char> buf(r.dat_data_bytes(i));  // the rank's owned part when partitioned
         r.dat_fetch_data(i, buf.data(), buf.size());
         std::string path = std::string(dump_dir) + "/" + d.name + ".bin";
         FILE *f = fopen(path.c_str(), "wb");

@@ -2,6 +2,7 @@
 #include <time.h>
 #include "../../include/ops_b200.h"
 
+#include <cstddef>
 #include <cstring>
 #include <string>
 
@@ -240,6 +241,7 @@ int ops_b200_set_option(const char *name, int value) {
     if (n == "graphs") rt().set_graphs(value);
     else if (n == "fusion") rt().set_fusion(value);
     else if (n == "tiling") rt().set_tiling(value);
+    else if (n == "lists") rt().set_lists(value);
     else throw opsb::Error(opsb::E_ARG, "unknown option " + n);
     return 0;
   });
@@ -262,6 +264,154 @@ int ops_b200_fusion_stats(long long *chains, long long *loops, double *fused_byt
     if (loops) *loops = s.loops;
     if (fused_bytes) *fused_bytes = s.bytes;
     if (loop_bytes) *loop_bytes = s.loop_bytes;
+    return 0;
+  });
+}
+
+// ---- decomposition across processes ----------------------------------------
+namespace {
+static_assert(sizeof(ops_b200_msg) == sizeof(opsb::Msg) && offsetof(ops_b200_msg, send) == offsetof(opsb::Msg, send) &&
+                  offsetof(ops_b200_msg, recv_bytes) == offsetof(opsb::Msg, recv_bytes),
+              "ops_b200_msg and opsb::Msg must share a layout");
+struct CCallbacks {
+  ops_b200_exchange_fn exchange = nullptr;
+  ops_b200_allgather_fn allgather = nullptr;
+  void *ctx = nullptr;
+};
+CCallbacks g_host_cb;  // one transport per process
+int host_exchange(void *c, const opsb::Msg *m, int n) {
+  const CCallbacks *cb = static_cast<const CCallbacks *>(c);
+  return cb->exchange(cb->ctx, reinterpret_cast<const ops_b200_msg *>(m), n);
+}
+int host_allgather(void *c, const void *send, size_t bytes, void *recv) {
+  const CCallbacks *cb = static_cast<const CCallbacks *>(c);
+  return cb->allgather(cb->ctx, send, bytes, recv);
+}
+}  // namespace
+
+int ops_b200_set_transport_host(int nranks, int rank, ops_b200_exchange_fn exchange, ops_b200_allgather_fn allgather,
+                                void *ctx) {
+  return guarded([&] {
+    if (!exchange || !allgather) throw opsb::Error(opsb::E_ARG, "ops_b200_set_transport_host: callbacks required");
+    opsb::Runtime &r = opsb::Runtime::get();
+    g_host_cb.exchange = exchange;
+    g_host_cb.allgather = allgather;
+    g_host_cb.ctx = ctx;
+    opsb::HostCallbacks hc;
+    hc.exchange = host_exchange;
+    hc.allgather = host_allgather;
+    hc.ctx = &g_host_cb;
+    r.set_transport(opsb::make_host_transport(nranks, rank, hc));
+    return 0;
+  });
+}
+
+int ops_b200_nccl_unique_id(void *id128) {
+  return guarded([&] {
+    if (!id128) throw opsb::Error(opsb::E_ARG, "ops_b200_nccl_unique_id: NULL buffer");
+    opsb::nccl_unique_id(id128);
+    return 0;
+  });
+}
+
+int ops_b200_set_transport_nccl(const void *id128, int nranks, int rank) {
+  return guarded([&] {
+    opsb::Runtime &r = rt();
+    OPSB_CUDA(cudaSetDevice(r.device()));
+    r.set_transport(opsb::make_nccl_transport(id128, nranks, rank));
+    return 0;
+  });
+}
+
+int ops_b200_partition(const char *routine) {
+  return guarded([&] {
+    // one process: nothing to split (needs no device, like the reference's
+    // single-process ops_partition)
+    if (opsb::Runtime::get().nranks() <= 1) return 0;
+    rt().partition(routine ? routine : "");
+    return 0;
+  });
+}
+
+int ops_b200_rank_info(int *rank, int *nranks, long long *exchanges) {
+  return guarded([&] {
+    opsb::Runtime &r = opsb::Runtime::get();
+    if (rank) *rank = r.rank();
+    if (nranks) *nranks = r.nranks();
+    if (exchanges) *exchanges = r.exchanges();
+    return 0;
+  });
+}
+
+int ops_b200_block_slab(int block, int *split_dim, int *extent, int *lo, int *hi, int *halo) {
+  return guarded([&] {
+    opsb::Runtime &r = rt();
+    r.block(block);
+    const opsb::Slab &s = r.slab(block);
+    if (split_dim) *split_dim = s.dim;
+    if (extent) *extent = s.extent;
+    if (lo) *lo = s.lo;
+    if (hi) *hi = s.hi;
+    if (halo) *halo = s.halo;
+    return 0;
+  });
+}
+
+int ops_b200_slab_window(int extent, int nranks, int rank, int halo, int gstart, int gend, int *lo, int *hi,
+                         int *own_lo, int *own_hi, int *win_lo, int *win_hi) {
+  return guarded([&] {
+    if (nranks < 1 || rank < 0 || rank >= nranks || extent < 0 || halo < 0 || gend < gstart)
+      throw opsb::Error(opsb::E_ARG, "ops_b200_slab_window: bad arguments");
+    opsb::Slab s;
+    s.dim = 0;
+    s.extent = extent;
+    s.halo = halo;
+    s.first = rank == 0;
+    s.last = rank == nranks - 1;
+    opsb::slab_bounds(extent, nranks, rank, &s.lo, &s.hi);
+    int a, b, c, d;
+    opsb::slab_window(s, gstart, gend, &a, &b, &c, &d);
+    if (lo) *lo = s.lo;
+    if (hi) *hi = s.hi;
+    if (own_lo) *own_lo = a;
+    if (own_hi) *own_hi = b;
+    if (win_lo) *win_lo = c;
+    if (win_hi) *win_hi = d;
+    return 0;
+  });
+}
+
+int ops_b200_transport_selftest(void) {
+  return guarded([&] {
+    opsb::Transport *t = opsb::Runtime::get().transport();
+    if (!t || t->device()) throw opsb::Error(opsb::E_STATE, "transport self-test: no host transport set");
+    const int N = t->nranks(), R = t->rank();
+    constexpr int kN = 16;
+    std::vector<double> out(2 * kN), in(2 * kN, -1.0);
+    std::vector<opsb::Msg> msgs;
+    for (int side = 0; side < 2; side++) {
+      const int peer = side == 0 ? R - 1 : R + 1;
+      if (peer < 0 || peer >= N) continue;
+      for (int i = 0; i < kN; i++) out[side * kN + i] = R * 1000.0 + peer * 10.0 + i;
+      opsb::Msg m;
+      m.peer = peer;
+      m.send = &out[side * kN];
+      m.send_bytes = kN * sizeof(double);
+      m.recv = &in[side * kN];
+      m.recv_bytes = kN * sizeof(double);
+      msgs.push_back(m);
+    }
+    t->exchange(msgs.data(), (int)msgs.size(), nullptr);
+    for (const opsb::Msg &m : msgs) {
+      const double *v = static_cast<const double *>(m.recv);
+      for (int i = 0; i < kN; i++)
+        if (v[i] != m.peer * 1000.0 + R * 10.0 + i)
+          throw opsb::Error(opsb::E_STATE, "transport self-test: wrong data from rank " + std::to_string(m.peer));
+    }
+    std::vector<int> all(N, -1);
+    t->allgather(&R, sizeof(int), all.data(), nullptr);
+    for (int q = 0; q < N; q++)
+      if (all[q] != q) throw opsb::Error(opsb::E_STATE, "transport self-test: allgather out of rank order");
     return 0;
   });
 }

@@ -90,8 +90,8 @@ PlanItem Runtime::prepare_swap_outside(const Desc &d) {
   int elo[3], ehi[3], rlo[3], rhi[3];
   for (int i = 0; i < 3; i++) {
     if (i < nd) {
-      elo[i] = A.d_m[i] - A.base[i];
-      ehi[i] = A.size[i] + A.d_m[i] - A.base[i];
+      elo[i] = A.lo[i];  // the stored window
+      ehi[i] = A.hi[i];
       rlo[i] = std::max(d.range[2 * i], elo[i]);
       rhi[i] = std::min(d.range[2 * i + 1], ehi[i]);
     } else {
@@ -153,7 +153,8 @@ void Runtime::elide_copies(std::vector<Desc> &q) {
       continue;
     bool same_extent = true;
     for (int k = 0; k < 3; k++)
-      same_extent &= (D.size[k] == S.size[k] && D.d_m[k] == S.d_m[k] && D.base[k] == S.base[k]);
+      same_extent &= (D.size[k] == S.size[k] && D.d_m[k] == S.d_m[k] && D.base[k] == S.base[k] &&
+                      D.lo[k] == S.lo[k] && D.hi[k] == S.hi[k]);
     if (!same_extent) continue;
     // Earlier loops of this flush must not see the renamed storage.
     bool earlier = false;

@@ -233,8 +233,7 @@ class FusionPlanner {
   }
 
   B2 alloc_box(const Dat &d) const {
-    const int x0 = d.base[0] + d.d_m[0], y0 = d.base[1] + d.d_m[1];
-    return {x0, x0 + d.size[0], y0, y0 + d.size[1]};
+    return {d.lo[0], d.hi[0], d.lo[1], d.hi[1]};
   }
 
   // Steps 1-4 of the analysis for q[first, first+n).

@@ -121,7 +121,7 @@ int Runtime::decl_halo(int from, int to, const int *iter, const int *from_base, 
     for (int i = 0; i < dims; i++) {
       const int n = h.iter[std::abs(dir[i]) - 1];
       if (n == 0) continue;
-      const int lo = d.base[i] + d.d_m[i], hi = lo + d.size[i];
+      const int lo = d.lo[i], hi = d.hi[i];
       HALO_REQUIRE(base[i] >= lo && base[i] + n <= hi, E_ARG,
               "ops_decl_halo: the box on dat " + d.name + " leaves its allocation in dimension " + std::to_string(i));
     }
@@ -153,6 +153,8 @@ void Runtime::halo_transfer(int group) {
     const Dat &f = dat(h.from);
     const Dat &t = dat(h.to);
     HALO_REQUIRE(f.locked == 0 && t.locked == 0, E_STATE, "ops_halo_transfer on a dat whose raw pointer is held");
+    HALO_REQUIRE(f.split < 0 && t.split < 0, E_UNSUPPORTED,
+                 "ops_halo_transfer between dats partitioned across ranks is not supported");
     HaloDev d;
     memset(&d, 0, sizeof(d));
     d.src = f.origin_ptr();

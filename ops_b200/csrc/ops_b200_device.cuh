@@ -449,6 +449,51 @@ __global__ void __launch_bounds__(256, LoopMinBlocks<K>::value) exec_loop(const 
   if (threadIdx.x == 0 && threadIdx.y == 0) *lp.red_counter = 0u;
 }
 
+// Several queued loops of one kernel, each over its own block or range (the
+// uneven domains of a multi-block application), in one launch: item i owns
+// the CTAs [first, first + gx * gy) of the linear grid and runs them as
+// exec_loop's (gx, gy) grid would. Loops with reductions are not batched.
+struct ListItem {
+  int gx, gy;
+  long long first;
+};
+
+template <class K>
+__global__ void __launch_bounds__(256, LoopMinBlocks<K>::value)
+    exec_loop_list(const LoopParams *__restrict__ items, const ListItem *__restrict__ grids, int nitems) {
+  using E = Exec<K, decltype(&K::operator())>;
+  const long long b = blockIdx.x;
+  int lo = 0, hi = nitems - 1;  // last item whose first CTA is <= b
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (grids[mid].first <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const LoopParams &lp = items[lo];
+  const ListItem g = grids[lo];
+  const int local = (int)(b - g.first);
+  const int bx = local % g.gx, by = local / g.gx;
+  typename E::Tup t;
+  E::init_all(t, lp, typename E::Seq{});
+  const K k{};
+  const int x = lp.start[0] + bx * blockDim.x + threadIdx.x;
+  const int ny = lp.end[1] - lp.start[1];
+  const int nz = lp.end[2] - lp.start[2];
+  const long long nrows = (long long)ny * nz;
+  if (x >= lp.end[0]) return;
+  const int ystep = g.gy * blockDim.y;
+  if (nz == 1) {
+    for (int y = lp.start[1] + by * blockDim.y + threadIdx.y; y < lp.end[1]; y += ystep)
+      E::call(k, t, lp, x, y, lp.start[2], typename E::Seq{});
+  } else {
+    for (long long r = (long long)by * blockDim.y + threadIdx.y; r < nrows; r += ystep) {
+      const int y = lp.start[1] + (int)(r % ny);
+      const int z = lp.start[2] + (int)(r / ny);
+      E::call(k, t, lp, x, y, z, typename E::Seq{});
+    }
+  }
+}
+
 // Host-side description of a kernel's parameter list, used to validate args
 // at enqueue time: 'A' accessor, 'R' reduction (ndim = width), 'I' index,
 // 'p' non-const pointer, 'c' const pointer; elem is the element size in bytes.

@@ -95,6 +95,9 @@ Runtime::~Runtime() {
   if (red_scratch_) cudaFree(red_scratch_);
   if (red_counters_) cudaFree(red_counters_);
   if (red_host_) cudaFreeHost(red_host_);
+  if (stage_h_) cudaFreeHost(stage_h_);
+  for (auto &kv : list_cache_) cudaFree(kv.second);
+  transport_.reset();
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -125,6 +128,8 @@ void Runtime::init(int device, int diags) {
   if (f) fusion_on_ = atoi(f);
   const char *t = getenv("OPS_B200_TILING");
   if (t) tiling_on_ = atoi(t);
+  const char *l = getenv("OPS_B200_LISTS");
+  if (l) lists_on_ = atoi(l);
   inited_ = true;
 }
 
@@ -211,6 +216,10 @@ int Runtime::decl_dat(int blk, int dim, const int *size, const int *base, const 
   d->origin = d->pad_front + (long long)(-d->base[0] - d->d_m[0]) + (long long)(-d->base[1] - d->d_m[1]) * d->pitch +
               (long long)(-d->base[2] - d->d_m[2]) * d->plane;
   d->bytes = (size_t)d->plane * d->size[2] * e;
+  for (int i = 0; i < 3; i++) {
+    d->lo[i] = d->own_lo[i] = d->base[i] + d->d_m[i];
+    d->hi[i] = d->own_hi[i] = d->lo[i] + d->size[i];
+  }
   d->data_d = alloc_dat_storage(d->bytes);
   OPSB_CUDA(cudaMemsetAsync(d->data_d, 0, d->bytes, stream_));
   int idx = d->index;
@@ -220,6 +229,8 @@ int Runtime::decl_dat(int blk, int dim, const int *size, const int *base, const 
     dat_set_data(idx, data, (size_t)dd.size[0] * dd.size[1] * dd.size[2] * dd.elem_size);
   }
   OPSB_CUDA(cudaStreamSynchronize(stream_));
+  // a dat declared on a block already partitioned gets its slab at once
+  if (blk < (int)slabs_.size()) window_dat(*dats_[idx]);
   return idx;
 }
 
@@ -326,6 +337,7 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
   d.args.assign(args, args + nargs);
   d.red_first.assign(nargs, 0);
   d.gbl_off.assign(nargs, 0);
+  clip_loop(d);  // the rank's slab of the range on a partitioned block
   int nred = 0;
   for (int i = 0; i < nargs; i++) {
     Arg &a = d.args[i];
@@ -373,11 +385,13 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
         throw Error(E_ARG, "unknown arg kind");
     }
   }
+  exchange_for_loop(d);  // neighbours' rows the loop reads (partitioned blocks)
   LoopRecord rec;
   if (redundant(d, rec)) {
     loops_skipped_++;
     return;
   }
+  mark_written(d);
   queue_.push_back(std::move(d));
   qrec_.push_back(std::move(rec));
   loops_enqueued_++;
@@ -386,7 +400,8 @@ void Runtime::par_loop(const LoopInfo *loop, const char *name, int blk, int dim,
 
 // Every point a loop argument can touch, the range widened by its stencil's
 // offsets along the dimensions the stencil walks, must lie in the dat's
-// allocation [base + d_m, base + d_m + size): the reference leaves this to
+// stored window [lo, hi) (the whole extent [base + d_m, base + d_m + size)
+// unless the dat is partitioned across ranks): the reference leaves this to
 // the application, a device kernel here would read or write outside its
 // buffer. Folded (stride 0) dimensions address index 0.
 void Runtime::check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) const {
@@ -416,7 +431,7 @@ void Runtime::check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) co
     } else {
       lo = hi = 0;
     }
-    const long long first = (long long)dt.base[k] + dt.d_m[k], last = first + dt.size[k] - 1;
+    const long long first = dt.lo[k], last = (long long)dt.hi[k] - 1;
     OPSB_REQUIRE(lo >= first && hi <= last, E_ARG,
             "loop " + d.loop->kernel + ": dat " + dt.name + " accessed at [" + std::to_string(lo) + ", " +
                 std::to_string(hi) + "] in dimension " + std::to_string(k) + ", allocated [" +
@@ -693,7 +708,7 @@ void Runtime::plan_plain(std::vector<Desc> &q, size_t from, size_t to, std::vect
   size_t i = from;
   while (i < to) {
     if (q[i].loop->internal) {
-      out.push_back(prepare_swap_outside(q[i]));
+      out.push_back(q[i].loop->internal == 2 ? prepare_exchange(q[i]) : prepare_swap_outside(q[i]));
       i++;
       continue;
     }
@@ -710,6 +725,13 @@ void Runtime::plan_plain(std::vector<Desc> &q, size_t from, size_t to, std::vect
         }
       }
       if (done) continue;
+      if (lists_on_) {
+        const size_t n = list_run(q, i, to);
+        if (n >= 2 && prepare_list(q, i, n, out)) {
+          i += n;
+          continue;
+        }
+      }
     }
     const Desc &d = q[i];
     LoopParams lp;
@@ -734,6 +756,102 @@ void Runtime::plan_plain(std::vector<Desc> &q, size_t from, size_t to, std::vect
     out.push_back(std::move(it));
     i++;
   }
+}
+
+// Consecutive loops of one kernel that are independent of one another (no
+// loop reads or writes a dat another one writes) and carry no reduction: the
+// steps of a multi-block application over its blocks, for one. Returns how
+// many, from q[i].
+size_t Runtime::list_run(const std::vector<Desc> &q, size_t i, size_t to) const {
+  const LoopInfo *L = q[i].loop;
+  if (L->internal || !L->launch_list) return 0;
+  auto eligible = [&](const Desc &d) {
+    if (d.loop != L) return false;
+    for (int k = 0; k < 3; k++)
+      if (d.range[2 * k + 1] <= d.range[2 * k]) return false;
+    for (const Arg &a : d.args)
+      if (a.kind == ARG_REDUCE) return false;
+    return true;
+  };
+  std::vector<int> written, touched;
+  auto has = [](const std::vector<int> &v, int x) { return std::find(v.begin(), v.end(), x) != v.end(); };
+  size_t j = i;
+  while (j < to && eligible(q[j])) {
+    bool ok = true;
+    for (const Arg &a : q[j].args)
+      if (a.kind == ARG_DAT && (has(written, a.dat) || (a.acc != ACC_READ && has(touched, a.dat)))) ok = false;
+    if (!ok) break;
+    for (const Arg &a : q[j].args)
+      if (a.kind == ARG_DAT) {
+        touched.push_back(a.dat);
+        if (a.acc != ACC_READ) written.push_back(a.dat);
+      }
+    j++;
+  }
+  return j - i;
+}
+
+// The work list of q[i, i+n): each loop's parameters and CTA grid (sized as
+// launch_shape sizes a single loop's), uploaded now, before any capture, and
+// kept by content (a captured graph keeps pointing at them).
+bool Runtime::prepare_list(std::vector<Desc> &q, size_t i, size_t n, std::vector<PlanItem> &out) {
+  std::vector<LoopParams> lps(n);
+  std::vector<ListItem> grids(n);
+  int bx = 32;
+  for (size_t k = 0; k < n; k++) {
+    const int nx = q[i + k].range[1] - q[i + k].range[0];
+    bx = std::max(bx, nx >= 128 ? 128 : (nx >= 64 ? 64 : 32));
+  }
+  const int by = 256 / bx;
+  long long total = 0;
+  double bytes = 0.0;
+  for (size_t k = 0; k < n; k++) {
+    const Desc &d = q[i + k];
+    int nred = 0;
+    build_params(d, lps[k], &nred);
+    const long long nx = (long long)d.range[1] - d.range[0];
+    const long long nrows = (long long)(d.range[3] - d.range[2]) * (d.range[5] - d.range[4]);
+    const long long gx = (nx + bx - 1) / bx;
+    long long gy = std::min((nrows + by - 1) / by, std::max(1LL, 148LL * 16 / gx));
+    gy = std::max(1LL, std::min(gy, 65535LL));
+    grids[k] = {(int)gx, (int)gy, total};
+    total += gx * gy;
+    if (timing_on_) bytes += alg_bytes(d);
+  }
+  if (total > 0x7fffffffLL) return false;
+  const size_t pb = n * sizeof(LoopParams), gb = n * sizeof(ListItem);
+  uint64_t h = 0xCBF29CE484222325ULL;
+  for (const unsigned char *c = (const unsigned char *)lps.data(), *e = c + pb; c < e; c++) h = (h ^ *c) * 0x100000001B3ULL;
+  for (const unsigned char *c = (const unsigned char *)grids.data(), *e = c + gb; c < e; c++)
+    h = (h ^ *c) * 0x100000001B3ULL;
+  h ^= n;
+  char *dev = nullptr;
+  auto it = list_cache_.find(h);
+  if (it != list_cache_.end()) {
+    dev = it->second;
+  } else {
+    OPSB_CUDA(cudaMalloc(&dev, pb + gb));
+    OPSB_CUDA(cudaMemcpyAsync(dev, lps.data(), pb, cudaMemcpyHostToDevice, stream_));
+    OPSB_CUDA(cudaMemcpyAsync(dev + pb, grids.data(), gb, cudaMemcpyHostToDevice, stream_));
+    list_cache_[h] = dev;
+  }
+  PlanItem p;
+  p.name = q[i].loop->kernel;
+  p.kernels = 1;
+  p.bytes = bytes;
+  auto launch = q[i].loop->launch_list;
+  const LoopParams *dl = reinterpret_cast<const LoopParams *>(dev);
+  const ListItem *dg = reinterpret_cast<const ListItem *>(dev + pb);
+  const int cnt = (int)n;
+  const dim3 block(bx, by, 1);
+  p.run = [launch, dl, dg, cnt, total, block](cudaStream_t s) {
+    launch(dl, dg, cnt, total, block, s);
+    OPSB_CUDA(cudaGetLastError());
+  };
+  out.push_back(std::move(p));
+  list_loops_ += (long long)n;
+  list_launches_++;
+  return true;
 }
 
 void Runtime::launch_plan(std::vector<PlanItem> &items) {
@@ -876,33 +994,64 @@ void Runtime::reduction_result(int handle, void *out) {
     red_dirty_ = false;
   }
   memcpy(out, red_host_ + (r.slot_d - red_arena_), r.size);
+  if (partitioned_ && nranks() > 1) combine_reduction(r, out);
   r.initialized = 0;  // ops_reduction_result_char resets the handle (ops_lib_core.cpp:1143)
 }
 
 // ---------------------------------------------------------------------------
-// Data access.
+// Data access. A partitioned dat's data are its owned part (the extents
+// ops_dat_get_extents reports, as the reference's MPI backend does,
+// ops/c/src/mpi/ops_mpi_rt_support.cpp:2216-2225); otherwise the whole dat.
 // ---------------------------------------------------------------------------
+namespace {
+// The stored x rows (pitch elements each, in storage order) that hold a
+// dat's owned part: the first one and how many.
+void owned_rows(const Dat &d, size_t *first, size_t *n) {
+  const size_t ny = (size_t)(d.hi[1] - d.lo[1]), nz = (size_t)(d.hi[2] - d.lo[2]);
+  if (d.split == 2) {
+    *first = (size_t)(d.own_lo[2] - d.lo[2]) * ny;
+    *n = (size_t)(d.own_hi[2] - d.own_lo[2]) * ny;
+  } else if (d.split == 1) {  // 2D blocks: nz == 1
+    *first = (size_t)(d.own_lo[1] - d.lo[1]);
+    *n = (size_t)(d.own_hi[1] - d.own_lo[1]) * nz;
+  } else {
+    *first = 0;
+    *n = ny * nz;
+  }
+}
+}  // namespace
+
+size_t Runtime::dat_data_bytes(int di) {
+  Dat &d = dat(di);
+  size_t first, n;
+  owned_rows(d, &first, &n);
+  return (size_t)d.size[0] * d.elem_size * n;
+}
+
 void Runtime::dat_set_data(int di, const void *host, size_t bytes) {
   execute();
   Dat &d = dat(di);
   OPSB_REQUIRE(d.locked == 0, E_STATE, "ops_dat_set_data on a dat whose raw pointer is held");
   size_t row = (size_t)d.size[0] * d.elem_size;
-  size_t rows = (size_t)d.size[1] * d.size[2];
+  size_t first, rows;
+  owned_rows(d, &first, &rows);
   OPSB_REQUIRE(bytes == row * rows, E_ARG, "ops_dat_set_data: buffer size does not match the dat extent");
-  OPSB_CUDA(cudaMemcpy2DAsync(d.data_d + (size_t)d.pad_front * d.elem_size, (size_t)d.pitch * d.elem_size, host, row,
-                              row, rows, cudaMemcpyHostToDevice, stream_));
+  OPSB_CUDA(cudaMemcpy2DAsync(d.data_d + ((size_t)d.pad_front + first * d.pitch) * d.elem_size,
+                              (size_t)d.pitch * d.elem_size, host, row, row, rows, cudaMemcpyHostToDevice, stream_));
   OPSB_CUDA(cudaStreamSynchronize(stream_));
   d.host.clear();
+  if (d.split >= 0) d.valid = 0;  // the neighbours' copies of the owned rows are stale
 }
 
 void Runtime::dat_fetch_data(int di, void *host, size_t bytes) {
   execute();
   Dat &d = dat(di);
   size_t row = (size_t)d.size[0] * d.elem_size;
-  size_t rows = (size_t)d.size[1] * d.size[2];
+  size_t first, rows;
+  owned_rows(d, &first, &rows);
   OPSB_REQUIRE(bytes == row * rows, E_ARG, "ops_dat_fetch_data: buffer size does not match the dat extent");
-  OPSB_CUDA(cudaMemcpy2DAsync(host, row, d.data_d + (size_t)d.pad_front * d.elem_size, (size_t)d.pitch * d.elem_size,
-                              row, rows, cudaMemcpyDeviceToHost, stream_));
+  OPSB_CUDA(cudaMemcpy2DAsync(host, row, d.data_d + ((size_t)d.pad_front + first * d.pitch) * d.elem_size,
+                              (size_t)d.pitch * d.elem_size, row, rows, cudaMemcpyDeviceToHost, stream_));
   OPSB_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -910,8 +1059,8 @@ void Runtime::dat_get_extents(int di, int *disp, int *size) {
   Dat &d = dat(di);
   int nd = blocks_[d.block].dims;
   for (int i = 0; i < nd; i++) {
-    if (disp) disp[i] = 0;
-    if (size) size[i] = d.size[i];
+    if (disp) disp[i] = d.own_lo[i] - (d.base[i] + d.d_m[i]);
+    if (size) size[i] = d.own_hi[i] - d.own_lo[i];
   }
 }
 
@@ -922,8 +1071,8 @@ char *Runtime::dat_get_raw_pointer(int di, int memspace, int *stride_elems) {
   OPSB_REQUIRE(d.locked == 0, E_STATE, "raw pointer already held for dat " + d.name);
   if (stride_elems) {
     stride_elems[0] = (int)d.pitch;
-    stride_elems[1] = d.size[1];
-    stride_elems[2] = d.size[2];
+    stride_elems[1] = d.hi[1] - d.lo[1];
+    stride_elems[2] = d.hi[2] - d.lo[2];
   }
   if (memspace == 2) {
     OPSB_CUDA(cudaStreamSynchronize(stream_));
@@ -944,6 +1093,7 @@ void Runtime::dat_release_raw_data(int di, int acc) {
     OPSB_CUDA(cudaMemcpyAsync(d.data_d, d.host.data(), d.bytes, cudaMemcpyHostToDevice, stream_));
     OPSB_CUDA(cudaStreamSynchronize(stream_));
   }
+  if (acc != ACC_READ && d.split >= 0) d.valid = 0;
   d.locked = 0;
 }
 
@@ -965,6 +1115,8 @@ void Runtime::release_to(const Mark &m) {
     dats_.pop_back();
   }
   release_fusion_plans();
+  if (slabs_.size() > m.blocks) slabs_.resize(m.blocks);
+  partitioned_ = !slabs_.empty();
   while (reductions_.size() > m.reductions) {
     reductions_.pop_back();
   }

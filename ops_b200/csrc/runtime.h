@@ -27,6 +27,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "decomp.h"
 #include "ops_b200_device.cuh"
 
 namespace opsb {
@@ -66,6 +67,14 @@ struct Dat {
   std::string type, name;
   int locked = 0;           // 0 free, 1 host raw pointer out, 2 device raw pointer out
   std::vector<char> host;   // host mirror for host raw pointers
+  // The stored window [lo, hi) and the owned part [own_lo, own_hi) of each
+  // dimension, in logical indices: the whole extent [base + d_m, base + d_m
+  // + size) unless the dat is partitioned across ranks (decomp.h), when the
+  // split dimension keeps the rank's slab plus its neighbours' halo rows.
+  int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  int own_lo[3] = {0, 0, 0}, own_hi[3] = {1, 1, 1};
+  int split = -1;           // dimension split across ranks (-1: whole)
+  int valid = 0;            // halo rows holding the neighbours' current values
   char *origin_ptr() const { return data_d + origin * elem_size; }
 };
 
@@ -104,6 +113,9 @@ struct LoopInfo {
   int internal = 0;         // runtime-internal item (not launched through exec_loop)
   int mgrid_ok = 0;         // the kernel maps multigrid (restrict/prolong) stencils
   void (*launch)(const LoopParams &, dim3, dim3, cudaStream_t) = nullptr;
+  // several loops of this kernel in one launch (exec_loop_list); null for
+  // kernels with their own launch
+  void (*launch_list)(const LoopParams *, const ListItem *, int, long long, dim3, cudaStream_t) = nullptr;
 };
 
 // A queued loop (ops_kernel_descriptor, ops/c/include/ops_internal2.h:141-157).
@@ -211,6 +223,7 @@ class Runtime {
   void dat_set_data(int dat, const void *host, size_t bytes);
   void dat_fetch_data(int dat, void *host, size_t bytes);
   void dat_get_extents(int dat, int *disp, int *size);
+  size_t dat_data_bytes(int dat);  // bytes of dat_set_data / dat_fetch_data
   char *dat_get_raw_pointer(int dat, int memspace, int *stride_elems);
   void dat_release_raw_data(int dat, int acc);
   void dat_swap(int a, int b);  // exchange device storage of two same-shape dats
@@ -253,6 +266,9 @@ class Runtime {
   void timed_launch_end();
   void set_fusion(int on) { fusion_on_ = on; }
   void set_tiling(int on) { tiling_on_ = on; }
+  void set_lists(int on) { lists_on_ = on; }
+  long long list_plans() const { return list_launches_; }
+  long long list_loops() const { return list_loops_; }
   long long loops_skipped() const { return loops_skipped_; }
   int fusion_enabled() const { return fusion_on_; }
   int diags() const { return diags_; }
@@ -285,15 +301,37 @@ class Runtime {
   const FusionStats &fusion_stats() const { return fstats_; }
   void reset_fusion_stats() { fstats_ = FusionStats(); }
 
+  // Decomposition across processes (decomp.cpp). The transport is set
+  // before ops_partition; without one (or with one rank) partition is a
+  // no-op, as ops_partition is in the reference's single-process backends.
+  void set_transport(std::unique_ptr<Transport> t);
+  void partition(const char *routine);
+  int nranks() const;
+  int rank() const;
+  bool partitioned() const { return partitioned_; }
+  const Slab &slab(int block) const;
+  long long exchanges() const { return exchanges_; }
+  Transport *transport() const { return transport_.get(); }
+  int device() const { return device_; }
+
  private:
   friend class FusionPlanner;
   Runtime() = default;
   void run_queue(std::vector<Desc> &q);
   void elide_copies(std::vector<Desc> &q);
   PlanItem prepare_swap_outside(const Desc &d);
+  PlanItem prepare_exchange(const Desc &d);
+  void window_dat(Dat &d);
+  void clip_loop(Desc &d);
+  void exchange_for_loop(const Desc &d);
+  void mark_written(const Desc &d);
+  void exchange_dats(const std::vector<int> &dats);
+  void combine_reduction(const Reduction &r, void *value);
   void plan_items(std::vector<Desc> &q, std::vector<PlanItem> &out, std::vector<int> &renamed, bool &tuning);
   void launch_plan(std::vector<PlanItem> &items);
   void plan_plain(std::vector<Desc> &q, size_t from, size_t to, std::vector<PlanItem> &out);
+  size_t list_run(const std::vector<Desc> &q, size_t i, size_t to) const;
+  bool prepare_list(std::vector<Desc> &q, size_t i, size_t n, std::vector<PlanItem> &out);
   void plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &items);
   void build_fused(const std::vector<Desc> &q, FusedItem &item);
   FusionState &fusion_state();
@@ -367,6 +405,7 @@ class Runtime {
   cudaEvent_t cur_ev_ = nullptr;
   int fusion_on_ = 1;
   int tiling_on_ = 1;  // loop-chain fusion into tiled kernels (needs fusion_on_)
+  int lists_on_ = 1;   // runs of one kernel over several blocks in one launch (needs fusion_on_)
   // Redundant-loop elimination within one flush: per queued loop, the
   // version of each dat arg (read: as observed, written: as produced);
   // dat versions count the writes of the queued loops and restart at every
@@ -382,6 +421,15 @@ class Runtime {
   bool redundant(const Desc &d, LoopRecord &rec);
   void check_in_allocation(const Desc &d, const Arg &a, const Dat &dt) const;
   long long kernels_launched_ = 0, graphs_launched_ = 0, loops_enqueued_ = 0;
+  std::unique_ptr<Transport> transport_;
+  std::vector<Slab> slabs_;  // per block, after partition
+  bool partitioned_ = false;
+  char *stage_h_ = nullptr;  // pinned staging of host-transport exchanges
+  size_t stage_cap_ = 0;
+  long long exchanges_ = 0;
+  long long list_launches_ = 0;  // work lists planned (loops they cover: list_loops_)
+  long long list_loops_ = 0;
+  std::unordered_map<uint64_t, char *> list_cache_;  // device work lists by content
 };
 
 // Releases an app call's declarations (blocks, dats, stencils, reductions
@@ -460,6 +508,11 @@ template <class K>
 void launch_exec(const LoopParams &lp, dim3 g, dim3 b, cudaStream_t s) {
   exec_loop<K><<<g, b, 0, s>>>(lp);
 }
+template <class K>
+void launch_exec_list(const LoopParams *items, const ListItem *grids, int n, long long blocks, dim3 b,
+                      cudaStream_t s) {
+  exec_loop_list<K><<<(unsigned)blocks, b, 0, s>>>(items, grids, n);
+}
 
 // A kernel may bring its own launch (a specialised executor for its access
 // pattern) as `static void launch(const LoopParams &, dim3, dim3,
@@ -490,10 +543,12 @@ LoopInfo make_loop_info(const char *kernel) {
     if (li.params[i].cls == 'A') li.ndim = li.params[i].ndim;
   li.copy_dst = CopyTrait<K>::dst;
   li.copy_src = CopyTrait<K>::src;
-  if constexpr (CustomLaunch<K>::value)
+  if constexpr (CustomLaunch<K>::value) {
     li.launch = &K::launch;
-  else
+  } else {
     li.launch = &launch_exec<K>;
+    li.launch_list = &launch_exec_list<K>;
+  }
   li.mgrid_ok = LoopMgridOk<K>::value ? 1 : 0;
   return li;
 }

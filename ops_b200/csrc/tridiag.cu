@@ -569,6 +569,9 @@ static int trid_dats(int ndim, int solvedim, const int *range, int a, int b, int
     if (!range) throw Error(E_ARG, "range required");
     Dat &A = r.dat(a), &B = r.dat(b), &C = r.dat(c), &Dd = r.dat(d);
     Dat *U = u >= 0 ? &r.dat(u) : nullptr;
+    // a line solve needs its whole line on one GPU: no partitioned dats
+    if (A.split >= 0 || B.split >= 0 || C.split >= 0 || Dd.split >= 0 || (U && U->split >= 0))
+      throw Error(E_UNSUPPORTED, "Tridsolver: dats partitioned across ranks are not supported");
     for (int i = 0; i < 3; i++)
       if (A.size[i] != B.size[i] || B.size[i] != C.size[i] || C.size[i] != Dd.size[i] ||
           (U && U->size[i] != A.size[i]))

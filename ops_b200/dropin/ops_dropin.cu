@@ -721,9 +721,12 @@ void ops_timers(double *cpu, double *et) {
   ops_timers_core(cpu, et);
 }
 
-int ops_is_root() { return 1; }
+int ops_is_root() { return opsb::Runtime::get().rank() == 0; }
 
-void ops_partition(const char *routine) { (void)routine; }
+// The runtime partitions across the ranks of its transport (none is set in
+// a drop-in binary, so this is the single-process no-op of the reference's
+// sequential and CUDA backends).
+void ops_partition(const char *routine) { opsb::Runtime::get().partition(routine); }
 
 // With diagnostics above 1 (ops_init's diags_level) the runtime times every
 // kernel with CUDA events; the table lists them.

@@ -234,7 +234,11 @@ def ops_dat_set_data(dat, data):
 
 
 def ops_dat_fetch_data(dat):
-    out = np.zeros(dat.extent_shape(), dtype=dat.dtype)
+    """The dat's data: the full extent, or the rank's owned part of a block
+    partitioned across ranks (ops_dat_get_extents)."""
+    _, size = ops_dat_get_extents(dat)
+    shp = list(reversed(size)) + ([dat.dim] if dat.dim > 1 else [])
+    out = np.zeros(tuple(shp), dtype=dat.dtype)
     check(lib().ops_b200_dat_fetch_data(dat.index, out.ctypes.data, out.nbytes))
     return out
 
@@ -342,9 +346,12 @@ def ops_fprintf(stream, fmt, *args):
 
 
 def ops_partition(routine=None, opts=None):
-    """ops_partition / ops_partition_opts (ops_dummy_singlenode.cpp:892-899):
-    nothing to partition with one process on one GPU."""
-    return None
+    """ops_partition / ops_partition_opts: splits the blocks declared so far
+    across the ranks of the transport set by ops_b200.dist (slabs along each
+    block's outermost dimension); with one process it does nothing, as in the
+    reference's single-process backends (ops_dummy_singlenode.cpp:892-899).
+    `opts` (the reference's decomposition hints) is accepted and ignored."""
+    check(lib().ops_b200_partition((routine or "").encode()))
 
 
 def ops_timing_output(stream=None):
