@@ -31,13 +31,13 @@ def _run(lists):
     O.reset_counters()
     for i, (nx, ny) in enumerate(SHAPES):
         O.ops_par_loop("mgrid/mgrid_populate_kernel_1", "populate", blocks[i], 2, [0, nx, 0, ny],
-                       O.ops_arg_dat(a[i], 1, s00, "double", O.WRITE), O.ops_arg_idx())
+                       O.ops_arg_dat(a[i], 1, s00, "double", O.OPS_WRITE), O.ops_arg_idx())
     O.ops_execute()
     k_populate = O.counters()["kernels"]
     O.reset_counters()
     for i, (nx, ny) in enumerate(SHAPES):
         O.ops_par_loop("laplace2d/copy", "copy", blocks[i], 2, [0, nx, 0, ny],
-                       O.ops_arg_dat(b[i], 1, s00, "double", O.WRITE), O.ops_arg_dat(a[i], 1, s00, "double", O.READ))
+                       O.ops_arg_dat(b[i], 1, s00, "double", O.OPS_WRITE), O.ops_arg_dat(a[i], 1, s00, "double", O.OPS_READ))
     O.ops_execute()
     k_copy = O.counters()["kernels"]
     out = [(O.ops_dat_fetch_data(a[i]), O.ops_dat_fetch_data(b[i])) for i in range(len(SHAPES))]
@@ -74,10 +74,10 @@ def test_dependent_loops_are_not_batched(gpu_runtime):
     c = O.ops_decl_dat(blk, 1, [n, n], [0, 0], [-1, -1], [1, 1], None, "double", "dep_c")
     O.ops_execute()
     O.reset_counters()
-    O.ops_par_loop("laplace2d/copy", "copy", blk, 2, [0, n, 0, n], O.ops_arg_dat(b, 1, s00, "double", O.WRITE),
-                   O.ops_arg_dat(a, 1, s00, "double", O.READ))
-    O.ops_par_loop("laplace2d/copy", "copy", blk, 2, [0, n, 0, n], O.ops_arg_dat(c, 1, s00, "double", O.WRITE),
-                   O.ops_arg_dat(b, 1, s00, "double", O.READ))
+    O.ops_par_loop("laplace2d/copy", "copy", blk, 2, [0, n, 0, n], O.ops_arg_dat(b, 1, s00, "double", O.OPS_WRITE),
+                   O.ops_arg_dat(a, 1, s00, "double", O.OPS_READ))
+    O.ops_par_loop("laplace2d/copy", "copy", blk, 2, [0, n, 0, n], O.ops_arg_dat(c, 1, s00, "double", O.OPS_WRITE),
+                   O.ops_arg_dat(b, 1, s00, "double", O.OPS_READ))
     O.ops_execute()
     assert O.counters()["kernels"] == 2
     C = O.ops_dat_fetch_data(c)
