@@ -167,7 +167,12 @@ int ops_b200_dat_release_raw_data(int dat, int acc);
  * reference's lazy tiling, ops/c/src/core/ops_lazy.cpp:380-1173) and
  * "lists" (consecutive independent loops of one kernel, e.g. over the
  * blocks of a multi-block application, launched as one kernel over a work
- * list of their uneven domains, default 1, needs "fusion"). */
+ * list of their uneven domains, default 1, needs "fusion").
+ * "tile_candidate": -1 (default) lets the autotuner pick each fused chain's
+ * tile shape and staging (or no fusion) by timing; 0..9 runs every chain
+ * that fits with that one candidate (tile shape index / 2 of 64x8, 128x8,
+ * 64x16, 128x16, 32x16; odd: read-only dats staged in shared memory), for
+ * parity tests and profiling of the fused kernels. */
 int ops_b200_set_option(const char *name, int value);
 /* Counters since the last reset: kernels launched by this library, CUDA
  * graphs launched, loops queued. */

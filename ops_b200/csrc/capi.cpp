@@ -242,6 +242,7 @@ int ops_b200_set_option(const char *name, int value) {
     else if (n == "fusion") rt().set_fusion(value);
     else if (n == "tiling") rt().set_tiling(value);
     else if (n == "lists") rt().set_lists(value);
+    else if (n == "tile_candidate") rt().set_tile_candidate(value);
     else throw opsb::Error(opsb::E_ARG, "unknown option " + n);
     return 0;
   });

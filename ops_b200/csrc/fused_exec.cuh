@@ -33,16 +33,23 @@ struct TileCtx {
   int cx0, cy0, cx1, cy1;
 };
 
+// Per-point work is kept free of memory the kernels' stores could alias:
+// every slot copies what it needs from the plan (global memory) into its own
+// members when a phase starts, and writes reduction partials back when it
+// ends, so a point costs only its address arithmetic and the kernel's own
+// loads and stores.
 template <class P> struct FSlot;
 
 // An accessor argument: where its point (x, y) lives is resolved once per
 // phase (a shared-memory tile, or the dat in HBM), so that a point costs
-// one multiply-add per argument.
+// one multiply-add per argument. Views are always coherent generic loads:
+// they may point into shared-memory tiles or at data other phases write.
 template <class T>
 struct FSlot<ACC2<T>> {
   ACC2<T> acc;
   T *base;       // address of logical (0, 0) in the bound storage (may lie outside it)
-  int sx, sy, ay, coh, masked;
+  int sx, sy, ay;
+  bool masked;
   T *sink;
   __device__ __forceinline__ void init(const TileCtx &c, const FArg &a) {
     if (a.mode == M_TILE) {
@@ -51,58 +58,63 @@ struct FSlot<ACC2<T>> {
       base = reinterpret_cast<T *>(c.sm) + o;
       sx = 1;
       sy = ay = b.pitch;
-      coh = 1;
     } else {
       base = reinterpret_cast<T *>(a.ptr);
       sx = a.sx;
       sy = a.sy;
       ay = a.ay;
-      coh = a.mode == M_RW;
     }
     masked = a.mode == M_RW && a.masked;
     sink = reinterpret_cast<T *>(c.scratch + 16 + a.slot);
   }
-  __device__ __forceinline__ ACC2<T> &at(const TileCtx &, const FArg &, int x, int y, bool core) {
-    acc = (masked && !core) ? ACC2<T>(sink, 0, 1) : ACC2<T>(base + (x * sx + y * sy), ay, coh);
+  __device__ __forceinline__ ACC2<T> &at(int x, int y, bool core) {
+    acc = (masked && !core) ? ACC2<T>(sink, 0, 1) : ACC2<T>(base + (x * sx + y * sy), ay, 1);
     return acc;
   }
-  __device__ __forceinline__ void done(const TileCtx &, const FArg &, bool) {}
+  __device__ __forceinline__ void done(bool) {}
+  __device__ __forceinline__ void fini(const TileCtx &, const FArg &) {}
 };
 
 template <class T, int N>
 struct FSlot<RED<T, N>> {
   static_assert(N == 1, "fused chains take one-component reductions");
   RED<T, N> r;
-  __device__ __forceinline__ void init(const TileCtx &, const FArg &) {}
-  __device__ __forceinline__ RED<T, N> &at(const TileCtx &c, const FArg &a, int, int, bool core) {
-    r.v[0] = core ? (T)c.racc[a.red] : red_identity<T>(c.P->red[a.red].acc);
+  T part, ident;  // this thread's partial over the core's points; the identity
+  __device__ __forceinline__ void init(const TileCtx &c, const FArg &a) {
+    part = (T)c.racc[a.red];
+    ident = red_identity<T>(c.P->red[a.red].acc);
+  }
+  __device__ __forceinline__ RED<T, N> &at(int, int, bool core) {
+    r.v[0] = core ? part : ident;
     return r;
   }
-  __device__ __forceinline__ void done(const TileCtx &c, const FArg &a, bool core) {
-    if (core) c.racc[a.red] = (double)r.v[0];
+  __device__ __forceinline__ void done(bool core) {
+    if (core) part = r.v[0];
   }
+  __device__ __forceinline__ void fini(const TileCtx &c, const FArg &a) { c.racc[a.red] = (double)part; }
 };
 
 template <>
 struct FSlot<IDX> {
   IDX i;
   __device__ __forceinline__ void init(const TileCtx &, const FArg &) {}
-  __device__ __forceinline__ IDX &at(const TileCtx &, const FArg &, int x, int y, bool) {
+  __device__ __forceinline__ IDX &at(int x, int y, bool) {
     i.v[0] = x;
     i.v[1] = y;
     i.v[2] = 0;
     return i;
   }
-  __device__ __forceinline__ void done(const TileCtx &, const FArg &, bool) {}
+  __device__ __forceinline__ void done(bool) {}
+  __device__ __forceinline__ void fini(const TileCtx &, const FArg &) {}
 };
 
 template <class T>
 struct FSlot<T *> {
-  __device__ __forceinline__ void init(const TileCtx &, const FArg &) {}
-  __device__ __forceinline__ T *at(const TileCtx &, const FArg &a, int, int, bool) {
-    return reinterpret_cast<T *>(a.ptr);
-  }
-  __device__ __forceinline__ void done(const TileCtx &, const FArg &, bool) {}
+  T *p;
+  __device__ __forceinline__ void init(const TileCtx &, const FArg &a) { p = reinterpret_cast<T *>(a.ptr); }
+  __device__ __forceinline__ T *at(int, int, bool) { return p; }
+  __device__ __forceinline__ void done(bool) {}
+  __device__ __forceinline__ void fini(const TileCtx &, const FArg &) {}
 };
 
 template <class K, class Sig> struct FusedCall;
@@ -116,28 +128,41 @@ struct FusedCall<K, void (C::*)(P...) const> {
     (get_leaf<I, FSlot<std::decay_t<P>>>(t).init(c, a[I]), ...);
   }
   template <size_t... I>
-  __device__ static __forceinline__ void point(const K &k, Tup &t, const TileCtx &c, const FArg *a, int x, int y,
-                                               bool core, std::index_sequence<I...>) {
-    k(get_leaf<I, FSlot<std::decay_t<P>>>(t).at(c, a[I], x, y, core)...);
-    (get_leaf<I, FSlot<std::decay_t<P>>>(t).done(c, a[I], core), ...);
+  __device__ static __forceinline__ void fini_all(Tup &t, const TileCtx &c, const FArg *a, std::index_sequence<I...>) {
+    (get_leaf<I, FSlot<std::decay_t<P>>>(t).fini(c, a[I]), ...);
+  }
+  template <size_t... I>
+  __device__ static __forceinline__ void point(const K &k, Tup &t, int x, int y, bool core,
+                                               std::index_sequence<I...>) {
+    k(get_leaf<I, FSlot<std::decay_t<P>>>(t).at(x, y, core)...);
+    (get_leaf<I, FSlot<std::decay_t<P>>>(t).done(core), ...);
   }
 
   // All points of the loop's region in this tile; consecutive threads take
-  // consecutive x so that HBM accesses coalesce.
-  __device__ static void phase(const TileCtx &c, const FLoop &L, int rx0, int rx1, int ry0, int ry1) {
+  // consecutive x so that HBM accesses coalesce. A thread steps through the
+  // region by a fixed (dx, dy) instead of dividing its flat index per point.
+  __device__ static __forceinline__ void phase(const TileCtx &c, const FLoop &L, int rx0, int rx1, int ry0,
+                                               int ry1) {
     const K k{};
     Tup t;
     const FArg *a = c.P->A + L.arg0;
     init_all(t, c, a, Seq{});
     const int w = rx1 - rx0;
-    const int n = w * (ry1 - ry0);
-    for (int p = threadIdx.x; p < n; p += kThreads) {
-      const int yy = p / w;
-      const int x = rx0 + (p - yy * w);
-      const int y = ry0 + yy;
-      const bool core = x >= c.cx0 && x < c.cx1 && y >= c.cy0 && y < c.cy1;
-      point(k, t, c, a, x, y, core, Seq{});
+    const int cx0 = c.cx0, cx1 = c.cx1, cy0 = c.cy0, cy1 = c.cy1;
+    const int dy = kThreads / w, dx = kThreads - dy * w;
+    int y = ry0 + (int)threadIdx.x / w;
+    int x = rx0 + ((int)threadIdx.x - (y - ry0) * w);
+    for (; y < ry1;) {
+      const bool core = x >= cx0 && x < cx1 && y >= cy0 && y < cy1;
+      point(k, t, x, y, core, Seq{});
+      x += dx;
+      y += dy;
+      if (x >= rx1) {
+        x -= w;
+        y++;
+      }
     }
+    fini_all(t, c, a, Seq{});
   }
 };
 
@@ -175,17 +200,37 @@ __device__ __forceinline__ double *fused_addr(const TileCtx &c, const FArg &a, i
 __device__ inline void copy_phase(const TileCtx &c, const FLoop &L, int rx0, int rx1, int ry0, int ry1) {
   const FArg *a = c.P->A + L.arg0;
   const int w = rx1 - rx0;
-  const int n = w * (ry1 - ry0);
-  for (int p = threadIdx.x; p < n; p += kThreads) {
-    const int yy = p / w;
-    const int x = rx0 + (p - yy * w);
-    const int y = ry0 + yy;
-    const bool core = x >= c.cx0 && x < c.cx1 && y >= c.cy0 && y < c.cy1;
-    for (int f = 0; f < L.cp_n; f++) {
-      const FArg &fa = a[L.cp_arg[f]];
-      if (fa.mode != M_TILE && !core) continue;
-      const double v = *fused_addr(c, fa, x + L.cp_ox, y + L.cp_oy);
-      *fused_addr(c, fa, x, y) = L.cp_neg ? -v : v;
+  const int cx0 = c.cx0, cx1 = c.cx1, cy0 = c.cy0, cy1 = c.cy1;
+  const int ox = L.cp_ox, oy = L.cp_oy, nf = L.cp_n;
+  const bool neg = L.cp_neg != 0;
+  const int dy = kThreads / w, dx = kThreads - dy * w;
+  // one field at a time: its address arithmetic is read from the plan once
+  for (int f = 0; f < nf; f++) {
+    const FArg &fa = a[L.cp_arg[f]];
+    const bool tile = fa.mode == M_TILE;
+    double *const o = fused_addr(c, fa, 0, 0);
+    int sx = 1, sy;
+    if (tile) {
+      sy = c.P->B[fa.buf].pitch;
+    } else {
+      sx = fa.sx;
+      sy = fa.sy;
+    }
+    const int moff = ox * sx + oy * sy;
+    int y = ry0 + (int)threadIdx.x / w;
+    int x = rx0 + ((int)threadIdx.x - (y - ry0) * w);
+    for (; y < ry1;) {
+      if (tile || (x >= cx0 && x < cx1 && y >= cy0 && y < cy1)) {
+        double *q = o + (x * sx + y * sy);
+        const double v = q[moff];
+        *q = neg ? -v : v;
+      }
+      x += dx;
+      y += dy;
+      if (x >= rx1) {
+        x -= w;
+        y++;
+      }
     }
   }
 }
@@ -228,19 +273,24 @@ __global__ void __launch_bounds__(kThreads, G::min_blocks) fused_chain_kernel(co
       const int y0 = max(c.cy0 - B.hy0, B.ay0), y1 = min(c.cy1 + B.hy1, B.ay1);
       const int w = x1 - x0;
       if (w <= 0 || y1 <= y0) continue;
-      const int n = w * (y1 - y0);
       const double *src = reinterpret_cast<const double *>(B.src);
-      double *dst = sm + B.off;
+      double *dst = sm + B.off + (x0 - (c.cx0 - B.hx0)) + (y0 - (c.cy0 - B.hy0)) * B.pitch;
+      src += x0 + (long long)y0 * B.ay;
       // asynchronous copies (cp.async, 8 bytes each): every tile's loads are
       // in flight at once instead of one dependent load per thread at a time
-      for (int p = threadIdx.x; p < n; p += kThreads) {
-        const int yy = p / w;
-        const int x = x0 + (p - yy * w);
-        const int y = y0 + yy;
-        const unsigned int s_addr = (unsigned int)__cvta_generic_to_shared(
-            dst + (x - (c.cx0 - B.hx0)) + (y - (c.cy0 - B.hy0)) * B.pitch);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s_addr), "l"(src + x + (long long)y * B.ay)
+      const int dy = kThreads / w, dx = kThreads - dy * w;
+      int yy = (int)threadIdx.x / w;
+      int xx = (int)threadIdx.x - yy * w;
+      for (; yy < y1 - y0;) {
+        const unsigned int s_addr = (unsigned int)__cvta_generic_to_shared(dst + xx + yy * B.pitch);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s_addr), "l"(src + xx + (long long)yy * B.ay)
                      : "memory");
+        xx += dx;
+        yy += dy;
+        if (xx >= w) {
+          xx -= w;
+          yy++;
+        }
       }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -268,12 +318,19 @@ __global__ void __launch_bounds__(kThreads, G::min_blocks) fused_chain_kernel(co
         const int y0 = max(wb[2], c.cy0), y1 = min(wb[3], c.cy1);
         const int w = x1 - x0;
         if (w <= 0 || y1 <= y0) continue;
-        const int n = w * (y1 - y0);
-        for (int p = threadIdx.x; p < n; p += kThreads) {
-          const int yy = p / w;
-          const int x = x0 + (p - yy * w);
-          const int y = y0 + yy;
-          dst[x + (long long)y * B.ay] = srcs[(x - (c.cx0 - B.hx0)) + (y - (c.cy0 - B.hy0)) * B.pitch];
+        double *d = dst + x0 + (long long)y0 * B.ay;
+        const double *sv = srcs + (x0 - (c.cx0 - B.hx0)) + (y0 - (c.cy0 - B.hy0)) * B.pitch;
+        const int dy = kThreads / w, dx = kThreads - dy * w;
+        int yy = (int)threadIdx.x / w;
+        int xx = (int)threadIdx.x - yy * w;
+        for (; yy < y1 - y0;) {
+          d[xx + (long long)yy * B.ay] = sv[xx + yy * B.pitch];
+          xx += dx;
+          yy += dy;
+          if (xx >= w) {
+            xx -= w;
+            yy++;
+          }
         }
       }
     }

@@ -747,6 +747,10 @@ FusionState &Runtime::fusion_state() {
 void Runtime::release_fusion_plans() {
   if (fusion_state_) fusion_state_->drop_plans();
 }
+void Runtime::set_tile_candidate(int c) {
+  if (c < -1 || c >= kNumCands) throw Error(E_ARG, "tile_candidate must be -1 or 0.." + std::to_string(kNumCands - 1));
+  tile_candidate_ = c;
+}
 void Runtime::release_fusion_state() {
   delete fusion_state_;
   fusion_state_ = nullptr;
@@ -830,10 +834,16 @@ void Runtime::plan_fusion(const std::vector<Desc> &q, std::vector<FusedItem> &it
       }
       if (ok->second > 0) fits.push_back(s);
     }
-    if (tuning_on && !fits.empty()) fits.push_back(kUnfused);
     bool tuning = false;
-    const int s = S.shape_for(A->key, fits, tuning_on, &tuning);
-    if (s < 0 || (s == kUnfused && !tuning)) continue;
+    int s;
+    if (tile_candidate_ >= 0) {  // one candidate for every chain it fits (tests, profiling): no tuning
+      if (std::find(fits.begin(), fits.end(), tile_candidate_) == fits.end()) continue;
+      s = tile_candidate_;
+    } else {
+      if (tuning_on && !fits.empty()) fits.push_back(kUnfused);
+      s = S.shape_for(A->key, fits, tuning_on, &tuning);
+      if (s < 0 || (s == kUnfused && !tuning)) continue;
+    }
     if (trace) FusionPlanner::trace(q, *A, *this);
     FusedItem it;
     it.first = A->first;

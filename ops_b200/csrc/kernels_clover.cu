@@ -747,7 +747,7 @@ REG(reset_field_kernel1) REG(reset_field_kernel2) REG(field_summary_kernel)
 // boundary copies between them, as one tiled kernel. The timestep and
 // Lagrangian loops compile leaner than the advection loops, so they get a
 // group (and register budget) of their own.
-static fuse::GroupRegistrar<3, ideal_gas_kernel, viscosity_kernel, calc_dt_kernel, calc_dt_kernel_min,
+static fuse::GroupRegistrar<2, ideal_gas_kernel, viscosity_kernel, calc_dt_kernel, calc_dt_kernel_min,
                             PdV_kernel_predict, PdV_kernel_nopredict, revert_kernel, accelerate_kernel,
                             flux_calc_kernelx, flux_calc_kernely, reset_field_kernel1, reset_field_kernel2>
     fused_lagrange("cloverleaf2d_lagrange");

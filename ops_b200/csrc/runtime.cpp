@@ -130,6 +130,8 @@ void Runtime::init(int device, int diags) {
   if (t) tiling_on_ = atoi(t);
   const char *l = getenv("OPS_B200_LISTS");
   if (l) lists_on_ = atoi(l);
+  const char *tc = getenv("OPS_B200_TILE_CANDIDATE");
+  if (tc) set_tile_candidate(atoi(tc));
   inited_ = true;
 }
 

@@ -267,6 +267,7 @@ class Runtime {
   void set_fusion(int on) { fusion_on_ = on; }
   void set_tiling(int on) { tiling_on_ = on; }
   void set_lists(int on) { lists_on_ = on; }
+  void set_tile_candidate(int c);
   long long list_plans() const { return list_launches_; }
   long long list_loops() const { return list_loops_; }
   long long loops_skipped() const { return loops_skipped_; }
@@ -406,6 +407,7 @@ class Runtime {
   int fusion_on_ = 1;
   int tiling_on_ = 1;  // loop-chain fusion into tiled kernels (needs fusion_on_)
   int lists_on_ = 1;   // runs of one kernel over several blocks in one launch (needs fusion_on_)
+  int tile_candidate_ = -1;  // >= 0: every fused chain runs this tuning candidate (no tuning)
   // Redundant-loop elimination within one flush: per queued loop, the
   // version of each dat arg (read: as observed, written: as produced);
   // dat versions count the writes of the queued loops and restart at every
