@@ -310,6 +310,19 @@ def cpu_reference_clover(steps, threads, n=CL_N):
     return n * n * steps / secs, secs
 
 
+def print_kernel_table(stats, steps, cells, peak_gbs):
+    """Per-kernel CUDA-event timing of `steps` cycles on stderr: launches,
+    ms per step, share, algorithmic bytes per cell and achieved GB/s."""
+    tot = sum(v[1] for v in stats.values())
+    print(f"{'kernel':56s} {'launch/step':>11s} {'ms/step':>8s} {'share':>6s} {'B/cell':>7s} {'GB/s':>7s} {'frac':>5s}",
+          file=sys.stderr)
+    for k, (n, ms, by) in sorted(stats.items(), key=lambda kv: -kv[1][1]):
+        gbs = by / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        print(f"{k:56s} {n / steps:11.2f} {ms / steps:8.4f} {ms / tot:6.1%} {by / steps / cells:7.1f} {gbs:7.0f}"
+              f" {gbs / peak_gbs:5.2f}", file=sys.stderr)
+    print(f"{'total':56s} {sum(v[0] for v in stats.values()) / steps:11.2f} {tot / steps:8.4f}", file=sys.stderr)
+
+
 def bench_clover(args, world, rank, local, pg):
     from ops_b200 import apps
     from ops_b200 import ops as O
@@ -342,6 +355,8 @@ def bench_clover(args, world, rank, local, pg):
     stats = O.kernel_stats()
     O.set_kernel_timing(0)
     launches_per_step = sum(v[0] for v in stats.values()) / kp
+    if args.kernel_table and rank == 0:
+        print_kernel_table(stats, kp, cells, peaks["hbm_gbs"])
     dom, (n, ms, by) = max(stats.items(), key=lambda kv: kv[1][1])
     achieved = (by / n) / (ms / n * 1e-3) / 1e9
     tot_ms = sum(v[1] for v in stats.values())
@@ -473,6 +488,8 @@ def bench_clover3d(args, world, rank, local, pg):
     stats = O.kernel_stats()
     O.set_kernel_timing(0)
     launches_per_step = sum(v[0] for v in stats.values()) / kp
+    if args.kernel_table and rank == 0:
+        print_kernel_table(stats, kp, cells, peaks["hbm_gbs"])
     dom, (n, ms, by) = max(stats.items(), key=lambda kv: kv[1][1])
     achieved = (by / n) / (ms / n * 1e-3) / 1e9
     tot_ms = sum(v[1] for v in stats.values())
@@ -1235,6 +1252,8 @@ def main():
                     help="tea: FP32 residual decrease between FP64 reliable updates")
     ap.add_argument("--cpu-tea-iters", type=int, default=100, help="tea: CG iterations in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-table", action="store_true",
+                    help="clover, clover3d: print the per-kernel timing table of the roofline pass on stderr")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"laplace": 200, "clover": 200, "clover3d": 100, "adi": 50, "tea": 3,
