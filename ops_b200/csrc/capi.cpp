@@ -59,6 +59,12 @@ std::vector<opsb::Arg> convert_args(int nargs, const ops_b200_arg *args) {
 }
 }  // namespace
 
+namespace opsb {
+namespace trid {
+void set_warp_mode(int m);
+}
+}  // namespace opsb
+
 extern "C" {
 
 const char *ops_b200_last_error(void) { return g_last_error.c_str(); }
@@ -243,6 +249,7 @@ int ops_b200_set_option(const char *name, int value) {
     else if (n == "tiling") rt().set_tiling(value);
     else if (n == "lists") rt().set_lists(value);
     else if (n == "tile_candidate") rt().set_tile_candidate(value);
+    else if (n == "trid_warp") opsb::trid::set_warp_mode(value);
     else throw opsb::Error(opsb::E_ARG, "unknown option " + n);
     return 0;
   });

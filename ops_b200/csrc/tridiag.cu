@@ -320,6 +320,195 @@ __global__ void __launch_bounds__(kTileThreads, kCtasPerSm) trid_tile_kernel(con
   }
 }
 
+// x sweeps (lines contiguous in HBM) of up to 32 R rows: one warp per line,
+// no block-wide barriers. The warp stages its line's a, b, c, d through its
+// own strip of shared memory with coalesced cp.async copies (row r at r + r / 8, so
+// that lanes reading neighbouring chunks hit different banks), every lane
+// eliminates a chunk of at most R rows in registers by the same partition
+// recurrences as trid_tile_kernel, the 64 chunk end rows (two per lane) are
+// solved by parallel cyclic reduction over warp shuffles, and the lanes
+// substitute back and store through the strip. Each thread keeps a whole
+// chunk in flight, so a warp has its line's 4 x n loads outstanding at once.
+constexpr int kWarpLines = 8;  // lines (warps) per CTA
+
+template <int R>
+__host__ __device__ constexpr int warp_strip(int) { return 32 * R + 4 * R + 2; }
+__device__ __forceinline__ int strip_pos(int r) { return r + (r >> 3); }
+
+template <class T, int R>
+__global__ void __launch_bounds__(32 * kWarpLines, 2)
+    trid_warp_kernel(const Sys *__restrict__ sys, const Work *__restrict__ work, int nwork) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int SW = warp_strip<R>(0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T *Sa = reinterpret_cast<T *>(smraw) + (size_t)warp * 4 * SW;
+  T *Sb = Sa + SW, *Sc = Sb + SW, *Sd = Sc + SW;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const Work wk = work[w];
+    const Sys s = sys[wk.sys];
+    const int li = wk.l0 + warp;
+    if (li >= s.nl0) continue;  // the same for the whole warp
+    const int n = s.n;
+    const long long base = (long long)li * s.s0 + (long long)wk.l1 * s.s1;
+    const T *ga = reinterpret_cast<const T *>(s.a) + base;
+    const T *gb = reinterpret_cast<const T *>(s.b) + base;
+    const T *gc = reinterpret_cast<const T *>(s.c) + base;
+    T *gd = reinterpret_cast<T *>(s.d) + base;
+    T *gu = s.u ? reinterpret_cast<T *>(s.u) + base : nullptr;
+    // asynchronous copies: the line's 4 n loads are all in flight at once
+    for (int i = lane; i < n; i += 32) {
+      const int p = strip_pos(i);
+      cp_async(Sa + p, ga + i);
+      cp_async(Sb + p, gb + i);
+      cp_async(Sc + p, gc + i);
+      cp_async(Sd + p, gd + i);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
+    // 1. this lane's chunk: forward and backward partition sweeps in registers
+    const int kact = n >= 64 ? 32 : (n / 2 > 0 ? n / 2 : 1);
+    const int r0 = lane * n / kact, m = (lane + 1) * n / kact - r0;
+    const bool act = lane < kact && n > 1;
+    T ra[R], rc[R], rd[R];
+    T fa[2] = {T(0), T(0)}, fb[2] = {T(1), T(1)}, fc[2] = {T(0), T(0)}, fd[2] = {T(0), T(0)};
+    if (act) {
+      T pa = T(0), pc = T(0), pd = T(0);
+#pragma unroll
+      for (int i = 0; i < R; i++) {
+        if (i < m) {
+          const int p = strip_pos(r0 + i);
+          const T ai = Sa[p], bi = Sb[p], ci = Sc[p], di = Sd[p];
+          T na, nc, nd;
+          if (i < 2) {
+            const T r = recip(bi);
+            na = ai * r;
+            nc = ci * r;
+            nd = di * r;
+          } else {
+            const T r = recip(bi - ai * pc);
+            nd = r * (di - ai * pd);
+            na = -r * ai * pa;
+            nc = r * ci;
+          }
+          ra[i] = na;
+          rc[i] = nc;
+          rd[i] = nd;
+          pa = na;
+          pc = nc;
+          pd = nd;
+        }
+      }
+      fa[1] = pa;
+      fc[1] = lane == kact - 1 ? T(0) : pc;
+      fd[1] = pd;
+      // backward: rows m-3 .. 1 fold in row i + 1 (whose values ride in
+      // na, nc, nd; rows from m-2 up pass theirs on unchanged)
+      T na = T(0), nc = T(0), nd = T(0);
+#pragma unroll
+      for (int t = 0; t < R - 1; t++) {
+        const int i = R - 1 - t;
+        if (i <= m - 3) {
+          const T ci = rc[i];
+          nd = rd[i] - ci * nd;
+          na = ra[i] - ci * na;
+          nc = -ci * nc;
+          ra[i] = na;
+          rc[i] = nc;
+          rd[i] = nd;
+        } else {
+          na = ra[i];
+          nc = rc[i];
+          nd = rd[i];
+        }
+      }
+      T a0 = ra[0], c0 = rc[0], d0 = rd[0];
+      if (m > 2) {
+        const T r = recip(T(1) - c0 * ra[1]);
+        d0 = r * (d0 - c0 * rd[1]);
+        a0 = r * a0;
+        c0 = -r * c0 * rc[1];
+      }
+      ra[0] = a0;
+      rc[0] = c0;
+      rd[0] = d0;
+      fa[0] = lane == 0 ? T(0) : a0;
+      fc[0] = c0;
+      fd[0] = d0;
+    }
+    // 2. the 64 chunk end rows (row 2 lane + j), parallel cyclic reduction
+    // over shuffles; lanes without a chunk hold identity rows
+    for (int h = 1; h < 64; h *= 2) {
+      T ma[2], mb[2], mc[2], md[2], pa[2], pb[2], pc[2], pd[2];
+      if (h == 1) {
+        ma[0] = __shfl_up_sync(0xffffffffu, fa[1], 1);
+        mb[0] = __shfl_up_sync(0xffffffffu, fb[1], 1);
+        mc[0] = __shfl_up_sync(0xffffffffu, fc[1], 1);
+        md[0] = __shfl_up_sync(0xffffffffu, fd[1], 1);
+        pa[1] = __shfl_down_sync(0xffffffffu, fa[0], 1);
+        pb[1] = __shfl_down_sync(0xffffffffu, fb[0], 1);
+        pc[1] = __shfl_down_sync(0xffffffffu, fc[0], 1);
+        pd[1] = __shfl_down_sync(0xffffffffu, fd[0], 1);
+        pa[0] = fa[1]; pb[0] = fb[1]; pc[0] = fc[1]; pd[0] = fd[1];
+        ma[1] = fa[0]; mb[1] = fb[0]; mc[1] = fc[0]; md[1] = fd[0];
+      } else {
+        const int q = h >> 1;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          ma[j] = __shfl_up_sync(0xffffffffu, fa[j], q);
+          mb[j] = __shfl_up_sync(0xffffffffu, fb[j], q);
+          mc[j] = __shfl_up_sync(0xffffffffu, fc[j], q);
+          md[j] = __shfl_up_sync(0xffffffffu, fd[j], q);
+          pa[j] = __shfl_down_sync(0xffffffffu, fa[j], q);
+          pb[j] = __shfl_down_sync(0xffffffffu, fb[j], q);
+          pc[j] = __shfl_down_sync(0xffffffffu, fc[j], q);
+          pd[j] = __shfl_down_sync(0xffffffffu, fd[j], q);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int k = 2 * lane + j;
+        T ak = fa[j], bk = fb[j], ck = fc[j], dk = fd[j];
+        if (k - h >= 0) {
+          const T al = -ak * recip(mb[j]);
+          ak = al * ma[j];
+          bk = bk + al * mc[j];
+          dk = dk + al * md[j];
+        } else {
+          ak = T(0);
+        }
+        if (k + h < 64) {
+          const T g = -ck * recip(pb[j]);
+          ck = g * pc[j];
+          bk = bk + g * pa[j];
+          dk = dk + g * pd[j];
+        } else {
+          ck = T(0);
+        }
+        fa[j] = ak;
+        fb[j] = bk;
+        fc[j] = ck;
+        fd[j] = dk;
+      }
+    }
+    // 3. substitute back, then store through the strip with the loads' mapping
+    if (act) {
+      const T xf = fd[0] * recip(fb[0]), xl = fd[1] * recip(fb[1]);
+#pragma unroll
+      for (int i = 0; i < R; i++)
+        if (i < m) Sd[strip_pos(r0 + i)] = (i == 0) ? xf : (i == m - 1) ? xl : rd[i] - ra[i] * xf - rc[i] * xl;
+    }
+    if (n == 1 && lane == 0) Sd[0] = Sd[0] * recip(Sb[0]);
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+      const T x = Sd[strip_pos(i)];
+      if (gu) gu[i] += x;
+      else gd[i] = x;
+    }
+    __syncwarp();
+  }
+}
+
 // Lines strided along the solve dimension and contiguous across lines (the
 // y and z sweeps): one thread per line runs the Thomas algorithm straight
 // from HBM, neighbouring threads reading neighbouring lines so every access
@@ -487,6 +676,31 @@ bool launch_lines(std::vector<Sys> systems, cudaStream_t stream, long long *kern
   return true;
 }
 
+// "trid_warp" option: -1 chooses by line length, 0 never, 1 whenever it applies.
+int &warp_mode() {
+  static int m = -1;
+  return m;
+}
+void set_warp_mode(int m) {
+  if (m < -1 || m > 1) throw Error(E_ARG, "trid_warp must be -1, 0 or 1");
+  warp_mode() = m;
+}
+
+template <class T, int R>
+void launch_warp(const Buffers &B, int nwork, cudaStream_t stream) {
+  const int smem = (int)(kWarpLines * 4 * warp_strip<R>(0) * sizeof(T));
+  static int occupancy = 0;  // CTAs per SM, per instantiation
+  if (occupancy == 0) {
+    OPSB_CUDA(cudaFuncSetAttribute(trid_warp_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    OPSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, trid_warp_kernel<T, R>, 32 * kWarpLines,
+                                                            smem));
+    occupancy = std::max(occupancy, 1);
+  }
+  const int grid = std::min(nwork, 148 * occupancy);
+  trid_warp_kernel<T, R><<<grid, 32 * kWarpLines, smem, stream>>>(B.sys, B.work, nwork);
+  OPSB_CUDA(cudaGetLastError());
+}
+
 template <class T>
 void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, long long *kernels) {
   (void)solvedim;
@@ -494,8 +708,23 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
   for (const Sys &s : systems) maxn = std::max(maxn, s.n);
   if (maxn == 0) return;
   if (launch_lines<T>(systems, stream, kernels)) return;
+  bool contig = true;
+  long long nlines = 0, nunk = 0;
+  for (const Sys &s : systems) {
+    contig = contig && (s.n == 0 || s.ss == 1);
+    nlines += (long long)s.nl0 * s.nl1;
+    nunk += (long long)s.nl0 * s.nl1 * s.n;
+  }
+  // x sweeps of lines up to 256 rows averaging at least 160: one warp per
+  // line (trid_warp_kernel). A warp's per-line latency (staging, chunk
+  // sweeps, six reduction steps) is nearly independent of the length, so
+  // batches of short lines go to the tile kernel (256^3 FP64 x sweep 0.40 ->
+  // 0.28 ms; the 64-block batch with edges in [32, 192] would take 1.89 ms
+  // against the tile kernel's 1.38 ms).
+  const int wm = warp_mode();
+  const bool warp_path = contig && maxn <= 256 && (wm == 1 || (wm < 0 && nunk >= 160 * nlines));
   // lines per work item: the largest power of two (<= 64) whose tiles fit
-  int L = 64;
+  int L = warp_path ? kWarpLines : 64;
   while (L > 1 && tile_smem<T>(L, maxn) > kTileSmem) L /= 2;
   if (tile_smem<T>(L, maxn) > kTileSmem) throw Error(E_UNSUPPORTED, "tridiagonal lines longer than the tile budget");
   std::vector<Work> work;
@@ -520,6 +749,14 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
   OPSB_CUDA(cudaMemcpyAsync(B.sys, systems.data(), systems.size() * sizeof(Sys), cudaMemcpyHostToDevice, stream));
   OPSB_CUDA(cudaMemcpyAsync(B.work, work.data(), work.size() * sizeof(Work), cudaMemcpyHostToDevice, stream));
   const int nwork = (int)work.size();
+  if (warp_path) {
+    if (maxn <= 128)
+      launch_warp<T, 4>(B, nwork, stream);
+    else
+      launch_warp<T, 8>(B, nwork, stream);
+    if (kernels) (*kernels)++;
+    return;
+  }
   const size_t smem = tile_smem<T>(L, maxn);
   static size_t attr_set = 0;
   if (smem > attr_set) {

@@ -90,12 +90,22 @@ def test_inc_form(gpu_runtime, orc, solvedim):
     np.testing.assert_allclose(ug, u + ref, rtol=1e-12, atol=1e-12)
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 15, 16, 17, 31, 63, 64, 65, 129, 256])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 15, 16, 17, 31, 63, 64, 65, 127, 128, 129, 200, 255, 256, 257, 700])
 @pytest.mark.parametrize("solvedim", [0, 1])
-def test_line_lengths(gpu_runtime, orc, n, solvedim):
+@pytest.mark.parametrize("warp", [-1, 0, 1])
+def test_line_lengths(gpu_runtime, orc, n, solvedim, warp):
+    """x lines: the warp-per-line kernel (4 or 8 rows a lane, lines up to
+    256 rows) and the shared-memory tile kernel, each forced and as chosen
+    by line length; y lines: the line kernel."""
+    if solvedim == 1 and warp != -1:
+        pytest.skip("the option steers x sweeps only")
     shape = (5, n) if solvedim == 0 else (n, 7)
     a, b, c, d = seeded.trid_system(shape, solvedim, n)
-    x, _ = run_gpu(a, b, c, d, solvedim)
+    O.set_option("trid_warp", warp)
+    try:
+        x, _ = run_gpu(a, b, c, d, solvedim)
+    finally:
+        O.set_option("trid_warp", -1)
     ref = d.copy()
     oracle_solve(orc, a, b, c, ref, solvedim)
     np.testing.assert_allclose(x, ref, rtol=1e-12, atol=1e-13)
