@@ -244,7 +244,8 @@ def bench_laplace(args, world, rank, local, pg):
                    "step": "apply_stencil + max|delta| readback + copy (elided by renaming)",
                    "l2": "inputs larger than L2 (two 134 MB fields)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": TRAFFIC_PER_CELL["laplace"] * cells,
+                     "traffic_source": "ncu capture at 4096^2 (profiles/laplace2d_4096_apply_stencil_dram.md)",
                      "kernel": "laplace2d/apply_stencil", "alg_bytes_per_launch": alg_bytes,
                      "avg_launch_ms": avg_s * 1e3, "peak_source": f"{peak_kind} hbm_gbs"},
         "e2e": {"value": world * cells * K / e2e_s, "unit": "cell-updates/s",
@@ -286,6 +287,21 @@ def reference_laplace(args, world, rank):
 # CloverLeaf 2D hydro
 # ---------------------------------------------------------------------------
 CL_N = 3840
+# DRAM bytes per cell of one launch of a workload's dominant kernel, from one
+# ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum; the
+# captures are summarised in profiles/, which names the command):
+#   CloverLeaf 2D PdV_kernel_nopredict at 2560^2: 89.3 + 21.0 B
+#     (profiles/cloverleaf2d_2560_dram_per_kernel.md)
+#   CloverLeaf 3D PdV_kernel_nopredict at 160^3: 141.4 + 22.6 B
+#     (profiles/cloverleaf3d_160_pdv_accelerate.md)
+#   Laplace apply_stencil at 4096^2: 227.4 MB per launch / 4096^2
+#     (profiles/laplace2d_4096_apply_stencil_dram.md)
+#   ADI 256^3 FP64 x / y / z sweeps: 650.1 / 1144.0 / 1283.4 MB per sweep / 256^3
+#     (profiles/adi_cube_256_fp64_dram.md)
+# Traffic grows with the cells (or unknowns) a launch processes, so a
+# launch's traffic is the figure times its cells.
+TRAFFIC_PER_CELL = {"clover": 110.3, "clover3d": 164.0, "laplace": 227.4e6 / 4096 ** 2,
+                    "adi_cube_fp64": (650.1e6 / 256 ** 3, 1144.0e6 / 256 ** 3, 1283.4e6 / 256 ** 3)}
 
 
 def clover_deck(steps, n=CL_N):
@@ -388,7 +404,10 @@ def bench_clover(args, world, rank, local, pg):
                            " + reset_field + field_summary (5 FP64 sums read back)",
                    "l2": "inputs larger than L2 (about 30 fields of 118 MB)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": dom,
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": TRAFFIC_PER_CELL["clover"] * cells
+                     if dom == "cloverleaf/PdV_kernel_nopredict" else None,
+                     "traffic_source": "ncu capture of PdV_kernel_nopredict at 2560^2, per cell x cells"
+                                       " (profiles/cloverleaf2d_2560_dram_per_kernel.md)", "kernel": dom,
                      "alg_bytes_per_launch": by / n, "avg_launch_ms": ms / n, "peak_source": f"{peak_kind} hbm_gbs",
                      "step_effective_gbs": tot_by / (tot_ms * 1e-3) / 1e9,
                      "step_alg_bytes_per_cell": tot_by / kp / cells},
@@ -520,7 +539,10 @@ def bench_clover3d(args, world, rank, local, pg):
                            " + field_summary (5 FP64 sums read back)",
                    "l2": "inputs larger than L2 (about 40 fields of 140 MB)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": dom,
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": TRAFFIC_PER_CELL["clover3d"] * cells
+                     if dom == "cloverleaf3d/PdV_kernel_nopredict" else None,
+                     "traffic_source": "ncu capture of PdV_kernel_nopredict at 160^3, per cell x cells"
+                                       " (profiles/cloverleaf3d_160_pdv_accelerate.md)", "kernel": dom,
                      "alg_bytes_per_launch": by / n, "avg_launch_ms": ms / n, "peak_source": f"{peak_kind} hbm_gbs",
                      "step_effective_gbs": tot_by / (tot_ms * 1e-3) / 1e9,
                      "step_alg_bytes_per_cell": tot_by / kp / cells},
@@ -689,7 +711,11 @@ def bench_adi(args, world, rank, local, pg):
                    if unknowns * es * 4 > 126e6 else "inputs fit in L2 (batch case)",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": f"sweep {'xyz'[dom]}",
+                     "frac": achieved / peaks["hbm_gbs"], "kernel": f"sweep {'xyz'[dom]}",
+                     "traffic": TRAFFIC_PER_CELL["adi_cube_fp64"][dom] * unknowns
+                     if name == "adi_cube_fp64" else None,
+                     "traffic_source": "ncu capture of one x, y and z sweep at 256^3 FP64"
+                                       " (profiles/adi_cube_256_fp64_dram.md); other cases not captured",
                      "sweep_ms": sweep_ms, "alg_bytes_per_unknown": byt, "peak_source": f"{peak_kind} hbm_gbs"},
         "e2e": {"value": world * 3 * unknowns / e2e_s, "unit": "unknowns solved/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": unknowns * es},
