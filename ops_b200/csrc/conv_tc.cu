@@ -126,12 +126,17 @@ template <int CIN, int COUT>
 struct Cfg {
   static constexpr int S = CIN * 2;                    // bytes per pixel row = swizzle span
   static constexpr uint32_t LAYOUT = CIN == 16 ? 6u : CIN == 32 ? 4u : 2u;  // SW32 / SW64 / SW128
-  static constexpr int A_BYTES = kTileM * S;
+  // 128-pixel MMA blocks per tile: at 16 input channels one TMA box per tap
+  // carries 4 blocks (16 KB instead of 4 KB; 4096^2 16->16 826 -> 665 us);
+  // at 32 channels 2 blocks a box measured slower (358 -> 407 us at 2048^2
+  // 32->32), at 64 no change, so those keep one block a box
+  static constexpr int SUB = CIN == 16 ? 4 : 1;
+  static constexpr int A_BYTES = SUB * kTileM * S;
   static constexpr int W_TAP = COUT * S;
   static constexpr int W_BYTES = 9 * W_TAP;
-  static constexpr int STAGES = CIN == 16 ? 16 : 8;
-  static constexpr int NACC = 4;                       // accumulator buffers in tensor memory
-  static constexpr int TMEM_COLS = NACC * COUT;        // 64, 128 or 256 columns
+  static constexpr int STAGES = SUB > 1 ? 6 : 8;
+  static constexpr int NACC = SUB > 1 ? 2 : 4;         // accumulator sets in tensor memory
+  static constexpr int TMEM_COLS = NACC * SUB * COUT;  // 64, 128 or 256 columns
   static constexpr int OFF_W = 0;
   static constexpr int OFF_A = (W_BYTES + 1023) / 1024 * 1024;
   static constexpr int OFF_BAR = OFF_A + STAGES * A_BYTES;
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t d = tmem + (uint32_t)(b * COUT);
+        const uint32_t d = tmem + (uint32_t)(b * C::SUB * COUT);
         for (int tap = 0; tap < 9 && ok; tap++) {
           if (!mbar_wait(&full[s], ph, abort_flag)) {
             record_error(a.err, abort_flag, ERR_WAIT_FULL);
@@ -249,11 +254,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           tc_fence_after();
 #pragma unroll
-          for (int kb = 0; kb < CIN / 16; kb++) {
-            const uint64_t ad = smem_desc(sA0 + s * C::A_BYTES + kb * 32, 8 * C::S, C::LAYOUT);
-            const uint64_t bd = smem_desc(sW0 + tap * C::W_TAP + kb * 32, 8 * C::S, C::LAYOUT);
-            umma_bf16(d, ad, bd, IDESC, (tap | kb) != 0 ? 1u : 0u);
-          }
+          for (int j = 0; j < C::SUB; j++)
+#pragma unroll
+            for (int kb = 0; kb < CIN / 16; kb++) {
+              const uint64_t ad =
+                  smem_desc(sA0 + s * C::A_BYTES + j * kTileM * C::S + kb * 32, 8 * C::S, C::LAYOUT);
+              const uint64_t bd = smem_desc(sW0 + tap * C::W_TAP + kb * 32, 8 * C::S, C::LAYOUT);
+              umma_bf16(d + (uint32_t)(j * COUT), ad, bd, IDESC, (tap | kb) != 0 ? 1u : 0u);
+            }
           umma_commit(&empty[s]);
           issued = true;
           last_commit = &empty[s];
@@ -291,48 +299,54 @@ __global__ void __launch_bounds__(kThreads, 1)
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
       tc_fence_after();
-      float v[COUT];
-      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * COUT);
+      const int img = t / per_img, rem = t - img * per_img;
+      const int ty = rem / a.tiles_x, tx = rem - ty * a.tiles_x;
+#pragma unroll 1
+      for (int j = 0; j < C::SUB; j++) {
+        float v[COUT];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((b * C::SUB + j) * COUT);
 #pragma unroll
-      for (int c = 0; c < COUT; c += 16) tmem_ld16(taddr + c, v + c);
-      tmem_wait_ld();
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[b]);
+        for (int c = 0; c < COUT; c += 16) tmem_ld16(taddr + c, v + c);
+        tmem_wait_ld();
+        if (j == C::SUB - 1) {  // this accumulator set is read: the MMA warp may reuse it
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[b]);
+        }
+        const int p = j * kTileM + row;  // pixel of the tile (row-major over tw x th)
+        const int x = tx * a.tw + p % a.tw, y = ty * a.th + p / a.tw;
+        if (x >= a.w || y >= a.h) continue;
+        const size_t pix = ((size_t)img * a.h + y) * a.w + x;
+        if (a.mode == CONV_BIAS_RELU || a.mode == CONV_BIAS) {
+#pragma unroll
+          for (int c = 0; c < COUT; c++) {
+            float o = v[c] + a.bias[c];
+            v[c] = (a.mode == CONV_BIAS_RELU) ? fmaxf(o, 0.0f) : o;
+          }
+        } else if (a.mode == CONV_MASK) {
+          const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + pix * COUT);
+#pragma unroll
+          for (int c8 = 0; c8 < COUT / 8; c8++) {
+            uint4 m = mp[c8];
+            const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&m);
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+              if (!(__bfloat162float(mb[k]) > 0.0f)) v[c8 * 8 + k] = 0.0f;
+          }
+        }
+        uint4 *yp = reinterpret_cast<uint4 *>(a.y + pix * COUT);
+#pragma unroll
+        for (int c8 = 0; c8 < COUT / 8; c8++) {
+          uint4 o;
+          __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+          for (int k = 0; k < 4; k++) ob[k] = __floats2bfloat162_rn(v[c8 * 8 + 2 * k], v[c8 * 8 + 2 * k + 1]);
+          yp[c8] = o;
+        }
+      }
       if (++b == C::NACC) {
         b = 0;
         aph ^= 1u;
-      }
-      const int img = t / per_img, rem = t - img * per_img;
-      const int ty = rem / a.tiles_x, tx = rem - ty * a.tiles_x;
-      const int x = tx * a.tw + row % a.tw, y = ty * a.th + row / a.tw;
-      if (x >= a.w || y >= a.h) continue;
-      const size_t pix = ((size_t)img * a.h + y) * a.w + x;
-      if (a.mode == CONV_BIAS_RELU || a.mode == CONV_BIAS) {
-#pragma unroll
-        for (int c = 0; c < COUT; c++) {
-          float o = v[c] + a.bias[c];
-          v[c] = (a.mode == CONV_BIAS_RELU) ? fmaxf(o, 0.0f) : o;
-        }
-      } else if (a.mode == CONV_MASK) {
-        const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + pix * COUT);
-#pragma unroll
-        for (int c8 = 0; c8 < COUT / 8; c8++) {
-          uint4 m = mp[c8];
-          const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&m);
-#pragma unroll
-          for (int k = 0; k < 8; k++)
-            if (!(__bfloat162float(mb[k]) > 0.0f)) v[c8 * 8 + k] = 0.0f;
-        }
-      }
-      uint4 *yp = reinterpret_cast<uint4 *>(a.y + pix * COUT);
-#pragma unroll
-      for (int c8 = 0; c8 < COUT / 8; c8++) {
-        uint4 o;
-        __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
-#pragma unroll
-        for (int k = 0; k < 4; k++) ob[k] = __floats2bfloat162_rn(v[c8 * 8 + 2 * k], v[c8 * 8 + 2 * k + 1]);
-        yp[c8] = o;
       }
     }
   }
@@ -430,7 +444,8 @@ cudaError_t conv3x3(const __nv_bfloat16 *x, const __nv_bfloat16 *w, int n, int h
   a.w = wd;
   a.tw = 128;
   while (a.tw > 16 && a.tw / 2 >= wd) a.tw /= 2;
-  a.th = kTileM / a.tw;
+  const int sub = cin == 16 ? 4 : 1;  // Cfg<cin, cout>::SUB
+  a.th = sub * kTileM / a.tw;
   a.tiles_x = (wd + a.tw - 1) / a.tw;
   a.tiles_y = (h + a.th - 1) / a.th;
   long long tiles = (long long)a.tiles_x * a.tiles_y * n;
