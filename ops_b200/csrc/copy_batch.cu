@@ -16,6 +16,7 @@
 // structure and stay valid when a captured graph replays them with other
 // flags. The values moved are the same doubles the loops would move: the
 // results are identical.
+#include <cstring>
 #include <unordered_map>
 
 #include "runtime.h"
@@ -42,25 +43,30 @@ struct CopyStrip {
   int neg, pad;
 };
 
-__global__ void copy_batch_kernel(const CopyStrip *__restrict__ s, int n, long long total) {
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
-       c += (long long)gridDim.x * blockDim.x) {
-    int lo = 0, hi = n - 1;  // last strip with first <= c
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (s[mid].first <= c) lo = mid;
-      else hi = mid - 1;
+// A batch is cut into chunks of kChunk cells of one strip each (the chunk
+// table follows the strips in the same device buffer); a CTA takes a chunk,
+// so it finds its strip with one load instead of a search per cell, and
+// the cell's (x, y, z) comes from 32-bit arithmetic.
+constexpr int kChunk = 1024;
+struct Chunk {
+  int strip, first;  // strip index, first cell of the chunk within the strip
+};
+
+__global__ void copy_batch_kernel(const CopyStrip *__restrict__ s, const Chunk *__restrict__ chunks, int nchunks) {
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const Chunk ch = chunks[c];
+    const CopyStrip &e = s[ch.strip];
+    if (e.flag && *e.flag != 1) continue;  // the same for the whole CTA
+    const int nx = e.nx, ny = e.ny;
+    const int end = min(ch.first + kChunk, nx * ny * e.nz);
+    double *const base = e.p + (long long)e.x0 + (long long)e.y0 * e.pitch + (long long)e.z0 * e.plane;
+    for (int k = ch.first + (int)threadIdx.x; k < end; k += blockDim.x) {
+      const int r = k / nx, x = k - r * nx;
+      const int z = r / ny, y = r - z * ny;
+      double *q = base + x + (long long)y * e.pitch + (long long)z * e.plane;
+      const double v = q[e.src];
+      *q = e.neg ? -v : v;
     }
-    const CopyStrip &e = s[lo];
-    if (e.flag && *e.flag != 1) continue;
-    long long k = c - e.first;
-    int x = (int)(k % e.nx);
-    long long r = k / e.nx;
-    int y = (int)(r % e.ny);
-    int z = (int)(r / e.ny);
-    double *q = e.p + (long long)(e.x0 + x) + (long long)(e.y0 + y) * e.pitch + (long long)(e.z0 + z) * e.plane;
-    const double v = q[e.src];
-    *q = e.neg ? -v : v;
   }
 }
 
@@ -134,8 +140,8 @@ bool plan(const std::vector<Desc> &q, size_t i, int n, Planned &out) {
   return true;
 }
 
-// Device copies of strip lists, kept by content: a captured graph keeps
-// pointing at them, so they are never rewritten or freed.
+// Device copies of strip lists and their chunk tables, kept by content: a
+// captured graph keeps pointing at them, so they are never rewritten or freed.
 std::unordered_map<uint64_t, CopyStrip *> &strip_cache() {
   static std::unordered_map<uint64_t, CopyStrip *> m;
   return m;
@@ -146,17 +152,31 @@ uint64_t hash_bytes(const void *p, size_t n) {
   for (size_t k = 0; k < n; k++) h = (h ^ c[k]) * 0x100000001B3ULL;
   return h ^ n;
 }
-CopyStrip *device_strips(const std::vector<CopyStrip> &b, bool may_upload) {
-  const size_t bytes = b.size() * sizeof(CopyStrip);
-  const uint64_t h = hash_bytes(b.data(), bytes);
+// The batch's chunks: every strip cut into runs of kChunk cells.
+std::vector<Chunk> chunks_of(const std::vector<CopyStrip> &b) {
+  std::vector<Chunk> ch;
+  for (size_t i = 0; i < b.size(); i++) {
+    const long long cells = (long long)b[i].nx * b[i].ny * b[i].nz;
+    if (cells >= (1LL << 31) - kChunk) throw Error(E_UNSUPPORTED, "copy batch: strip of 2^31 cells or more");
+    for (long long f = 0; f < cells; f += kChunk) ch.push_back({(int)i, (int)f});
+  }
+  return ch;
+}
+// One buffer: the strips, then (16-byte aligned) the chunk table.
+CopyStrip *device_strips(const std::vector<CopyStrip> &b, const std::vector<Chunk> &ch, bool may_upload) {
+  const size_t sbytes = (b.size() * sizeof(CopyStrip) + 15) / 16 * 16;
+  std::vector<unsigned char> blob(sbytes + ch.size() * sizeof(Chunk), 0);
+  memcpy(blob.data(), b.data(), b.size() * sizeof(CopyStrip));
+  if (!ch.empty()) memcpy(blob.data() + sbytes, ch.data(), ch.size() * sizeof(Chunk));
+  const uint64_t h = hash_bytes(blob.data(), blob.size());
   auto it = strip_cache().find(h);
   if (it != strip_cache().end()) return it->second;
   if (!may_upload) return nullptr;
   CopyStrip *d = nullptr;
-  OPSB_CUDA(cudaMalloc(&d, bytes));
+  OPSB_CUDA(cudaMalloc(&d, blob.size()));
   // ordered before the batch's launch on the same stream; the pageable
   // source is staged before the call returns
-  OPSB_CUDA(cudaMemcpyAsync(d, b.data(), bytes, cudaMemcpyHostToDevice, Runtime::get().stream()));
+  OPSB_CUDA(cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, Runtime::get().stream()));
   strip_cache()[h] = d;
   return d;
 }
@@ -177,14 +197,17 @@ int match_copy_run(const std::vector<Desc> &q, size_t i) {
 PlanItem prepare_copy_run(const std::vector<Desc> &q, size_t i, int n) {
   Planned pl;
   if (!plan(q, i, n, pl)) throw Error(E_STATE, "copy batch: plan failed after a match");
-  struct Launch { CopyStrip *d; int n; long long total; int blocks; };
+  struct Launch { CopyStrip *d; const Chunk *ch; int nchunks; int blocks; };
   std::vector<Launch> ls;
   for (const auto &b : pl.batches) {
     if (b.empty()) continue;
-    CopyStrip *d = device_strips(b, true);
-    long long total = b.back().first + (long long)b.back().nx * b.back().ny * b.back().nz;
-    int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
-    ls.push_back({d, (int)b.size(), total, blocks});
+    const std::vector<Chunk> ch = chunks_of(b);
+    if (ch.empty()) continue;
+    CopyStrip *d = device_strips(b, ch, true);
+    const size_t sbytes = (b.size() * sizeof(CopyStrip) + 15) / 16 * 16;
+    const Chunk *dch = reinterpret_cast<const Chunk *>(reinterpret_cast<const char *>(d) + sbytes);
+    const int blocks = (int)std::min<size_t>(ch.size(), 148 * 8);
+    ls.push_back({d, dch, (int)ch.size(), blocks});
   }
   PlanItem it;
   it.name = "runtime/copy_batch";
@@ -193,7 +216,7 @@ PlanItem prepare_copy_run(const std::vector<Desc> &q, size_t i, int n) {
   if (!ls.empty())
     it.run = [ls](cudaStream_t s) {
       for (const Launch &l : ls) {
-        copy_batch_kernel<<<l.blocks, 256, 0, s>>>(l.d, l.n, l.total);
+        copy_batch_kernel<<<l.blocks, 256, 0, s>>>(l.d, l.ch, l.nchunks);
         OPSB_CUDA(cudaGetLastError());
       }
     };
