@@ -414,7 +414,9 @@ def bench_clover(args, world, rank, local, pg):
         "e2e": {"value": world * cells * K / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": 0.0,
                 "d2h_bytes_per_step": 6 * 8 + 3 * 8,
                 "note": "one C-ABI call: deck in, device set-up (generate), K cycles each reading dt and the"
-                        " 5-value field summary back"},
+                        " 5-value field summary back; the state is generated on the device from the deck, as the"
+                        " reference app generates it, so no field crosses the boundary; the dats' storage comes"
+                        " from the runtime's pool of storage kept from the bench's earlier calls (warm pool)"},
         "gpu_launches": int(round(launches_per_step * K)),
         "clocks": clocks,
         "fusion": {"chains_per_step": fs["chains"] / (W + K), "loops_fused_per_step": fs["loops"] / (W + K),
