@@ -60,12 +60,18 @@ def _newer(target, deps):
     return os.path.exists(target) and all(os.path.getmtime(target) >= os.path.getmtime(d) for d in deps)
 
 
+def _lib_headers():
+    """The library headers the shim and the generated loop stubs compile
+    against: a change to any of them (a struct's layout) rebuilds both."""
+    hs = [os.path.join(PKG, "csrc", f) for f in os.listdir(os.path.join(PKG, "csrc")) if f.endswith((".h", ".cuh"))]
+    return hs + [os.path.join(ROOT, "include", "ops_b200.h")]
+
+
 def shim_object(ref):
     inc = os.path.join(ref, "ops", "c", "include")
     obj = os.path.join(OUT, "obj", "ops_dropin.o")
     os.makedirs(os.path.dirname(obj), exist_ok=True)
-    deps = [os.path.join(HERE, "ops_dropin.cu"), os.path.join(HERE, "ops_dropin.h")] + [
-        os.path.join(PKG, "csrc", f) for f in ("runtime.h", "ops_b200_device.cuh")]
+    deps = [os.path.join(HERE, "ops_dropin.cu"), os.path.join(HERE, "ops_dropin.h")] + _lib_headers()
     if not _newer(obj, deps):
         _run([NVCC] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I" + inc,
                               "-I" + os.path.join(PKG, "csrc"), "-I" + HERE, "-I" + os.path.join(ROOT, "include"),
@@ -82,7 +88,8 @@ def build_app(ref, name):
     wd = os.path.join(OUT, name)
     exe = os.path.join(OUT, "bin", name)
     deps = [os.path.join(src, f) for f in os.listdir(src)] + [
-        os.path.join(HERE, f) for f in ("sm100a_target.py", "ops_dropin.cu", "ops_dropin.h", "build_apps.py")]
+        os.path.join(HERE, f) for f in ("sm100a_target.py", "ops_dropin.cu", "ops_dropin.h", "build_apps.py")
+    ] + _lib_headers()
     if _newer(exe, deps):
         return exe
     if os.path.isdir(wd):
