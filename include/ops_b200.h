@@ -174,8 +174,8 @@ int ops_b200_dat_release_raw_data(int dat, int acc);
  * 64x16, 128x16, 32x16; odd: read-only dats staged in shared memory), for
  * parity tests and profiling of the fused kernels.
  * "trid_warp": x sweeps of the batched tridiagonal solver with lines of at
- * most 256 rows run one warp per line when the lines average 160 rows or
- * more (-1, default), never (0) or always (1). */
+ * most 256 rows run on the warp-per-lines kernel (-1, default, or 1) or on
+ * the shared-memory tile kernel (0). */
 int ops_b200_set_option(const char *name, int value);
 /* Counters since the last reset: kernels launched by this library, CUDA
  * graphs launched, loops queued. */

@@ -320,23 +320,34 @@ __global__ void __launch_bounds__(kTileThreads, kCtasPerSm) trid_tile_kernel(con
   }
 }
 
-// x sweeps (lines contiguous in HBM) of up to 32 R rows: one warp per line,
-// no block-wide barriers. The warp stages its line's a, b, c, d through its
-// own strip of shared memory with coalesced cp.async copies (row r at r + r / 8, so
-// that lanes reading neighbouring chunks hit different banks), every lane
-// eliminates a chunk of at most R rows in registers by the same partition
-// recurrences as trid_tile_kernel, the 64 chunk end rows (two per lane) are
-// solved by parallel cyclic reduction over warp shuffles, and the lanes
-// substitute back and store through the strip. Each thread keeps a whole
-// chunk in flight, so a warp has its line's 4 x n loads outstanding at once.
-constexpr int kWarpLines = 8;  // lines (warps) per CTA
+// x sweeps (lines contiguous in HBM) of up to 32 R rows, no block-wide
+// barriers: a warp solves 32 / P lines at once, P lanes per line (P = 32,
+// 16 or 8: the fewest lanes whose chunks of at most R rows cover a line, so
+// short lines share a warp). The warp stages its lines' a, b, c, d through
+// its own strip of shared memory with coalesced cp.async copies (row r at
+// r + r / 8, so that lanes reading neighbouring chunks hit different
+// banks), every lane eliminates its chunk in registers by the same partition
+// recurrences as trid_tile_kernel, each line's 2 P chunk end rows are solved
+// by parallel cyclic reduction over shuffles within its lane group, and the
+// lanes substitute back and store through the strip. A warp keeps all its
+// lines' 4 n loads in flight at once.
+constexpr int kWarpLines = 8;  // warps per CTA
 
 template <int R>
 __host__ __device__ constexpr int warp_strip(int) { return 32 * R + 4 * R + 2; }
 __device__ __forceinline__ int strip_pos(int r) { return r + (r >> 3); }
+// Lanes per line for lines of n rows and chunks of at most R rows.
+__host__ __device__ inline int lanes_per_line(int n, int R) {
+  int p = 32;
+  while (p > 8 && (p / 2) * R >= n) p /= 2;
+  return p;
+}
 
-template <class T, int R>
-__global__ void __launch_bounds__(32 * kWarpLines, 2)
+// FP32 lines hold half the registers: three CTAs per SM. FP: lanes per
+// line fixed at compile time (32: every line of the launch fills a warp), or
+// 0 to choose per system.
+template <class T, int R, int FP>
+__global__ void __launch_bounds__(32 * kWarpLines, sizeof(T) == 4 ? 3 : 2)
     trid_warp_kernel(const Sys *__restrict__ sys, const Work *__restrict__ work, int nwork) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int SW = warp_strip<R>(0);
@@ -346,30 +357,37 @@ __global__ void __launch_bounds__(32 * kWarpLines, 2)
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const Work wk = work[w];
     const Sys s = sys[wk.sys];
-    const int li = wk.l0 + warp;
-    if (li >= s.nl0) continue;  // the same for the whole warp
     const int n = s.n;
-    const long long base = (long long)li * s.s0 + (long long)wk.l1 * s.s1;
-    const T *ga = reinterpret_cast<const T *>(s.a) + base;
-    const T *gb = reinterpret_cast<const T *>(s.b) + base;
-    const T *gc = reinterpret_cast<const T *>(s.c) + base;
-    T *gd = reinterpret_cast<T *>(s.d) + base;
-    T *gu = s.u ? reinterpret_cast<T *>(s.u) + base : nullptr;
-    // asynchronous copies: the line's 4 n loads are all in flight at once
-    for (int i = lane; i < n; i += 32) {
-      const int p = strip_pos(i);
-      cp_async(Sa + p, ga + i);
-      cp_async(Sb + p, gb + i);
-      cp_async(Sc + p, gc + i);
-      cp_async(Sd + p, gd + i);
+    const int P = FP ? FP : lanes_per_line(n, R), G = 32 / P;  // lanes per line, lines per warp
+    const int line0 = wk.l0 + warp * G;               // this warp's first line
+    if (line0 >= s.nl0) continue;                     // the same for the whole warp
+    const long long base0 = (long long)line0 * s.s0 + (long long)wk.l1 * s.s1;
+    const T *ga = reinterpret_cast<const T *>(s.a) + base0;
+    const T *gb = reinterpret_cast<const T *>(s.b) + base0;
+    const T *gc = reinterpret_cast<const T *>(s.c) + base0;
+    T *gd = reinterpret_cast<T *>(s.d) + base0;
+    T *gu = s.u ? reinterpret_cast<T *>(s.u) + base0 : nullptr;
+    const int nlines = min(G, s.nl0 - line0);
+    // asynchronous copies, line by line over the whole warp: every load in flight at once
+    for (int g = 0; g < nlines; g++) {
+      const long long lo = (long long)g * s.s0;
+      const int ro = g * P * R;
+      for (int i = lane; i < n; i += 32) {
+        const int p = strip_pos(ro + i);
+        cp_async(Sa + p, ga + lo + i);
+        cp_async(Sb + p, gb + lo + i);
+        cp_async(Sc + p, gc + lo + i);
+        cp_async(Sd + p, gd + lo + i);
+      }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncwarp();
-    // 1. this lane's chunk: forward and backward partition sweeps in registers
-    const int kact = n >= 64 ? 32 : (n / 2 > 0 ? n / 2 : 1);
-    const int r0 = lane * n / kact, m = (lane + 1) * n / kact - r0;
-    const bool act = lane < kact && n > 1;
+    // 1. this lane's chunk of its line: forward and backward partition sweeps in registers
+    const int g = lane / P, gl = lane - g * P, ro = g * P * R;
+    const int kact = n >= 2 * P ? P : (n / 2 > 0 ? n / 2 : 1);
+    const int r0 = ro + gl * n / kact, m = (gl + 1) * n / kact - gl * n / kact;
+    const bool act = g < nlines && gl < kact && n > 1;
     T ra[R], rc[R], rd[R];
     T fa[2] = {T(0), T(0)}, fb[2] = {T(1), T(1)}, fc[2] = {T(0), T(0)}, fd[2] = {T(0), T(0)};
     if (act) {
@@ -400,7 +418,7 @@ __global__ void __launch_bounds__(32 * kWarpLines, 2)
         }
       }
       fa[1] = pa;
-      fc[1] = lane == kact - 1 ? T(0) : pc;
+      fc[1] = gl == kact - 1 ? T(0) : pc;
       fd[1] = pd;
       // backward: rows m-3 .. 1 fold in row i + 1 (whose values ride in
       // na, nc, nd; rows from m-2 up pass theirs on unchanged)
@@ -432,42 +450,44 @@ __global__ void __launch_bounds__(32 * kWarpLines, 2)
       ra[0] = a0;
       rc[0] = c0;
       rd[0] = d0;
-      fa[0] = lane == 0 ? T(0) : a0;
+      fa[0] = gl == 0 ? T(0) : a0;
       fc[0] = c0;
       fd[0] = d0;
     }
-    // 2. the 64 chunk end rows (row 2 lane + j), parallel cyclic reduction
-    // over shuffles; lanes without a chunk hold identity rows
-    for (int h = 1; h < 64; h *= 2) {
+    // 2. each line's 2 P chunk end rows (row 2 gl + j), parallel cyclic
+    // reduction over shuffles within the line's lane group; lanes without a
+    // chunk hold identity rows
+    const int N = 2 * P;
+    for (int h = 1; h < N; h *= 2) {
       T ma[2], mb[2], mc[2], md[2], pa[2], pb[2], pc[2], pd[2];
       if (h == 1) {
-        ma[0] = __shfl_up_sync(0xffffffffu, fa[1], 1);
-        mb[0] = __shfl_up_sync(0xffffffffu, fb[1], 1);
-        mc[0] = __shfl_up_sync(0xffffffffu, fc[1], 1);
-        md[0] = __shfl_up_sync(0xffffffffu, fd[1], 1);
-        pa[1] = __shfl_down_sync(0xffffffffu, fa[0], 1);
-        pb[1] = __shfl_down_sync(0xffffffffu, fb[0], 1);
-        pc[1] = __shfl_down_sync(0xffffffffu, fc[0], 1);
-        pd[1] = __shfl_down_sync(0xffffffffu, fd[0], 1);
+        ma[0] = __shfl_up_sync(0xffffffffu, fa[1], 1, P);
+        mb[0] = __shfl_up_sync(0xffffffffu, fb[1], 1, P);
+        mc[0] = __shfl_up_sync(0xffffffffu, fc[1], 1, P);
+        md[0] = __shfl_up_sync(0xffffffffu, fd[1], 1, P);
+        pa[1] = __shfl_down_sync(0xffffffffu, fa[0], 1, P);
+        pb[1] = __shfl_down_sync(0xffffffffu, fb[0], 1, P);
+        pc[1] = __shfl_down_sync(0xffffffffu, fc[0], 1, P);
+        pd[1] = __shfl_down_sync(0xffffffffu, fd[0], 1, P);
         pa[0] = fa[1]; pb[0] = fb[1]; pc[0] = fc[1]; pd[0] = fd[1];
         ma[1] = fa[0]; mb[1] = fb[0]; mc[1] = fc[0]; md[1] = fd[0];
       } else {
         const int q = h >> 1;
 #pragma unroll
         for (int j = 0; j < 2; j++) {
-          ma[j] = __shfl_up_sync(0xffffffffu, fa[j], q);
-          mb[j] = __shfl_up_sync(0xffffffffu, fb[j], q);
-          mc[j] = __shfl_up_sync(0xffffffffu, fc[j], q);
-          md[j] = __shfl_up_sync(0xffffffffu, fd[j], q);
-          pa[j] = __shfl_down_sync(0xffffffffu, fa[j], q);
-          pb[j] = __shfl_down_sync(0xffffffffu, fb[j], q);
-          pc[j] = __shfl_down_sync(0xffffffffu, fc[j], q);
-          pd[j] = __shfl_down_sync(0xffffffffu, fd[j], q);
+          ma[j] = __shfl_up_sync(0xffffffffu, fa[j], q, P);
+          mb[j] = __shfl_up_sync(0xffffffffu, fb[j], q, P);
+          mc[j] = __shfl_up_sync(0xffffffffu, fc[j], q, P);
+          md[j] = __shfl_up_sync(0xffffffffu, fd[j], q, P);
+          pa[j] = __shfl_down_sync(0xffffffffu, fa[j], q, P);
+          pb[j] = __shfl_down_sync(0xffffffffu, fb[j], q, P);
+          pc[j] = __shfl_down_sync(0xffffffffu, fc[j], q, P);
+          pd[j] = __shfl_down_sync(0xffffffffu, fd[j], q, P);
         }
       }
 #pragma unroll
       for (int j = 0; j < 2; j++) {
-        const int k = 2 * lane + j;
+        const int k = 2 * gl + j;
         T ak = fa[j], bk = fb[j], ck = fc[j], dk = fd[j];
         if (k - h >= 0) {
           const T al = -ak * recip(mb[j]);
@@ -477,11 +497,11 @@ __global__ void __launch_bounds__(32 * kWarpLines, 2)
         } else {
           ak = T(0);
         }
-        if (k + h < 64) {
-          const T g = -ck * recip(pb[j]);
-          ck = g * pc[j];
-          bk = bk + g * pa[j];
-          dk = dk + g * pd[j];
+        if (k + h < N) {
+          const T gg = -ck * recip(pb[j]);
+          ck = gg * pc[j];
+          bk = bk + gg * pa[j];
+          dk = dk + gg * pd[j];
         } else {
           ck = T(0);
         }
@@ -498,12 +518,16 @@ __global__ void __launch_bounds__(32 * kWarpLines, 2)
       for (int i = 0; i < R; i++)
         if (i < m) Sd[strip_pos(r0 + i)] = (i == 0) ? xf : (i == m - 1) ? xl : rd[i] - ra[i] * xf - rc[i] * xl;
     }
-    if (n == 1 && lane == 0) Sd[0] = Sd[0] * recip(Sb[0]);
+    if (n == 1 && gl == 0 && g < nlines) Sd[strip_pos(ro)] = Sd[strip_pos(ro)] * recip(Sb[strip_pos(ro)]);
     __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-      const T x = Sd[strip_pos(i)];
-      if (gu) gu[i] += x;
-      else gd[i] = x;
+    for (int gg = 0; gg < nlines; gg++) {
+      const long long lo = (long long)gg * s.s0;
+      const int rg = gg * P * R;
+      for (int i = lane; i < n; i += 32) {
+        const T x = Sd[strip_pos(rg + i)];
+        if (gu) gu[lo + i] += x;
+        else gd[lo + i] = x;
+      }
     }
     __syncwarp();
   }
@@ -676,7 +700,7 @@ bool launch_lines(std::vector<Sys> systems, cudaStream_t stream, long long *kern
   return true;
 }
 
-// "trid_warp" option: -1 chooses by line length, 0 never, 1 whenever it applies.
+// "trid_warp" option: -1 and 1 use the warp kernel whenever it applies, 0 never.
 int &warp_mode() {
   static int m = -1;
   return m;
@@ -686,18 +710,18 @@ void set_warp_mode(int m) {
   warp_mode() = m;
 }
 
-template <class T, int R>
+template <class T, int R, int FP>
 void launch_warp(const Buffers &B, int nwork, cudaStream_t stream) {
   const int smem = (int)(kWarpLines * 4 * warp_strip<R>(0) * sizeof(T));
   static int occupancy = 0;  // CTAs per SM, per instantiation
   if (occupancy == 0) {
-    OPSB_CUDA(cudaFuncSetAttribute(trid_warp_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    OPSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, trid_warp_kernel<T, R>, 32 * kWarpLines,
-                                                            smem));
+    OPSB_CUDA(cudaFuncSetAttribute(trid_warp_kernel<T, R, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    OPSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, trid_warp_kernel<T, R, FP>,
+                                                            32 * kWarpLines, smem));
     occupancy = std::max(occupancy, 1);
   }
   const int grid = std::min(nwork, 148 * occupancy);
-  trid_warp_kernel<T, R><<<grid, 32 * kWarpLines, smem, stream>>>(B.sys, B.work, nwork);
+  trid_warp_kernel<T, R, FP><<<grid, 32 * kWarpLines, smem, stream>>>(B.sys, B.work, nwork);
   OPSB_CUDA(cudaGetLastError());
 }
 
@@ -709,30 +733,27 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
   if (maxn == 0) return;
   if (launch_lines<T>(systems, stream, kernels)) return;
   bool contig = true;
-  long long nlines = 0, nunk = 0;
-  for (const Sys &s : systems) {
-    contig = contig && (s.n == 0 || s.ss == 1);
-    nlines += (long long)s.nl0 * s.nl1;
-    nunk += (long long)s.nl0 * s.nl1 * s.n;
-  }
-  // x sweeps of lines up to 256 rows averaging at least 160: one warp per
-  // line (trid_warp_kernel). A warp's per-line latency (staging, chunk
-  // sweeps, six reduction steps) is nearly independent of the length, so
-  // batches of short lines go to the tile kernel (256^3 FP64 x sweep 0.40 ->
-  // 0.28 ms; the 64-block batch with edges in [32, 192] would take 1.89 ms
-  // against the tile kernel's 1.38 ms).
+  for (const Sys &s : systems) contig = contig && (s.n == 0 || s.ss == 1);
+  // x sweeps of lines up to 256 rows: a warp per 1, 2 or 4 lines
+  // (trid_warp_kernel); longer lines, or the option set to 0, take the tile
+  // kernel
   const int wm = warp_mode();
-  const bool warp_path = contig && maxn <= 256 && (wm == 1 || (wm < 0 && nunk >= 160 * nlines));
-  // lines per work item: the largest power of two (<= 64) whose tiles fit
-  int L = warp_path ? kWarpLines : 64;
-  while (L > 1 && tile_smem<T>(L, maxn) > kTileSmem) L /= 2;
-  if (tile_smem<T>(L, maxn) > kTileSmem) throw Error(E_UNSUPPORTED, "tridiagonal lines longer than the tile budget");
+  const bool warp_path = contig && maxn <= 256 && wm != 0;
+  const int wR = maxn <= 128 ? 4 : 8;  // rows per lane of the warp kernel
+  // tile kernel: lines per work item, the largest power of two (<= 64) whose tiles fit
+  int L = 64;
+  if (!warp_path) {
+    while (L > 1 && tile_smem<T>(L, maxn) > kTileSmem) L /= 2;
+    if (tile_smem<T>(L, maxn) > kTileSmem) throw Error(E_UNSUPPORTED, "tridiagonal lines longer than the tile budget");
+  }
   std::vector<Work> work;
   for (int i = 0; i < (int)systems.size(); i++) {
     const Sys &s = systems[i];
     if (s.n == 0) continue;
+    // warp kernel: a CTA's warps take kWarpLines x (lines per warp) lines
+    const int Ls = warp_path ? kWarpLines * (32 / lanes_per_line(s.n, wR)) : L;
     for (int l1 = 0; l1 < s.nl1; l1++)
-      for (int l0 = 0; l0 < s.nl0; l0 += L) work.push_back({i, l0, l1});
+      for (int l0 = 0; l0 < s.nl0; l0 += Ls) work.push_back({i, l0, l1});
   }
   if (work.empty()) return;
   Buffers &B = buffers();
@@ -750,10 +771,12 @@ void launch(const std::vector<Sys> &systems, int solvedim, cudaStream_t stream, 
   OPSB_CUDA(cudaMemcpyAsync(B.work, work.data(), work.size() * sizeof(Work), cudaMemcpyHostToDevice, stream));
   const int nwork = (int)work.size();
   if (warp_path) {
-    if (maxn <= 128)
-      launch_warp<T, 4>(B, nwork, stream);
+    bool full = true;  // every line needs all 32 lanes
+    for (const Sys &s : systems) full = full && (s.n == 0 || lanes_per_line(s.n, wR) == 32);
+    if (wR == 4)
+      full ? launch_warp<T, 4, 32>(B, nwork, stream) : launch_warp<T, 4, 0>(B, nwork, stream);
     else
-      launch_warp<T, 8>(B, nwork, stream);
+      full ? launch_warp<T, 8, 32>(B, nwork, stream) : launch_warp<T, 8, 0>(B, nwork, stream);
     if (kernels) (*kernels)++;
     return;
   }
