@@ -1074,6 +1074,25 @@ def bench_learned(args, world, rank, local, pg):
             row[name] = {"iterations": st["iterations"], "seconds": st["seconds"], "fallbacks": st["fallbacks"]}
         small.append(row)
 
+    # the network's gain as the grid grows (one seeded field per size, rx 400,
+    # the middle of the training range): iterations and time of plain PCG and
+    # of the learned FCG on the same problem
+    sweep = []
+    for n_ in (64, 128, 256, 512, 1024):
+        r_, e_ = lmg.density_field(n_, 91000 + n_)
+        a, c, d = lmg.padded_problem(r_, e_)
+        skx, sky, sb = (torch.from_numpy(v).cuda(local) for v in (a, c, d))
+        row = {"n": n_}
+        for name, m in (("pcg", lmg.PCG_TRUE), ("learned_fcg", lmg.FCG_LEARNED)):
+            su = sb.clone()
+            lmg.solve(skx, sky, sb, su, 400.0, 400.0, method=m, net=net.h, eps=1e-10, window=40)  # untimed
+            su = sb.clone()
+            st = lmg.solve(skx, sky, sb, su, 400.0, 400.0, method=m, net=net.h, eps=1e-10, window=40)
+            row[name] = {"iterations": st["iterations"], "seconds": st["seconds"], "fallbacks": st["fallbacks"]}
+        row["iteration_ratio"] = row["learned_fcg"]["iterations"] / max(1, row["pcg"]["iterations"])
+        row["time_ratio"] = row["learned_fcg"]["seconds"] / max(1e-12, row["pcg"]["seconds"])
+        sweep.append(row)
+
     # e2e: Kx, Ky, u0 in from pinned host memory, one solve through the C-ABI,
     # the solution out to pinned host memory (buffers allocated before timing;
     # one untimed call first, as the timed solves above had)
@@ -1131,6 +1150,7 @@ def bench_learned(args, world, rank, local, pg):
                            "note": "M(r) = V-cycle(r) + the network's correction, trained on e - V-cycle(r)"},
         "training": {"seconds": train_s, "final_loss_per_round": [float(np.mean(h[-50:])) for h in hists]},
         "small_scale_gain_64x64_rx400": small,
+        "grid_sweep_rx400": sweep,
         "roofline": {"bound": "hbm", "achieved": conv_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": conv_gbs / peaks["hbm_gbs"], "traffic": None,
                      "kernel": "conv3x3_tc_kernel<16,16> (full-resolution layer)", "avg_launch_ms": conv_ms,

@@ -127,6 +127,29 @@ def test_learned_fcg_beats_jacobi_pcg(trained):
     assert sum(its_fcg) < 0.8 * sum(its_pcg), (its_fcg, its_pcg)
 
 
+@pytest.mark.parametrize("n", [256, 512])
+def test_learned_fcg_gain_beyond_the_training_size(trained, n):
+    """Trained on 64 x 64 fields, the network still cuts the iterations of the
+    heat solve on larger grids: fewer than half of Jacobi-PCG's at 256^2 and
+    512^2 (measured about a sixth and a fifth). Each application costs about
+    ten PCG iterations, so the wall time is not lower (bench.py --workload
+    learned, grid_sweep_rx400); at 1024^2 the gain falls to 1.6x and at
+    4096^2 it is gone."""
+    from ops_b200 import lmg
+    net, _ = trained
+    rho, en = lmg.density_field(n, 91000 + n)
+    Kx, Ky, u0 = lmg.padded_problem(rho, en)
+    kx, ky, b = cuda(Kx), cuda(Ky), cuda(u0)
+    u = b.clone()
+    sp = lmg.solve(kx, ky, b, u, 400.0, 400.0, method=lmg.PCG_TRUE, eps=1e-10)
+    u2 = b.clone()
+    sl = lmg.solve(kx, ky, b, u2, 400.0, 400.0, method=lmg.FCG_LEARNED, net=net.h, eps=1e-10, window=40)
+    for st in (sp, sl):
+        assert st["converged"] and st["final_residual"] < 1.5e-10 * st["initial_residual"]
+    assert rel(u2.cpu().numpy(), u.cpu().numpy()) < 1e-8
+    assert sl["iterations"] < 0.5 * sp["iterations"], (sl["iterations"], sp["iterations"])
+
+
 def test_untrained_learned_multigrid_is_the_vcycle(gpu_runtime):
     """FCG_LEARNED_MG applies V-cycle(r) + (network output - r / D); with the
     output layer at zero that is the V-cycle exactly, so the solve repeats
