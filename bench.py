@@ -613,9 +613,19 @@ def bench_adi(args, world, rank, local, pg):
     O.ops_init(local, 0)
     dt = np.float64 if args.precision == "fp64" else np.float32
     es = np.dtype(dt).itemsize
-    shapes = [(ADI_N,) * 3] if args.adi_case == "cube" else adi_batch_shapes()
+    all_shapes = [(ADI_N,) * 3] if args.adi_case == "cube" else adi_batch_shapes()
+    # the batch's blocks are independent units: over N GPUs each rank solves
+    # its share, assigned by cost (unknowns), with no collective; the 256^3
+    # cube runs as N replicas
+    shard = args.adi_case == "batch" and world > 1
+    owned = list(range(len(all_shapes)))
+    if shard:
+        from ops_b200.dist import assign_by_cost
+        owned = assign_by_cost([int(np.prod(s)) for s in all_shapes], world)[rank]
+    shapes = [all_shapes[i] for i in owned]
+    total_unknowns = sum(int(np.prod(s)) for s in all_shapes)
     sets = []
-    for i, shp in enumerate(shapes):
+    for i, shp in zip(owned, shapes):
         a, b, c, d = seeded.trid_system(shp, 0, 3 + i, dt)
         t = [torch.from_numpy(v).cuda(local) for v in (a, b, c, d)] + [torch.zeros(shp, dtype=torch.from_numpy(a).dtype,
                                                                                device=f"cuda:{local}")]
@@ -704,14 +714,16 @@ def bench_adi(args, world, rank, local, pg):
     h2d = sum(5 * int(np.prod(s)) * es for s, _ in host)
     name = f"adi_{args.adi_case}_{args.precision}"
     line = {
-        "metric": "cell-solves/s", "value": world * 3 * unknowns * K / secs, "unit": "unknowns solved/s",
+        "metric": "cell-solves/s", "value": (total_unknowns if shard else world * unknowns) * 3 * K / secs,
+        "unit": "unknowns solved/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": secs * 1e3 / K, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": args.precision.replace("fp", "f"),
+        "scaling": "strong" if shard else "weak", "vs_baseline": None, "dtype": args.precision.replace("fp", "f"),
         "data": "synthetic (a=c=-lam, b=1+2lam, lam~U[0.1,1] per line, d~N(0,1))",
-        "config": {"workload": name, "blocks": len(shapes), "unknowns": unknowns,
+        "config": {"workload": name, "blocks": len(all_shapes), "unknowns": total_unknowns,
                    "step": "x sweep + y sweep + z sweep (_Inc into u)", "l2": "inputs larger than L2"
                    if unknowns * es * 4 > 126e6 else "inputs fit in L2 (batch case)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": (f"{len(all_shapes)} blocks by cost over {world} GPUs (rank 0: {len(owned)})"
+                                   if shard else f"replicas x{world}")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "kernel": f"sweep {'xyz'[dom]}",
                      "traffic": TRAFFIC_PER_CELL["adi_cube_fp64"][dom] * unknowns
@@ -719,7 +731,8 @@ def bench_adi(args, world, rank, local, pg):
                      "traffic_source": "ncu capture of one x, y and z sweep at 256^3 FP64"
                                        " (profiles/adi_cube_256_fp64_dram.md); other cases not captured",
                      "sweep_ms": sweep_ms, "alg_bytes_per_unknown": byt, "peak_source": f"{peak_kind} hbm_gbs"},
-        "e2e": {"value": world * 3 * unknowns / e2e_s, "unit": "unknowns solved/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": (total_unknowns if shard else world * unknowns) * 3 / e2e_s, "unit": "unknowns solved/s",
+                "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": unknowns * es},
         "gpu_launches": launches, "clocks": clocks,
     }

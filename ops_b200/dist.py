@@ -129,3 +129,22 @@ def transport_selftest():
     """Exchange a pattern with the neighbours and gather the ranks through
     the library's transport path (no GPU); raises on a mismatch."""
     check(lib().ops_b200_transport_selftest())
+
+
+def assign_by_cost(costs, nparts):
+    """Independent work units (the blocks of a batched tridiagonal solve) over
+    `nparts` ranks by cost, longest first onto the least loaded rank (ties:
+    the lower rank, then the lower unit index), so every rank computes the
+    same assignment without communicating. Returns one ascending list of unit
+    indices per rank; the heaviest load is at most 4/3 of the optimum plus
+    one unit (Graham's bound for this rule)."""
+    if nparts < 1:
+        raise ValueError("nparts must be at least 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0] * nparts
+    parts = [[] for _ in range(nparts)]
+    for i in order:
+        r = min(range(nparts), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]

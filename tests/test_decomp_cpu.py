@@ -91,3 +91,23 @@ def test_host_transport_gloo(opsb_lib, world):
         assert res["nranks"] == world
         seen.add(res["rank"])
     assert seen == set(range(world))
+
+
+@pytest.mark.parametrize("nranks", [1, 2, 3, 4, 8])
+def test_tridiagonal_batch_blocks_by_cost(nranks):
+    """The 64 uneven blocks of the batched tridiagonal workload (edges
+    log-uniform in [32, 192]) go to ranks by cost, longest first onto the
+    least loaded: every block exactly once, the same answer on every call,
+    and the heaviest rank within Graham's LPT bound of the optimum."""
+    import numpy as np
+
+    import bench
+    from ops_b200.dist import assign_by_cost
+    costs = [int(np.prod(s)) for s in bench.adi_batch_shapes()]
+    parts = assign_by_cost(costs, nranks)
+    assert len(parts) == nranks
+    assert sorted(i for p in parts for i in p) == list(range(len(costs)))
+    assert parts == assign_by_cost(costs, nranks)
+    loads = [sum(costs[i] for i in p) for p in parts]
+    opt = max(sum(costs) / nranks, max(costs))
+    assert max(loads) <= (4.0 / 3.0 - 1.0 / (3 * nranks)) * opt + 1e-9 * opt
