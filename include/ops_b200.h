@@ -175,7 +175,11 @@ int ops_b200_dat_release_raw_data(int dat, int acc);
  * parity tests and profiling of the fused kernels.
  * "trid_warp": x sweeps of the batched tridiagonal solver with lines of at
  * most 256 rows run on the warp-per-lines kernel (-1, default, or 1) or on
- * the shared-memory tile kernel (0). */
+ * the shared-memory tile kernel (0).
+ * "fcg_chunks": the flexible-CG heat solves with the learned or the Jacobi
+ * preconditioner replay their iterations from CUDA graphs in chunks with the
+ * stopping and restart tests on the device (1, default) or run the host loop,
+ * one round trip per iteration (0); both give the same iterates. */
 int ops_b200_set_option(const char *name, int value);
 /* Counters since the last reset: kernels launched by this library, CUDA
  * graphs launched, loops queued. */

@@ -63,6 +63,7 @@ namespace opsb {
 namespace trid {
 void set_warp_mode(int m);
 }
+void set_fcg_chunks(int on);
 }  // namespace opsb
 
 extern "C" {
@@ -250,6 +251,7 @@ int ops_b200_set_option(const char *name, int value) {
     else if (n == "lists") rt().set_lists(value);
     else if (n == "tile_candidate") rt().set_tile_candidate(value);
     else if (n == "trid_warp") opsb::trid::set_warp_mode(value);
+    else if (n == "fcg_chunks") opsb::set_fcg_chunks(value);
     else throw opsb::Error(opsb::E_ARG, "unknown option " + n);
     return 0;
   });

@@ -151,6 +151,16 @@ lmg::Fields fields_of(const ops_b200_heat_batch *b) {
 }  // namespace
 }  // namespace opsb
 
+namespace opsb {
+// "fcg_chunks" option: replayed FCG chunks on (default) or the host loop.
+bool &fcg_chunks_flag() {
+  static bool on = true;
+  return on;
+}
+bool fcg_chunks_on() { return fcg_chunks_flag(); }
+void set_fcg_chunks(int on) { fcg_chunks_flag() = on != 0; }
+}  // namespace opsb
+
 extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, double eps, int max_iters,
                                    int window, double *r_out, ops_b200_heat_stats *stats, void *stream) {
   using namespace opsb;
@@ -234,7 +244,13 @@ extern "C" int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, 
         mg->setup(sys->nx, sys->ny, sys->pitch, sys->Kx, sys->Ky, sys->rx, sys->ry, s);
         M = [mg](const double *r, double *z, cudaStream_t ss) -> long long { return mg->apply(r, z, ss); };
       }
-      ws.solver.fcg(f, sys->rx, sys->ry, eps, max_iters, M, window, s, &st, fallback ? &fallback : nullptr);
+      // the network's application and Jacobi are plain kernel launches, so
+      // those solves replay their iterations from graphs; the multigrid
+      // variants launch the V-cycle's own graph and keep the host loop
+      const bool chunked =
+          fcg_chunks_on() && (method == OPS_B200_HEAT_FCG_LEARNED || method == OPS_B200_HEAT_FCG_JACOBI);
+      ws.solver.fcg(f, sys->rx, sys->ry, eps, max_iters, M, window, s, &st, fallback ? &fallback : nullptr,
+                    chunked);
     }
     OPSB_CUDA(cudaEventRecord(e1, s));
     OPSB_CUDA(cudaEventSynchronize(e1));

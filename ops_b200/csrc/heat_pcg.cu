@@ -37,10 +37,15 @@ constexpr int kTargetBlocks = 148 * kResident;
 struct Scalars {
   double rro, rro_prev, pw, alpha, beta;
   double err, stop, ref, rr, rr0;
-  int done;       // 0 running, 1 converged, 2 iteration limit, 3 reliable update due
+  int done;       // 0 running, 1 converged, 2 iteration limit, 3 reliable update due,
+                  // 4 FCG lost positive curvature, 5 FCG restart (||r|| not halved over the window)
   int iters;
   int max_iters;
   int first;
+  // FCG restart test on the device (replayed chunks): ||r|| of the last
+  // iterations since the last (re)start, `window` 0 when the test is off
+  int window, hcount;
+  double hist[64];
 };
 
 // Stopping quantity of k_ur.
@@ -392,6 +397,12 @@ __global__ void __launch_bounds__(NT, kResident) k_fupd(Geom g, double *__restri
       s->iters = s->iters + 1;
       if (s->err < s->stop) s->done = 1;
       else if (s->iters >= s->max_iters) s->done = 2;
+      if (s->done == 0 && s->window > 0) {  // the same test the host loop applies
+        const int k = s->hcount;
+        s->hist[k & 63] = s->err;
+        s->hcount = k + 1;
+        if (k + 1 > s->window && s->err > 0.5 * s->hist[(k - s->window) & 63]) s->done = 5;
+      }
       *cnt = 0u;
     }
   }
@@ -402,6 +413,7 @@ __global__ void __launch_bounds__(NT, kResident) k_fzw(Geom g, const double *__r
                                             Scalars *s, double *part, unsigned *cnt) {
   __shared__ double sm[kWarps];
   __shared__ int last;
+  if (s->done) return;  // the solve stopped earlier in a replayed chunk
   double acc[1] = {0.0};
   HEAT_CELLS(g) {
     const long long i = (long long)y * g.pitch + x;
@@ -419,6 +431,7 @@ __global__ void __launch_bounds__(NT, kResident) k_fzw(Geom g, const double *__r
 // p = z + beta p, or p = z on a restart.
 __global__ void __launch_bounds__(NT, kResident) k_fp(Geom g, double *__restrict__ p, const double *__restrict__ z,
                                            const Scalars *s, int restart) {
+  if (!restart && s->done) return;  // the solve stopped earlier in a replayed chunk
   const double beta = restart ? 0.0 : s->beta;
   HEAT_CELLS(g) {
     const long long i = (long long)y * g.pitch + x;
@@ -762,7 +775,7 @@ double Solver::residual(const Field2D &f, double rx, double ry, double *outp, cu
 }
 
 void Solver::fcg(const Field2D &f, double rx, double ry, double eps, int max_iters, const Precond &M, int window,
-                 cudaStream_t st, SolveStats *out, const Precond *fallback) {
+                 cudaStream_t st, SolveStats *out, const Precond *fallback, bool chunked) {
   validate(f);
   Impl &m = *m_;
   m.ensure_base();
@@ -798,8 +811,65 @@ void Solver::fcg(const Field2D &f, double rx, double ry, double eps, int max_ite
     k_fp<<<grid, block, 0, st>>>(g, f.p, f.z, m.s64, 1);
     launches_ += 1;
   }
+  bool host_loop = true;
+  if (chunked && window < 64 && !done) {
+    host_loop = false;
+    // Replayed chunks of kFcgChunk iterations (w = A p, update, precondition,
+    // beta, direction); the device stops them (done != 0) and the host reads
+    // the flag one chunk behind. A restart (done 4 or 5) falls back to the
+    // Jacobi (or fallback) preconditioner and continues with that chunk.
+    // The graphs hold this call's pointers and are rebuilt per call.
+    constexpr int kFcgChunk = 4;
+    int set[2] = {learned ? window : 0, 0};
+    OPSB_CUDA(cudaMemcpyAsync(&m.s64->window, set, sizeof(set), cudaMemcpyHostToDevice, st));
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // learned, fallback
+    long long per_chunk[2] = {0, 0};
+    try {
+      while (!done) {
+        const int which = learned ? 0 : 1;
+        if (!graphs[which]) {
+          const long long before = launches_;
+          graphs[which] = capture(st, [&] {
+            for (int it = 0; it < kFcgChunk; it++) {
+              k_fw<<<grid, block, 0, st>>>(g, f.Kx, f.Ky, f.p, f.r, f.w, rx, ry, m.s64, m.part, m.cnt);
+              k_fupd<<<grid, block, 0, st>>>(g, f.u, f.p, f.r, f.w, m.s64, m.part, m.cnt);
+              launches_ += 2;
+              precond();
+              k_fzw<<<grid, block, 0, st>>>(g, f.z, f.w, m.s64, m.part, m.cnt);
+              k_fp<<<grid, block, 0, st>>>(g, f.p, f.z, m.s64, 0);
+              launches_ += 2;
+            }
+          });
+          per_chunk[which] = launches_ - before;
+          launches_ = before;
+        }
+        // run_chunks stops after (its bound) / kChunk + 2 chunks at most; the
+        // device stops them first (done 2 at max_iters)
+        launches_ += run_chunks(graphs[which], m.s64, (max_iters / kFcgChunk + 2) * kChunk, m.h_flag, m.ev, st,
+                                per_chunk[which]);
+        OPSB_CUDA(cudaMemcpyAsync(&h, m.s64, sizeof(h), cudaMemcpyDeviceToHost, st));
+        OPSB_CUDA(cudaStreamSynchronize(st));
+        if (h.done == 1 || h.done == 2 || h.done == 0) break;
+        // done 4 (lost curvature) or 5 (not halved over the window): restart
+        if (learned) out->fallbacks++;
+        learned = false;
+        const int zero3[3] = {0, 0, 0};  // done = 0; window = hcount = 0 (no restart test on the fallback)
+        OPSB_CUDA(cudaMemcpyAsync(&m.s64->done, zero3, sizeof(int), cudaMemcpyHostToDevice, st));
+        OPSB_CUDA(cudaMemcpyAsync(&m.s64->window, zero3 + 1, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+        precond();
+        k_fp<<<grid, block, 0, st>>>(g, f.p, f.z, m.s64, 1);
+        launches_ += 1;
+      }
+    } catch (...) {
+      for (cudaGraphExec_t x : graphs)
+        if (x) cudaGraphExecDestroy(x);
+      throw;
+    }
+    for (cudaGraphExec_t x : graphs)
+      if (x) cudaGraphExecDestroy(x);
+  }
   std::vector<double> hist;
-  while (!done) {
+  while (!done && host_loop) {
     k_fw<<<grid, block, 0, st>>>(g, f.Kx, f.Ky, f.p, f.r, f.w, rx, ry, m.s64, m.part, m.cnt);
     k_fupd<<<grid, block, 0, st>>>(g, f.u, f.p, f.r, f.w, m.s64, m.part, m.cnt);
     check_launch("fcg iteration");

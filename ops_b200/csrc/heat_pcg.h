@@ -63,8 +63,13 @@ class Solver {
   // On a restart (p.w <= 0, or no halving of ||r|| over `window`
   // iterations) the solve continues with `fallback` when one is given, else
   // with Jacobi.
+  // With `chunked`, M (and the fallback) must be stream-capturable (kernel
+  // launches and memsets only, after one call outside capture): iterations
+  // are then replayed from CUDA graphs in chunks, with the stopping and
+  // restart tests on the device and the host polling one chunk behind;
+  // iteration counts and results are those of the host loop.
   void fcg(const Field2D &f, double rx, double ry, double eps, int max_iters, const Precond &M, int window,
-           cudaStream_t s, SolveStats *st, const Precond *fallback = nullptr);
+           cudaStream_t s, SolveStats *st, const Precond *fallback = nullptr, bool chunked = false);
   // Mi = 1 / diag(A) on the interior (tea_leaf_common_init_diag_init_kernel).
   void diag(const Field2D &f, double rx, double ry, cudaStream_t s);
   // out = u0 - A u on the interior; returns ||out||.

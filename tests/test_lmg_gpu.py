@@ -150,6 +150,34 @@ def test_learned_fcg_gain_beyond_the_training_size(trained, n):
     assert sl["iterations"] < 0.5 * sp["iterations"], (sl["iterations"], sp["iterations"])
 
 
+@pytest.mark.parametrize("n", [64, 256])
+def test_replayed_fcg_chunks_match_the_host_loop(trained, n):
+    """The learned and Jacobi flexible-CG solves run their iterations from
+    replayed graph chunks (stopping and restart tests on the device); with the
+    option off they run the host loop. Same iterations, same restarts, and
+    the same solution bit for bit."""
+    from ops_b200 import lmg
+    from ops_b200 import ops as O
+    net, _ = trained
+    rho, en = lmg.density_field(n, 91000 + n)
+    Kx, Ky, u0 = lmg.padded_problem(rho, en)
+    kx, ky, b = cuda(Kx), cuda(Ky), cuda(u0)
+    for method, h in ((lmg.FCG_LEARNED, net.h), (lmg.FCG_JACOBI, -1)):
+        out = {}
+        for chunks in (1, 0):
+            O.set_option("fcg_chunks", chunks)
+            try:
+                u = b.clone()
+                st = lmg.solve(kx, ky, b, u, 400.0, 400.0, method=method, net=h, eps=1e-10, window=40)
+            finally:
+                O.set_option("fcg_chunks", 1)
+            out[chunks] = (st, u.cpu().numpy())
+        (s1, u1), (s0, u0_) = out[1], out[0]
+        assert s1["converged"] and s0["converged"]
+        assert (s1["iterations"], s1["fallbacks"]) == (s0["iterations"], s0["fallbacks"]), (method, s1, s0)
+        assert np.array_equal(u1, u0_), method
+
+
 def test_untrained_learned_multigrid_is_the_vcycle(gpu_runtime):
     """FCG_LEARNED_MG applies V-cycle(r) + (network output - r / D); with the
     output layer at zero that is the V-cycle exactly, so the solve repeats
