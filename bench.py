@@ -1290,10 +1290,137 @@ def bench_mg(args, world, rank, local, pg):
     return line
 
 
+# ---------------------------------------------------------------------------
+# 3D heat solve: the 7-point operator at 512^3, FP64 Jacobi-PCG to 1e-10
+# ---------------------------------------------------------------------------
+H3_N = 512
+HEAT3D_BYTES = 128.0  # FP64 per cell-iteration: w = A p (p, Kx, Ky, Kz, w: 40) + u, r, z updates (64) + p (24)
+
+
+def heat3d_problem(n, seed, local):
+    """16 seeded boxes of density log-uniform in [0.1, 100] over rho = 1 and
+    energy U[0, 1] (the 2D heat configuration's recipe in 3D); face
+    conductivities as ops_b200.lmg.faces3d, built on the device."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    dev = f"cuda:{local}"
+    rho = torch.ones((n, n, n), dtype=torch.float64, device=dev)
+    for _ in range(16):
+        lo = rng.integers(0, n - 1, 3)
+        hi = np.minimum(n, lo + rng.integers(n // 16, n // 3, 3))
+        rho[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = float(np.exp(rng.uniform(np.log(0.1), np.log(100.0))))
+    g = torch.Generator(device=dev).manual_seed(seed)
+    en = torch.rand((n, n, n), dtype=torch.float64, device=dev, generator=g)
+    shape = (n + 2, n + 2, n + 2)
+    Kx, Ky, Kz, u0 = (torch.zeros(shape, dtype=torch.float64, device=dev) for _ in range(4))
+    w = rho
+    Kx[1:-1, 1:-1, 2:-1] = (w[:, :, :-1] + w[:, :, 1:]) / (2.0 * w[:, :, :-1] * w[:, :, 1:])
+    Ky[1:-1, 2:-1, 1:-1] = (w[:, :-1, :] + w[:, 1:, :]) / (2.0 * w[:, :-1, :] * w[:, 1:, :])
+    Kz[2:-1, 1:-1, 1:-1] = (w[:-1, :, :] + w[1:, :, :]) / (2.0 * w[:-1, :, :] * w[1:, :, :])
+    u0[1:-1, 1:-1, 1:-1] = en * rho
+    del rho, en
+    return Kx, Ky, Kz, u0
+
+
+def bench_heat3d(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    from ops_b200 import lmg
+    from ops_b200 import ops as O
+
+    peaks, peak_kind = load_peaks()
+    O.ops_init(local, 0)
+    N = args.grid or H3_N
+    cells = N ** 3
+    rxyz = 100.0
+    Kx, Ky, Kz, u0 = heat3d_problem(N, 6, local)
+    u = torch.empty_like(u0)
+    K, W = args.steps, args.warmup
+    barrier(pg, local)
+    times, stats = [], None
+    with ClockSampler(local) as cs:
+        for it in range(W + K):
+            u.copy_(u0)
+            st = lmg.solve3d(Kx, Ky, Kz, u0, u, rxyz, rxyz, rxyz, method=lmg.PCG_TRUE, eps=1e-10)
+            if it >= W:
+                times.append(st["seconds"])
+                stats = st
+    clocks = cs.summary()
+    t = max_over_ranks(pg, float(np.median(times)), local)
+    iters = stats["iterations"]
+    achieved = HEAT3D_BYTES * cells * iters / t / 1e9
+    # e2e: Kx, Ky, Kz, u0 in from pinned host memory, one solve through the
+    # C-ABI, u out to pinned host memory (buffers allocated before timing)
+    hk = [x.cpu().pin_memory() for x in (Kx, Ky, Kz, u0)]
+    hu = torch.empty_like(hk[3]).pin_memory()
+    barrier(pg, local)
+    torch.cuda.synchronize(local)
+    te0 = time.perf_counter()
+    for d_, h_ in zip((Kx, Ky, Kz, u0), hk):
+        d_.copy_(h_, non_blocking=True)
+    u.copy_(u0)
+    lmg.solve3d(Kx, Ky, Kz, u0, u, rxyz, rxyz, rxyz, method=lmg.PCG_TRUE, eps=1e-10)
+    hu.copy_(u, non_blocking=True)
+    torch.cuda.synchronize(local)
+    e2e_s = max_over_ranks(pg, time.perf_counter() - te0, local)
+    line = {
+        "metric": "time to 1e-10 residual", "value": t, "unit": "s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (rho=1 background + 16 seeded boxes, rho log-uniform [0.1,100], energy U[0,1], seed 6)",
+        "config": {"workload": f"heat3d_pcg_{N}^3", "grid": [N, N, N], "rx=ry=rz": rxyz, "eps": 1e-10,
+                   "step": "one FP64 Jacobi-PCG solve of the 7-point operator to ||u0 - A u|| < 1e-10 ||r0||",
+                   "l2": "inputs larger than L2 (fields of 1.09 GB)", "parallelism": f"replicas x{world}"},
+        "iterations": iters, "final_residual_ratio": stats["final_residual"] / max(stats["initial_residual"], 1e-300),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "kernel": "PCG iteration (k_w3 + k_ur + k_p)", "alg_bytes_per_cell_iteration": HEAT3D_BYTES,
+                     "avg_iteration_ms": t * 1e3 / max(iters, 1), "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": sum(h.numel() * 8 for h in hk),
+                "d2h_bytes_per_step": hu.numel() * 8},
+        "gpu_launches": int(stats["launches"]), "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the same iteration in numpy on a 96^3 sample, one core (no 3D reference exists)
+        n_ = 96
+        rng = np.random.default_rng(7)
+        sh = (n_ + 2,) * 3
+        A = [np.zeros(sh) for _ in range(5)]
+        for a in A:
+            a[1:-1, 1:-1, 1:-1] = rng.uniform(0.1, 1.0, (n_,) * 3)
+        kx, ky, kz, p_, r_ = A
+        c = (slice(1, -1),) * 3
+        nit = 10
+        t0 = time.perf_counter()
+        for _ in range(nit):
+            w_ = np.zeros(sh)
+            w_[c] = ((1.0 + rxyz * (kz[2:, 1:-1, 1:-1] + kz[c] + ky[1:-1, 2:, 1:-1] + ky[c]
+                                    + kx[1:-1, 1:-1, 2:] + kx[c])) * p_[c]
+                     - rxyz * (kz[2:, 1:-1, 1:-1] * p_[2:, 1:-1, 1:-1] + kz[c] * p_[:-2, 1:-1, 1:-1])
+                     - rxyz * (ky[1:-1, 2:, 1:-1] * p_[1:-1, 2:, 1:-1] + ky[c] * p_[1:-1, :-2, 1:-1])
+                     - rxyz * (kx[1:-1, 1:-1, 2:] * p_[1:-1, 1:-1, 2:] + kx[c] * p_[1:-1, 1:-1, :-2]))
+            al = np.sum(r_ * r_) / max(np.sum(p_ * w_), 1e-300)
+            r_ -= al * w_
+            z_ = r_ / (1.0 + 6.0 * rxyz)
+            p_ = z_ + 0.5 * p_
+        secs = (time.perf_counter() - t0) / nit
+        line["cpu_baseline"] = {"value": n_ ** 3 / secs, "unit": "cell-iterations/s", "cores": 1, "kind": "port",
+                                "sample": f"{nit} iterations of the same 7-point PCG step in numpy on a {n_}^3 sample, one core"
+                                          " (no 3D reference exists)",
+                                "est_time_to_solution_s": iters * cells * secs / n_ ** 3}
+    return line
+
+
+def reference_heat3d(args, world, rank):
+    return {"impl": "reference", "unavailable": "the reference has no 3D heat solve (OPS TeaLeaf is 2D)"}
+
+
 WORKLOADS = {"laplace": (bench_laplace, reference_laplace), "clover": (bench_clover, reference_clover),
              "clover3d": (bench_clover3d, reference_clover3d),
              "adi": (bench_adi, reference_adi), "tea": (bench_tea, reference_tea),
-             "learned": (bench_learned, reference_tea), "mg": (bench_mg, reference_tea)}
+             "learned": (bench_learned, reference_tea), "mg": (bench_mg, reference_tea),
+             "heat3d": (bench_heat3d, reference_heat3d)}
 
 
 def main():
@@ -1318,7 +1445,7 @@ def main():
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"laplace": 200, "clover": 200, "clover3d": 100, "adi": 50, "tea": 3,
-                      "learned": 2, "mg": 10}.get(args.workload, 20)
+                      "learned": 2, "mg": 10, "heat3d": 2}.get(args.workload, 20)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_setup(args)

@@ -538,6 +538,24 @@ typedef struct ops_b200_heat_stats {
 int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, double eps, int max_iters, int window,
                         double *r_out, ops_b200_heat_stats *stats, void *stream);
 
+/* The 3D 7-point heat operator (the 512^3 case of the heat solve; no
+ * reference counterpart: OPS TeaLeaf is 2D): A u = (1 + rx (Kx + Kx+x) +
+ * ry (Ky + Ky+y) + rz (Kz + Kz+z)) u - rx (Kx+x u+x + Kx u-x) - ... with
+ * face conductivities K (Kz(x,y,z) the face between z-1 and z). Pointers
+ * address the first interior cell of FP64 volumes with one halo cell on
+ * each side; plane == pitch * (ny + 2). Methods OPS_B200_HEAT_PCG and
+ * OPS_B200_HEAT_PCG_TRUE (FP64 Jacobi-PCG, device-resident iterations).
+ * Synchronous on `stream`; not reentrant (a workspace is kept per size). */
+typedef struct ops_b200_heat_system3d {
+  int nx, ny, nz;
+  long long pitch, plane;
+  const double *Kx, *Ky, *Kz, *u0;
+  double *u;
+  double rx, ry, rz;
+} ops_b200_heat_system3d;
+int ops_b200_heat_solve3d(const ops_b200_heat_system3d *sys, int method, double eps, int max_iters,
+                          ops_b200_heat_stats *stats, void *stream);
+
 /* Native multigrid preconditioner of method 5: z = M r, one FP32 V-cycle
  * over a hierarchy of 2 x 2 aggregates (coarse mass = sum of the aggregate's,
  * coarse face weight = half the sum of the fine faces it covers, coarsening

@@ -110,6 +110,13 @@ class HeatSystem(ctypes.Structure):
                 ("rx", ctypes.c_double), ("ry", ctypes.c_double)]
 
 
+class HeatSystem3D(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("pitch", ctypes.c_longlong),
+                ("plane", ctypes.c_longlong), ("Kx", ctypes.c_void_p), ("Ky", ctypes.c_void_p),
+                ("Kz", ctypes.c_void_p), ("u0", ctypes.c_void_p), ("u", ctypes.c_void_p), ("rx", ctypes.c_double),
+                ("ry", ctypes.c_double), ("rz", ctypes.c_double)]
+
+
 class HeatStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("updates", ctypes.c_int), ("converged", ctypes.c_int),
                 ("fallbacks", ctypes.c_int), ("initial_residual", ctypes.c_double),
@@ -203,6 +210,7 @@ def _declare(L):
         "ops_b200_trid_batch": ([i, i, i, P, P], i),
         "ops_b200_conv3x3_bf16": ([P, P, P, P, P, i, i, i, i, i, i, P], i),
         "ops_b200_heat_solve": ([P, i, i, ctypes.c_double, i, i, P, P, P], i),
+        "ops_b200_heat_solve3d": ([P, i, ctypes.c_double, i, P, P], i),
         "ops_b200_heat_mg_apply": ([P, P, P, P, P], i),
         "ops_b200_lmg_create": ([ctypes.c_ulonglong], i),
         "ops_b200_lmg_destroy": ([i], i),

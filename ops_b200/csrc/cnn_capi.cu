@@ -152,6 +152,38 @@ lmg::Fields fields_of(const ops_b200_heat_batch *b) {
 }  // namespace opsb
 
 namespace opsb {
+namespace {
+// The 3D solver's own fields (zero on every halo cell), kept per size.
+struct Heat3DWorkspace {
+  int nx = 0, ny = 0, nz = 0;
+  long long pitch = 0;
+  double *buf = nullptr;
+  double *r = nullptr, *w = nullptr, *p = nullptr, *z = nullptr, *Mi = nullptr;
+  heat::Solver solver;
+  ~Heat3DWorkspace() { cudaFree(buf); }
+  void ensure(int x, int y, int zz, long long pt, cudaStream_t s) {
+    if (x == nx && y == ny && zz == nz && pt == pitch && buf) return;
+    cudaFree(buf);
+    buf = nullptr;
+    nx = ny = nz = 0;
+    const size_t one = (size_t)pt * (y + 2) * (zz + 2);
+    OPSB_CUDA(cudaMalloc(&buf, 5 * one * sizeof(double)));
+    OPSB_CUDA(cudaMemsetAsync(buf, 0, 5 * one * sizeof(double), s));
+    const size_t first = (size_t)pt * (y + 2) + pt + 1;
+    double **f[5] = {&r, &w, &p, &z, &Mi};
+    for (int k = 0; k < 5; k++) *f[k] = buf + k * one + first;
+    nx = x;
+    ny = y;
+    nz = zz;
+    pitch = pt;
+  }
+};
+Heat3DWorkspace &workspace3d() {
+  static Heat3DWorkspace w;
+  return w;
+}
+}  // namespace
+
 // "fcg_chunks" option: replayed FCG chunks on (default) or the host loop.
 bool &fcg_chunks_flag() {
   static bool on = true;
@@ -373,6 +405,69 @@ extern "C" int ops_b200_lmg_train_step(int net, const ops_b200_heat_batch *b, co
     if (lr > 0.0) nt.adam(lr, s);
     OPSB_CUDA(cudaStreamSynchronize(s));
     if (loss) *loss = L;
+    return 0;
+  });
+}
+
+extern "C" int ops_b200_heat_solve3d(const ops_b200_heat_system3d *sys, int method, double eps, int max_iters,
+                                     ops_b200_heat_stats *stats, void *stream) {
+  using namespace opsb;
+  return capi_guard([&] {
+    if (!sys || !sys->Kx || !sys->Ky || !sys->Kz || !sys->u0 || !sys->u) throw Error(E_ARG, "heat system 3D: null field");
+    if (sys->nx < 1 || sys->ny < 1 || sys->nz < 1 || sys->pitch < sys->nx + 2 || sys->plane != sys->pitch * (sys->ny + 2))
+      throw Error(E_ARG, "heat system 3D: bad shape (pitch >= nx + 2, plane == pitch * (ny + 2))");
+    if (method != OPS_B200_HEAT_PCG && method != OPS_B200_HEAT_PCG_TRUE)
+      throw Error(E_ARG, "heat system 3D: methods OPS_B200_HEAT_PCG and OPS_B200_HEAT_PCG_TRUE");
+    if (!(eps > 0.0) || max_iters < 0) throw Error(E_ARG, "heat system 3D: eps > 0 and max_iters >= 0 required");
+    std::lock_guard<std::mutex> lk(g_mu);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!s) s = own_stream();
+    Heat3DWorkspace &ws = workspace3d();
+    ws.ensure(sys->nx, sys->ny, sys->nz, sys->pitch, s);
+    heat::Field3D f;
+    f.nx = sys->nx;
+    f.ny = sys->ny;
+    f.nz = sys->nz;
+    f.pitch = sys->pitch;
+    f.plane = sys->plane;
+    f.Kx = sys->Kx;
+    f.Ky = sys->Ky;
+    f.Kz = sys->Kz;
+    f.u0 = sys->u0;
+    f.u = sys->u;
+    f.r = ws.r;
+    f.w = ws.w;
+    f.p = ws.p;
+    f.z = ws.z;
+    f.Mi = ws.Mi;
+    ws.solver.diag3(f, sys->rx, sys->ry, sys->rz, s);
+    heat::SolveStats st;
+    cudaEvent_t e0, e1;
+    OPSB_CUDA(cudaEventCreate(&e0));
+    OPSB_CUDA(cudaEventCreate(&e1));
+    OPSB_CUDA(cudaEventRecord(e0, s));
+    try {
+      ws.solver.pcg3d(f, sys->rx, sys->ry, sys->rz, method == OPS_B200_HEAT_PCG_TRUE, eps, max_iters, s, &st);
+      OPSB_CUDA(cudaEventRecord(e1, s));
+      OPSB_CUDA(cudaEventSynchronize(e1));
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+      memset(stats, 0, sizeof(*stats));
+      stats->iterations = st.iterations;
+      stats->converged = st.converged;
+      stats->initial_residual = st.initial_residual;
+      stats->final_residual = st.true_residual;
+      stats->seconds = ms * 1e-3;
+      stats->launches = ws.solver.launches();
+    }
     return 0;
   });
 }

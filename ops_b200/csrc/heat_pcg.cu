@@ -458,6 +458,108 @@ __global__ void __launch_bounds__(NT, kResident) k_diag(Geom g, const double *__
   }
 }
 
+// ---- 3D: the 7-point heat operator ------------------------------------------
+// Interior cells (x, y, z) at i = z * plane + y * pitch + x from the first
+// interior cell; Kz[i] is the face between z-1 and z (as Kx, Ky in 2D).
+// The pointwise CG kernels run on the padded volume as a flat array (the
+// solver's own fields are zero on every halo cell), so only the operator,
+// the residual and the diagonal need these.
+struct Geom3 {
+  int nx, ny, nz;
+  long long pitch, plane;
+};
+
+#define HEAT_CELLS3(g)                                                                                        \
+  for (int row = blockIdx.y * BY + threadIdx.y, y = row % (g).ny, z = row / (g).ny; row < (g).ny * (g).nz;   \
+       row += gridDim.y * BY, y = row % (g).ny, z = row / (g).ny)                                            \
+    for (int x = blockIdx.x * BX + threadIdx.x; x < (g).nx; x += gridDim.x * BX)
+
+__device__ __forceinline__ double smvp3(const double *__restrict__ Kx, const double *__restrict__ Ky,
+                                        const double *__restrict__ Kz, const double *__restrict__ u, long long i,
+                                        long long P, long long Q, double rx, double ry, double rz) {
+  const double kx0 = Kx[i], kx1 = Kx[i + 1], ky0 = Ky[i], ky1 = Ky[i + P], kz0 = Kz[i], kz1 = Kz[i + Q];
+  return (1.0 + rz * (kz1 + kz0) + ry * (ky1 + ky0) + rx * (kx1 + kx0)) * u[i] - rz * (kz1 * u[i + Q] + kz0 * u[i - Q]) -
+         ry * (ky1 * u[i + P] + ky0 * u[i - P]) - rx * (kx1 * u[i + 1] + kx0 * u[i - 1]);
+}
+
+// w = A p on the interior, pw = p.w -> alpha = rro / pw (k_w in 3D).
+__global__ void __launch_bounds__(NT, kResident) k_w3(Geom3 g, const double *__restrict__ Kx,
+                                                     const double *__restrict__ Ky, const double *__restrict__ Kz,
+                                                     const double *__restrict__ p, double *__restrict__ w, double rx,
+                                                     double ry, double rz, Scalars *s, double *part, unsigned *cnt) {
+  __shared__ double sm[kWarps];
+  __shared__ int last;
+  if (s->done) return;
+  double acc[1] = {0.0};
+  HEAT_CELLS3(g) {
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    const double wv = smvp3(Kx, Ky, Kz, p, i, g.pitch, g.plane, rx, ry, rz);
+    w[i] = wv;
+    acc[0] = acc[0] + wv * p[i];
+  }
+  if (publish<1>(acc, part, cnt, sm, &last)) {
+    const double t = grid_total<1>(part, 0, sm);
+    if (tid_() == 0) {
+      s->pw = t;
+      s->alpha = s->rro / t;
+      *cnt = 0u;
+    }
+  }
+}
+
+// r = u0 - A u, rr = r.r; the first call of a solve fixes ||r0|| and the stop
+// threshold (k_resid in 3D).
+__global__ void __launch_bounds__(NT, kResident) k_resid3(Geom3 g, const double *__restrict__ Kx,
+                                                         const double *__restrict__ Ky, const double *__restrict__ Kz,
+                                                         const double *__restrict__ u, const double *__restrict__ u0,
+                                                         double *__restrict__ r, double rx, double ry, double rz,
+                                                         double eps, Scalars *s, double *part, unsigned *cnt) {
+  __shared__ double sm[kWarps];
+  __shared__ int last;
+  double acc[1] = {0.0};
+  HEAT_CELLS3(g) {
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    const double rv = u0[i] - smvp3(Kx, Ky, Kz, u, i, g.pitch, g.plane, rx, ry, rz);
+    r[i] = rv;
+    acc[0] = acc[0] + rv * rv;
+  }
+  if (publish<1>(acc, part, cnt, sm, &last)) {
+    const double t = grid_total<1>(part, 0, sm);
+    if (tid_() == 0) {
+      s->rr = t;
+      const double nrm = sqrt(fabs(t));
+      if (s->first) {
+        s->rr0 = t;
+        s->stop = eps * nrm;
+        s->first = 0;
+      }
+      s->err = nrm;
+      s->done = (fabs(nrm) < s->stop) ? 1 : 0;
+      *cnt = 0u;
+    }
+  }
+}
+
+// Mi = 1 / diag(A) on the interior.
+__global__ void __launch_bounds__(NT, kResident) k_diag3(Geom3 g, const double *__restrict__ Kx,
+                                                        const double *__restrict__ Ky, const double *__restrict__ Kz,
+                                                        double rx, double ry, double rz, double *__restrict__ Mi) {
+  HEAT_CELLS3(g) {
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    Mi[i] = 1.0 / (1.0 + rz * (Kz[i + g.plane] + Kz[i]) + ry * (Ky[i + g.pitch] + Ky[i]) + rx * (Kx[i + 1] + Kx[i]));
+  }
+}
+
+dim3 grid_for3(int nx, int rows) {
+  int gx = (nx + BX - 1) / BX;
+  if (gx > 1024) gx = 1024;
+  int gy = kTargetBlocks / gx;
+  const int r = (rows + BY - 1) / BY;
+  if (gy > r) gy = r;
+  if (gy < 1) gy = 1;
+  return dim3(gx, gy);
+}
+
 void check_launch(const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw Error(E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -753,6 +855,85 @@ void Solver::pcg_mixed(const Field2D &f, double rx, double ry, bool precond, dou
   out->true_residual = h.err;
 }
 
+
+namespace {
+void validate3(const Field3D &f) {
+  if (f.nx < 1 || f.ny < 1 || f.nz < 1) throw Error(E_ARG, "heat solver 3D: empty interior");
+  if (f.pitch < f.nx + 2 || f.plane != f.pitch * (f.ny + 2))
+    throw Error(E_ARG, "heat solver 3D: pitch >= nx + 2 and plane == pitch * (ny + 2) required");
+  if (!f.Kx || !f.Ky || !f.Kz || !f.u0 || !f.u || !f.r || !f.w || !f.p || !f.z || !f.Mi)
+    throw Error(E_ARG, "heat solver 3D: null field");
+  if ((long long)(f.ny + 2) * (f.nz + 2) > (1LL << 30) || f.plane * (f.nz + 2) > (1LL << 40))
+    throw Error(E_ARG, "heat solver 3D: field too large");
+}
+}  // namespace
+
+void Solver::diag3(const Field3D &f, double rx, double ry, double rz, cudaStream_t st) {
+  validate3(f);
+  k_diag3<<<grid_for3(f.nx, f.ny * f.nz), dim3(BX, BY), 0, st>>>(Geom3{f.nx, f.ny, f.nz, f.pitch, f.plane}, f.Kx,
+                                                                   f.Ky, f.Kz, rx, ry, rz, f.Mi);
+  check_launch("heat solver 3D diagonal");
+}
+
+void Solver::pcg3d(const Field3D &f, double rx, double ry, double rz, bool true_stop, double eps, int max_iters,
+                   cudaStream_t st, SolveStats *out) {
+  validate3(f);
+  Impl &m = *m_;
+  m.ensure_base();
+  launches_ = 0;
+  const Geom3 g{f.nx, f.ny, f.nz, f.pitch, f.plane};
+  const dim3 grid3 = grid_for3(f.nx, f.ny * f.nz), block(BX, BY);
+  // the pointwise kernels see the padded volume as rows of `pitch`
+  const long long off = f.plane + f.pitch + 1;
+  const int rows = (f.ny + 2) * (f.nz + 2);
+  const Geom gf{(int)f.pitch, rows, f.pitch};
+  const dim3 gridf = grid_for((int)f.pitch, rows);
+  double *u = f.u - off, *r = f.r - off, *w = f.w - off, *p = f.p - off, *z = f.z - off;
+  const double *Mi = f.Mi - off;
+  Scalars h = fresh(0.0);
+  OPSB_CUDA(cudaMemcpyAsync(m.s64, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  k_resid3<<<grid3, block, 0, st>>>(g, f.Kx, f.Ky, f.Kz, f.u, f.u0, f.r, rx, ry, rz, eps, m.s64, m.part, m.cnt);
+  k_init<true><<<gridf, block, 0, st>>>(gf, r, Mi, z, p, max_iters, m.s64, m.part, m.cnt);
+  check_launch("heat solver 3D init");
+  launches_ += 2;
+  if (max_iters > 0) {
+    const std::string key = "3d" + key_of({f.Kx, f.Ky, f.Kz, f.u, f.r, f.w, f.p, f.z, f.Mi},
+                                          {rx, ry, rz, (double)f.nx, (double)f.ny, (double)f.nz, (double)f.pitch,
+                                           true_stop ? 1.0 : 0.0});
+    if (m.chunk64.key != key) {
+      if (m.chunk64.exec) cudaGraphExecDestroy(m.chunk64.exec);
+      m.chunk64.exec = nullptr;
+      m.chunk64.key.clear();
+      m.chunk64.exec = capture(st, [&] {
+        for (int it = 0; it < kChunk; it++) {
+          k_w3<<<grid3, block, 0, st>>>(g, f.Kx, f.Ky, f.Kz, f.p, f.w, rx, ry, rz, m.s64, m.part, m.cnt);
+          if (true_stop)
+            k_ur<double, true, STOP_TRUE><<<gridf, block, 0, st>>>(gf, u, p, r, w, Mi, z, m.s64, m.part, m.cnt);
+          else
+            k_ur<double, true, STOP_TEALEAF><<<gridf, block, 0, st>>>(gf, u, p, r, w, Mi, z, m.s64, m.part, m.cnt);
+          k_p<double><<<gridf, block, 0, st>>>(gf, p, z, m.s64);
+        }
+      });
+      m.chunk64.key = key;
+    }
+    launches_ += run_chunks(m.chunk64.exec, m.s64, max_iters, m.h_flag, m.ev, st, 3 * kChunk);
+  }
+  OPSB_CUDA(cudaMemcpyAsync(&h, m.s64, sizeof(h), cudaMemcpyDeviceToHost, st));
+  OPSB_CUDA(cudaStreamSynchronize(st));
+  out->initial_residual = sqrt(fabs(h.rr0));
+  out->error = h.err;
+  out->converged = h.done == 1 || (max_iters <= 0 && h.err < h.stop);
+  out->iterations = h.done == 1 ? h.iters - 1 : h.iters;
+  out->outer = 0;
+  Scalars t = fresh(0.0);
+  OPSB_CUDA(cudaMemcpyAsync(m.s32, &t, sizeof(t), cudaMemcpyHostToDevice, st));
+  k_resid3<<<grid3, block, 0, st>>>(g, f.Kx, f.Ky, f.Kz, f.u, f.u0, f.w, rx, ry, rz, 0.0, m.s32, m.part, m.cnt);
+  check_launch("heat solver 3D residual");
+  launches_ += 1;
+  OPSB_CUDA(cudaMemcpyAsync(&t, m.s32, sizeof(t), cudaMemcpyDeviceToHost, st));
+  OPSB_CUDA(cudaStreamSynchronize(st));
+  out->true_residual = sqrt(fabs(t.rr));
+}
 
 void Solver::diag(const Field2D &f, double rx, double ry, cudaStream_t st) {
   validate(f);

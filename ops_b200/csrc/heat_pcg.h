@@ -37,6 +37,17 @@ struct Field2D {
   double *u = nullptr, *r = nullptr, *w = nullptr, *p = nullptr, *z = nullptr, *Mi = nullptr;
 };
 
+// The 3D 7-point operator's fields: pointers address the first interior
+// cell of FP64 volumes with one halo cell on each side, x fastest, `pitch`
+// elements between rows and plane == pitch * (ny + 2) between z planes. The
+// solver's own fields (r, w, p, z, Mi) must be zero on every halo cell.
+struct Field3D {
+  int nx = 0, ny = 0, nz = 0;
+  long long pitch = 0, plane = 0;
+  const double *Kx = nullptr, *Ky = nullptr, *Kz = nullptr, *u0 = nullptr;
+  double *u = nullptr, *r = nullptr, *w = nullptr, *p = nullptr, *z = nullptr, *Mi = nullptr;
+};
+
 struct SolveStats {
   int iterations = 0;         // as the reference reports it (n - 1 on convergence)
   int outer = 0;              // reliable updates (mixed only)
@@ -70,6 +81,11 @@ class Solver {
   // iteration counts and results are those of the host loop.
   void fcg(const Field2D &f, double rx, double ry, double eps, int max_iters, const Precond &M, int window,
            cudaStream_t s, SolveStats *st, const Precond *fallback = nullptr, bool chunked = false);
+  // The same FP64 Jacobi-PCG for the 3D 7-point operator (stopping rule as
+  // pcg_fp64: TeaLeaf's sqrt|r.z|, or ||r|| with true_stop).
+  void pcg3d(const Field3D &f, double rx, double ry, double rz, bool true_stop, double eps, int max_iters,
+             cudaStream_t s, SolveStats *st);
+  void diag3(const Field3D &f, double rx, double ry, double rz, cudaStream_t s);
   // Mi = 1 / diag(A) on the interior (tea_leaf_common_init_diag_init_kernel).
   void diag(const Field2D &f, double rx, double ry, cudaStream_t s);
   // out = u0 - A u on the interior; returns ||out||.

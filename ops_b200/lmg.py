@@ -25,7 +25,7 @@ import ctypes
 import numpy as np
 
 from . import seeded
-from ._lib import HeatBatch, HeatStats, HeatSystem, check, lib
+from ._lib import HeatBatch, HeatStats, HeatSystem, HeatSystem3D, check, lib
 
 PCG, PCG_TRUE, MIXED, FCG_LEARNED, FCG_JACOBI, FCG_MG, FCG_LEARNED_MG = 0, 1, 2, 3, 4, 5, 6
 
@@ -83,6 +83,40 @@ def solve(Kx, Ky, u0, u, rx, ry, method=PCG_TRUE, net=-1, eps=1e-10, max_iters=1
                                     None if r_out is None else interior(r_out, pitch), ctypes.byref(st),
                                     None if stream is None else ctypes.c_void_p(stream)))
     return {k: getattr(st, k) for k, _ in HeatStats._fields_}
+
+
+def solve3d(Kx, Ky, Kz, u0, u, rx, ry, rz, method=PCG_TRUE, eps=1e-10, max_iters=100000, stream=None):
+    """3D 7-point heat solve (FP64 Jacobi-PCG) on padded (nz + 2, ny + 2,
+    nx + 2) FP64 CUDA tensors; u is updated. Returns the solve statistics."""
+    import torch
+    nz, ny, nx = Kx.shape[0] - 2, Kx.shape[1] - 2, Kx.shape[2] - 2
+    for t in (Kx, Ky, Kz, u0, u):
+        assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and tuple(t.shape) == tuple(Kx.shape)
+    pitch, plane = nx + 2, (nx + 2) * (ny + 2)
+
+    def first(t):
+        return ctypes.c_void_p(t.data_ptr() + 8 * (plane + pitch + 1))
+
+    sysd = HeatSystem3D(nx, ny, nz, pitch, plane, first(Kx), first(Ky), first(Kz), first(u0), first(u), rx, ry, rz)
+    st = HeatStats()
+    check(lib().ops_b200_heat_solve3d(ctypes.byref(sysd), method, eps, max_iters, ctypes.byref(st),
+                                      None if stream is None else ctypes.c_void_p(stream)))
+    return {k: getattr(st, k) for k, _ in HeatStats._fields_}
+
+
+def faces3d(rho):
+    """Face conductivities of a 3D density field, as padded_problem's in 2D:
+    (w- + w) / (2 w- w) on the faces between two interior cells, zero on the
+    domain's boundary faces; Kx, Ky, Kz as (nz + 2, ny + 2, nx + 2) arrays."""
+    nz, ny, nx = rho.shape
+    w = rho
+    Kx = np.zeros((nz + 2, ny + 2, nx + 2))
+    Ky = np.zeros_like(Kx)
+    Kz = np.zeros_like(Kx)
+    Kx[1:-1, 1:-1, 2:-1] = (w[:, :, :-1] + w[:, :, 1:]) / (2.0 * w[:, :, :-1] * w[:, :, 1:])
+    Ky[1:-1, 2:-1, 1:-1] = (w[:, :-1, :] + w[:, 1:, :]) / (2.0 * w[:, :-1, :] * w[:, 1:, :])
+    Kz[2:-1, 1:-1, 1:-1] = (w[:-1, :, :] + w[1:, :, :]) / (2.0 * w[:-1, :, :] * w[1:, :, :])
+    return Kx, Ky, Kz
 
 
 def mg_apply(Kx, Ky, r, z, rx, ry, stream=None):

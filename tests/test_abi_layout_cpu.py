@@ -15,6 +15,7 @@ PAIRS = [("ops_b200_arg", _lib.Arg), ("ops_b200_trid_system", _lib.TridSystem),
          ("ops_b200_clover_deck", _lib.CloverDeck), ("ops_b200_clover3d_state", _lib.Clover3DState),
          ("ops_b200_clover3d_deck", _lib.Clover3DDeck), ("ops_b200_tea_deck", _lib.TeaDeck),
          ("ops_b200_heat_system", _lib.HeatSystem), ("ops_b200_heat_stats", _lib.HeatStats),
+         ("ops_b200_heat_system3d", _lib.HeatSystem3D),
          ("ops_b200_heat_batch", _lib.HeatBatch), ("ops_b200_tridsolver_params", _lib.TridsolverParams)]
 
 
