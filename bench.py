@@ -1295,6 +1295,9 @@ def bench_mg(args, world, rank, local, pg):
 # ---------------------------------------------------------------------------
 H3_N = 512
 HEAT3D_BYTES = 128.0  # FP64 per cell-iteration: w = A p (p, Kx, Ky, Kz, w: 40) + u, r, z updates (64) + p (24)
+# DRAM bytes per cell of one iteration (k_w3 + k_ur + k_p) from one ncu capture
+# at 256^3 (profiles/heat3d_256_pcg_iteration_dram.md); they scale with the cells
+HEAT3D_TRAFFIC = 124.8
 
 
 def heat3d_problem(n, seed, local):
@@ -1371,10 +1374,13 @@ def bench_heat3d(args, world, rank, local, pg):
         "data": "synthetic (rho=1 background + 16 seeded boxes, rho log-uniform [0.1,100], energy U[0,1], seed 6)",
         "config": {"workload": f"heat3d_pcg_{N}^3", "grid": [N, N, N], "rx=ry=rz": rxyz, "eps": 1e-10,
                    "step": "one FP64 Jacobi-PCG solve of the 7-point operator to ||u0 - A u|| < 1e-10 ||r0||",
-                   "l2": "inputs larger than L2 (fields of 1.09 GB)", "parallelism": f"replicas x{world}"},
+                   "l2": f"inputs larger than L2 (fields of {8 * (N + 2) ** 3 / 1e9:.2f} GB)",
+                   "parallelism": f"replicas x{world}"},
         "iterations": iters, "final_residual_ratio": stats["final_residual"] / max(stats["initial_residual"], 1e-300),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": HEAT3D_TRAFFIC * cells,
+                     "traffic_source": "ncu capture of one iteration at 256^3, per cell x cells"
+                                       " (profiles/heat3d_256_pcg_iteration_dram.md)",
                      "kernel": "PCG iteration (k_w3 + k_ur + k_p)", "alg_bytes_per_cell_iteration": HEAT3D_BYTES,
                      "avg_iteration_ms": t * 1e3 / max(iters, 1), "peak_source": f"{peak_kind} hbm_gbs"},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": sum(h.numel() * 8 for h in hk),
