@@ -100,3 +100,30 @@ def test_heat_solve_arguments_are_checked_before_any_device_work():
     assert L.ops_b200_heat_solve(C.byref(bad), 5, -1, 1e-10, 100, 0, None, C.byref(st), None) == -1
     assert L.ops_b200_heat_mg_apply(C.byref(bad), fake, fake, None, None) == -1
     assert b"shape" in L.ops_b200_last_error()
+
+
+def test_heat_solve3d_arguments_are_checked_before_any_device_work():
+    """The 3D solve refuses a plane other than pitch * (ny + 2), a pitch
+    below nx + 2, methods other than the two PCG rules, a non-positive
+    tolerance and null fields with OPS_B200_ERR_ARG, before any device work."""
+    import ctypes as C
+
+    from ops_b200 import lib
+    from ops_b200._lib import HeatStats, HeatSystem3D
+    L = lib()
+    fake = C.c_void_p(4096)
+    st = HeatStats()
+
+    def solve(nx, ny, nz, pitch, plane, method=1, eps=1e-10, ptr=fake):
+        sysd = HeatSystem3D(nx, ny, nz, pitch, plane, ptr, fake, fake, fake, fake, 1.0, 1.0, 1.0)
+        return L.ops_b200_heat_solve3d(C.byref(sysd), method, eps, 100, C.byref(st), None)
+
+    assert solve(8, 8, 8, 10, 99) == -1                  # plane != pitch * (ny + 2)
+    assert b"shape" in L.ops_b200_last_error()
+    assert solve(8, 8, 8, 9, 90) == -1                   # pitch < nx + 2
+    assert solve(8, 8, 0, 10, 100) == -1                 # empty
+    assert solve(8, 8, 8, 10, 100, method=3) == -1       # the learned FCG is 2D only
+    assert b"method" in L.ops_b200_last_error()
+    assert solve(8, 8, 8, 10, 100, eps=0.0) == -1
+    assert solve(8, 8, 8, 10, 100, ptr=None) == -1       # null Kx
+    assert b"null" in L.ops_b200_last_error()
