@@ -544,7 +544,8 @@ int ops_b200_heat_solve(const ops_b200_heat_system *sys, int method, int net, do
  * face conductivities K (Kz(x,y,z) the face between z-1 and z). Pointers
  * address the first interior cell of FP64 volumes with one halo cell on
  * each side; plane == pitch * (ny + 2). Methods OPS_B200_HEAT_PCG and
- * OPS_B200_HEAT_PCG_TRUE (FP64 Jacobi-PCG, device-resident iterations).
+ * OPS_B200_HEAT_PCG_TRUE (FP64 Jacobi-PCG, device-resident iterations) and
+ * OPS_B200_HEAT_MIXED (FP32 Jacobi-PCG under FP64 reliable updates).
  * Synchronous on `stream`; not reentrant (a workspace is kept per size). */
 typedef struct ops_b200_heat_system3d {
   int nx, ny, nz;

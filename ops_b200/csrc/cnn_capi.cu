@@ -416,8 +416,8 @@ extern "C" int ops_b200_heat_solve3d(const ops_b200_heat_system3d *sys, int meth
     if (!sys || !sys->Kx || !sys->Ky || !sys->Kz || !sys->u0 || !sys->u) throw Error(E_ARG, "heat system 3D: null field");
     if (sys->nx < 1 || sys->ny < 1 || sys->nz < 1 || sys->pitch < sys->nx + 2 || sys->plane != sys->pitch * (sys->ny + 2))
       throw Error(E_ARG, "heat system 3D: bad shape (pitch >= nx + 2, plane == pitch * (ny + 2))");
-    if (method != OPS_B200_HEAT_PCG && method != OPS_B200_HEAT_PCG_TRUE)
-      throw Error(E_ARG, "heat system 3D: methods OPS_B200_HEAT_PCG and OPS_B200_HEAT_PCG_TRUE");
+    if (method != OPS_B200_HEAT_PCG && method != OPS_B200_HEAT_PCG_TRUE && method != OPS_B200_HEAT_MIXED)
+      throw Error(E_ARG, "heat system 3D: methods OPS_B200_HEAT_PCG, OPS_B200_HEAT_PCG_TRUE and OPS_B200_HEAT_MIXED");
     if (!(eps > 0.0) || max_iters < 0) throw Error(E_ARG, "heat system 3D: eps > 0 and max_iters >= 0 required");
     std::lock_guard<std::mutex> lk(g_mu);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -447,7 +447,10 @@ extern "C" int ops_b200_heat_solve3d(const ops_b200_heat_system3d *sys, int meth
     OPSB_CUDA(cudaEventCreate(&e1));
     OPSB_CUDA(cudaEventRecord(e0, s));
     try {
-      ws.solver.pcg3d(f, sys->rx, sys->ry, sys->rz, method == OPS_B200_HEAT_PCG_TRUE, eps, max_iters, s, &st);
+      if (method == OPS_B200_HEAT_MIXED)
+        ws.solver.pcg3d_mixed(f, sys->rx, sys->ry, sys->rz, eps, 0.1, max_iters, s, &st);
+      else
+        ws.solver.pcg3d(f, sys->rx, sys->ry, sys->rz, method == OPS_B200_HEAT_PCG_TRUE, eps, max_iters, s, &st);
       OPSB_CUDA(cudaEventRecord(e1, s));
       OPSB_CUDA(cudaEventSynchronize(e1));
     } catch (...) {
@@ -462,6 +465,7 @@ extern "C" int ops_b200_heat_solve3d(const ops_b200_heat_system3d *sys, int meth
     if (stats) {
       memset(stats, 0, sizeof(*stats));
       stats->iterations = st.iterations;
+      stats->updates = st.outer;
       stats->converged = st.converged;
       stats->initial_residual = st.initial_residual;
       stats->final_residual = st.true_residual;

@@ -474,28 +474,30 @@ struct Geom3 {
        row += gridDim.y * BY, y = row % (g).ny, z = row / (g).ny)                                            \
     for (int x = blockIdx.x * BX + threadIdx.x; x < (g).nx; x += gridDim.x * BX)
 
-__device__ __forceinline__ double smvp3(const double *__restrict__ Kx, const double *__restrict__ Ky,
-                                        const double *__restrict__ Kz, const double *__restrict__ u, long long i,
-                                        long long P, long long Q, double rx, double ry, double rz) {
-  const double kx0 = Kx[i], kx1 = Kx[i + 1], ky0 = Ky[i], ky1 = Ky[i + P], kz0 = Kz[i], kz1 = Kz[i + Q];
-  return (1.0 + rz * (kz1 + kz0) + ry * (ky1 + ky0) + rx * (kx1 + kx0)) * u[i] - rz * (kz1 * u[i + Q] + kz0 * u[i - Q]) -
+template <class T>
+__device__ __forceinline__ T smvp3(const T *__restrict__ Kx, const T *__restrict__ Ky, const T *__restrict__ Kz,
+                                   const T *__restrict__ u, long long i, long long P, long long Q, T rx, T ry, T rz) {
+  const T kx0 = Kx[i], kx1 = Kx[i + 1], ky0 = Ky[i], ky1 = Ky[i + P], kz0 = Kz[i], kz1 = Kz[i + Q];
+  return (T(1) + rz * (kz1 + kz0) + ry * (ky1 + ky0) + rx * (kx1 + kx0)) * u[i] - rz * (kz1 * u[i + Q] + kz0 * u[i - Q]) -
          ry * (ky1 * u[i + P] + ky0 * u[i - P]) - rx * (kx1 * u[i + 1] + kx0 * u[i - 1]);
 }
 
-// w = A p on the interior, pw = p.w -> alpha = rro / pw (k_w in 3D).
-__global__ void __launch_bounds__(NT, kResident) k_w3(Geom3 g, const double *__restrict__ Kx,
-                                                     const double *__restrict__ Ky, const double *__restrict__ Kz,
-                                                     const double *__restrict__ p, double *__restrict__ w, double rx,
-                                                     double ry, double rz, Scalars *s, double *part, unsigned *cnt) {
+// w = A p on the interior, pw = p.w -> alpha = rro / pw (k_w in 3D; FP64, or
+// FP32 for the mixed solver's inner iterations).
+template <class T>
+__global__ void __launch_bounds__(NT, kResident) k_w3(Geom3 g, const T *__restrict__ Kx, const T *__restrict__ Ky,
+                                                     const T *__restrict__ Kz, const T *__restrict__ p,
+                                                     T *__restrict__ w, T rx, T ry, T rz, Scalars *s, double *part,
+                                                     unsigned *cnt) {
   __shared__ double sm[kWarps];
   __shared__ int last;
   if (s->done) return;
   double acc[1] = {0.0};
   HEAT_CELLS3(g) {
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
-    const double wv = smvp3(Kx, Ky, Kz, p, i, g.pitch, g.plane, rx, ry, rz);
+    const T wv = smvp3<T>(Kx, Ky, Kz, p, i, g.pitch, g.plane, rx, ry, rz);
     w[i] = wv;
-    acc[0] = acc[0] + wv * p[i];
+    acc[0] = acc[0] + (double)wv * (double)p[i];
   }
   if (publish<1>(acc, part, cnt, sm, &last)) {
     const double t = grid_total<1>(part, 0, sm);
@@ -519,7 +521,7 @@ __global__ void __launch_bounds__(NT, kResident) k_resid3(Geom3 g, const double 
   double acc[1] = {0.0};
   HEAT_CELLS3(g) {
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
-    const double rv = u0[i] - smvp3(Kx, Ky, Kz, u, i, g.pitch, g.plane, rx, ry, rz);
+    const double rv = u0[i] - smvp3<double>(Kx, Ky, Kz, u, i, g.pitch, g.plane, rx, ry, rz);
     r[i] = rv;
     acc[0] = acc[0] + rv * rv;
   }
@@ -548,6 +550,12 @@ __global__ void __launch_bounds__(NT, kResident) k_diag3(Geom3 g, const double *
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     Mi[i] = 1.0 / (1.0 + rz * (Kz[i + g.plane] + Kz[i]) + ry * (Ky[i + g.pitch] + Ky[i]) + rx * (Kx[i + 1] + Kx[i]));
   }
+}
+
+// FP32 copy of n consecutive FP64 values (a padded volume, halos included).
+__global__ void __launch_bounds__(NT, kResident) k_flat_to_float(const double *__restrict__ a, float *__restrict__ fa,
+                                                                long long n) {
+  for (long long k = (long long)blockIdx.x * NT + tid_(); k < n; k += (long long)gridDim.x * NT) fa[k] = (float)a[k];
 }
 
 dim3 grid_for3(int nx, int rows) {
@@ -579,6 +587,7 @@ struct Solver::Impl {
   long long pitch32 = 0;
   float *Kx = nullptr, *Ky = nullptr, *Mi = nullptr, *r = nullptr, *p = nullptr, *w = nullptr, *z = nullptr,
         *e = nullptr;
+  float *Kz = nullptr;  // 3D only
   // replayed iteration chunks, rebuilt when any argument changes
   struct Chunk {
     cudaGraphExec_t exec = nullptr;
@@ -606,6 +615,23 @@ struct Solver::Impl {
     OPSB_CUDA(cudaMemset(cnt, 0, 64));
     OPSB_CUDA(cudaMallocHost(&h_flag, 2 * sizeof(int)));
     for (cudaEvent_t &x : ev) OPSB_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+  }
+
+  // The 3D mixed solver's nine FP32 fields, each a padded volume of nf
+  // values in the FP64 fields' flat layout, zero on every halo cell.
+  void ensure_f32_flat(size_t nf, cudaStream_t st) {
+    const size_t bytes = 9 * nf * sizeof(float);
+    if (bytes != f32_bytes || pitch32 != -1) {
+      cudaFree(f32);
+      f32 = nullptr;
+      OPSB_CUDA(cudaMalloc(&f32, bytes));
+      f32_bytes = bytes;
+      pitch32 = -1;  // the 2D layout must be rebuilt
+      chunk32.key.clear();
+    }
+    OPSB_CUDA(cudaMemsetAsync(f32, 0, bytes, st));
+    float **fields[9] = {&Kx, &Ky, &Kz, &Mi, &r, &p, &w, &z, &e};
+    for (int k = 0; k < 9; k++) *fields[k] = f32 + k * nf;
   }
 
   // Eight FP32 fields with a one-cell ring; x = 0 of the interior starts a
@@ -906,7 +932,7 @@ void Solver::pcg3d(const Field3D &f, double rx, double ry, double rz, bool true_
       m.chunk64.key.clear();
       m.chunk64.exec = capture(st, [&] {
         for (int it = 0; it < kChunk; it++) {
-          k_w3<<<grid3, block, 0, st>>>(g, f.Kx, f.Ky, f.Kz, f.p, f.w, rx, ry, rz, m.s64, m.part, m.cnt);
+          k_w3<double><<<grid3, block, 0, st>>>(g, f.Kx, f.Ky, f.Kz, f.p, f.w, rx, ry, rz, m.s64, m.part, m.cnt);
           if (true_stop)
             k_ur<double, true, STOP_TRUE><<<gridf, block, 0, st>>>(gf, u, p, r, w, Mi, z, m.s64, m.part, m.cnt);
           else
@@ -933,6 +959,86 @@ void Solver::pcg3d(const Field3D &f, double rx, double ry, double rz, bool true_
   OPSB_CUDA(cudaMemcpyAsync(&t, m.s32, sizeof(t), cudaMemcpyDeviceToHost, st));
   OPSB_CUDA(cudaStreamSynchronize(st));
   out->true_residual = sqrt(fabs(t.rr));
+}
+
+void Solver::pcg3d_mixed(const Field3D &f, double rx, double ry, double rz, double eps, double delta, int max_iters,
+                         cudaStream_t st, SolveStats *out) {
+  validate3(f);
+  if (!(delta > 0.0 && delta < 1.0)) throw Error(E_ARG, "heat solver: reliable-update delta must be in (0, 1)");
+  Impl &m = *m_;
+  m.ensure_base();
+  const long long off = f.plane + f.pitch + 1;
+  const size_t nf = (size_t)f.plane * (f.nz + 2);
+  m.ensure_f32_flat(nf, st);
+  launches_ = 0;
+  const Geom3 g{f.nx, f.ny, f.nz, f.pitch, f.plane};
+  const dim3 grid3 = grid_for3(f.nx, f.ny * f.nz), block(BX, BY);
+  const int rows = (f.ny + 2) * (f.nz + 2);
+  const Geom gf{(int)f.pitch, rows, f.pitch};
+  const dim3 gridf = grid_for((int)f.pitch, rows);
+  const dim3 grid1((unsigned)std::min<long long>(((long long)nf + NT - 1) / NT, 148LL * 16));
+  const float rxf = (float)rx, ryf = (float)ry, rzf = (float)rz;
+  k_flat_to_float<<<grid1, block, 0, st>>>(f.Kx - off, m.Kx, (long long)nf);
+  k_flat_to_float<<<grid1, block, 0, st>>>(f.Ky - off, m.Ky, (long long)nf);
+  k_flat_to_float<<<grid1, block, 0, st>>>(f.Kz - off, m.Kz, (long long)nf);
+  k_flat_to_float<<<grid1, block, 0, st>>>(f.Mi - off, m.Mi, (long long)nf);
+  Scalars h = fresh(0.0);
+  OPSB_CUDA(cudaMemcpyAsync(m.s64, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  k_resid3<<<grid3, block, 0, st>>>(g, f.Kx, f.Ky, f.Kz, f.u, f.u0, f.r, rx, ry, rz, eps, m.s64, m.part, m.cnt);
+  check_launch("heat solver 3D init");
+  launches_ += 5;
+  OPSB_CUDA(cudaMemcpyAsync(&h, m.s64, sizeof(h), cudaMemcpyDeviceToHost, st));
+  OPSB_CUDA(cudaStreamSynchronize(st));
+  const double r0 = sqrt(fabs(h.rr0));
+  out->initial_residual = r0;
+  const std::string key = "3d" + key_of({m.Kx, m.Ky, m.Kz, m.e, m.r, m.w, m.p, m.z, m.Mi},
+                                        {(double)rxf, (double)ryf, (double)rzf, (double)f.nx, (double)f.ny,
+                                         (double)f.nz, (double)f.pitch});
+  if (m.chunk32.key != key) {
+    if (m.chunk32.exec) cudaGraphExecDestroy(m.chunk32.exec);
+    m.chunk32.exec = nullptr;
+    m.chunk32.key.clear();
+    m.chunk32.exec = capture(st, [&] {
+      for (int it = 0; it < kChunk; it++) {
+        k_w3<float><<<grid3, block, 0, st>>>(g, m.Kx + off, m.Ky + off, m.Kz + off, m.p + off, m.w + off, rxf, ryf,
+                                             rzf, m.s32, m.part, m.cnt);
+        k_ur<float, true, STOP_RELIABLE><<<gridf, block, 0, st>>>(gf, m.e, m.p, m.r, m.w, m.Mi, m.z, m.s32, m.part,
+                                                                  m.cnt);
+        k_p<float><<<gridf, block, 0, st>>>(gf, m.p, m.z, m.s32);
+      }
+    });
+    m.chunk32.key = key;
+  }
+  int updates = 0, iters = 0;
+  double scale = 1.0;
+  bool done = h.done == 1 || r0 == 0.0;
+  Scalars in;
+  memset(&in, 0, sizeof(in));
+  while (!done) {
+    k_reinit32<true><<<gridf, block, 0, st>>>(gf, gf, f.r - off, m.r, m.Mi, m.z, updates == 0, eps, scale, delta,
+                                              max_iters, m.s32, m.part, m.cnt);
+    k_p<float><<<gridf, block, 0, st>>>(gf, m.p, m.z, m.s32);
+    check_launch("heat solver 3D reliable update");
+    launches_ += 2;
+    launches_ += run_chunks(m.chunk32.exec, m.s32, max_iters, m.h_flag, m.ev, st, 3 * kChunk);
+    OPSB_CUDA(cudaMemcpyAsync(&in, m.s32, sizeof(in), cudaMemcpyDeviceToHost, st));
+    k_update<<<gridf, block, 0, st>>>(gf, gf, f.u - off, m.e);
+    k_resid3<<<grid3, block, 0, st>>>(g, f.Kx, f.Ky, f.Kz, f.u, f.u0, f.r, rx, ry, rz, eps, m.s64, m.part, m.cnt);
+    check_launch("heat solver 3D reliable update");
+    launches_ += 2;
+    OPSB_CUDA(cudaMemcpyAsync(&h, m.s64, sizeof(h), cudaMemcpyDeviceToHost, st));
+    OPSB_CUDA(cudaStreamSynchronize(st));
+    updates++;
+    iters = in.iters;
+    done = h.done == 1;
+    if (done || in.done == 2 || in.iters >= max_iters || updates > 10000) break;
+    if (in.done == 1) scale *= 0.1;  // the estimate said converged, the FP64 residual disagrees
+  }
+  out->iterations = iters;
+  out->outer = updates;
+  out->converged = done;
+  out->error = h.err;
+  out->true_residual = h.err;
 }
 
 void Solver::diag(const Field2D &f, double rx, double ry, cudaStream_t st) {

@@ -86,6 +86,10 @@ class Solver {
   void pcg3d(const Field3D &f, double rx, double ry, double rz, bool true_stop, double eps, int max_iters,
              cudaStream_t s, SolveStats *st);
   void diag3(const Field3D &f, double rx, double ry, double rz, cudaStream_t s);
+  // pcg_mixed for the 3D operator: FP32 PCG under FP64 reliable updates,
+  // stopping on the FP64 ||u0 - A u|| < eps ||r0||. f.Mi must hold diag3's.
+  void pcg3d_mixed(const Field3D &f, double rx, double ry, double rz, double eps, double delta, int max_iters,
+                   cudaStream_t s, SolveStats *st);
   // Mi = 1 / diag(A) on the interior (tea_leaf_common_init_diag_init_kernel).
   void diag(const Field2D &f, double rx, double ry, cudaStream_t s);
   // out = u0 - A u on the interior; returns ||out||.

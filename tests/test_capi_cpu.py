@@ -122,7 +122,7 @@ def test_heat_solve3d_arguments_are_checked_before_any_device_work():
     assert b"shape" in L.ops_b200_last_error()
     assert solve(8, 8, 8, 9, 90) == -1                   # pitch < nx + 2
     assert solve(8, 8, 0, 10, 100) == -1                 # empty
-    assert solve(8, 8, 8, 10, 100, method=3) == -1       # the learned FCG is 2D only
+    assert solve(8, 8, 8, 10, 100, method=3) == -1       # the learned FCG is 2D only (methods 0, 1, 2)
     assert b"method" in L.ops_b200_last_error()
     assert solve(8, 8, 8, 10, 100, eps=0.0) == -1
     assert solve(8, 8, 8, 10, 100, ptr=None) == -1       # null Kx

@@ -118,6 +118,24 @@ def test_pcg_matches_numpy(gpu_runtime, shape, rxyz):
     assert np.linalg.norm(un[1:-1, 1:-1, 1:-1].reshape(-1) - exact) <= 1e-6 * np.linalg.norm(exact)
 
 
+@pytest.mark.parametrize("shape", [(24, 20, 16), (40, 8, 3)])
+def test_mixed_precision_reaches_the_fp64_residual(gpu_runtime, shape):
+    """FP32 inner PCG under FP64 reliable updates: the FP64 residual reaches
+    1e-10 and the solution agrees with the FP64 PCG solution."""
+    from ops_b200 import lmg
+    nx, ny, nz = shape
+    Kx, Ky, Kz, u0 = problem(nx, ny, nz, 31)
+    k = [cuda(a) for a in (Kx, Ky, Kz, u0)]
+    u64, u32 = cuda(u0), cuda(u0)
+    s64 = lmg.solve3d(*k, u64, 10.0, 10.0, 10.0, method=lmg.PCG_TRUE, eps=1e-10)
+    s32 = lmg.solve3d(*k, u32, 10.0, 10.0, 10.0, method=lmg.MIXED, eps=1e-10)
+    assert s64["converged"] and s32["converged"] and s32["updates"] >= 1
+    assert s32["final_residual"] < 1e-10 * s32["initial_residual"]
+    a, b = u64.cpu().numpy(), u32.cpu().numpy()
+    assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(a)
+    assert s32["iterations"] <= 1.3 * s64["iterations"] + 10
+
+
 def test_bad_shapes_are_refused(gpu_runtime):
     import ctypes
 
@@ -130,4 +148,4 @@ def test_bad_shapes_are_refused(gpu_runtime):
     bad = HeatSystem3D(4, 4, 4, 6, 35, *ptr, 1.0, 1.0, 1.0)  # plane != pitch * (ny + 2)
     assert lib().ops_b200_heat_solve3d(ctypes.byref(bad), lmg.PCG, 1e-10, 10, ctypes.byref(st), None) < 0
     ok = HeatSystem3D(4, 4, 4, 6, 36, *ptr, 1.0, 1.0, 1.0)
-    assert lib().ops_b200_heat_solve3d(ctypes.byref(ok), 3, 1e-10, 10, ctypes.byref(st), None) < 0  # method
+    assert lib().ops_b200_heat_solve3d(ctypes.byref(ok), 3, 1e-10, 10, ctypes.byref(st), None) < 0  # method (0-2)
