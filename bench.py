@@ -427,6 +427,8 @@ def bench_clover(args, world, rank, local, pg):
         "final_summary": {"vol": summ[-1, 2], "mass": summ[-1, 3], "ie": summ[-1, 4], "ke": summ[-1, 5],
                           "press": summ[-1, 6]},
     }
+    if rank == 0 and world == 1 and not args.no_learned:
+        line["learned_vs_pcg"] = learned_vs_pcg(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         base = cpu_reference_clover(args.cpu_clover_steps, threads)
@@ -435,6 +437,31 @@ def bench_clover(args, world, rank, local, pg):
                                     "sample": f"reference CloverLeaf OpenMP build, {CL_N}^2, {args.cpu_clover_steps}"
                                               f" steps (hydro loop wall time {base[1]:.2f} s)"}
     return line
+
+
+def learned_vs_pcg(args, local):
+    """The second half of the headline metric in the default line: time to
+    the 1e-10 residual of the 4096^2 heat solve with the learned
+    preconditioners against plain FP64 PCG, on this GPU in this run (the
+    networks are trained first, as `--workload learned` does). Failures are
+    reported in the object; they do not affect the CloverLeaf figures."""
+    import copy
+    try:
+        a = copy.copy(args)
+        a.steps, a.warmup, a.grid, a.no_cpu_baseline = 1, 3, None, True
+        t0 = time.perf_counter()
+        d = bench_learned(a, 1, 0, local, None)
+        return {"grid": [TEA_N, TEA_N], "eps": 1e-10, "plain_pcg_s": d["plain_pcg"]["seconds"],
+                "learned_fcg_s": d["learned_fcg"]["seconds"],
+                "learned_fcg_over_pcg": d["learned_fcg"]["time_ratio_vs_plain"],
+                "learned_mg_fcg_s": d["learned_mg_fcg"]["seconds"],
+                "learned_mg_fcg_over_pcg": d["learned_mg_fcg"]["time_ratio_vs_plain"],
+                "multigrid_fcg_s": d["multigrid_fcg"]["seconds"],
+                "note": "median of the timed solves after training both networks (bench.py --workload learned has"
+                        " the full record); not part of the CloverLeaf timing",
+                "wall_s": time.perf_counter() - t0}
+    except Exception as e:  # the headline line must survive
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 def reference_clover(args, world, rank):
@@ -1458,6 +1485,8 @@ def main():
                     help="tea: FP32 residual decrease between FP64 reliable updates")
     ap.add_argument("--cpu-tea-iters", type=int, default=100, help="tea: CG iterations in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="clover: skip the learned-vs-PCG heat solve comparison in the line")
     ap.add_argument("--kernel-table", action="store_true",
                     help="clover, clover3d: print the per-kernel timing table of the roofline pass on stderr")
     args = ap.parse_args()
